@@ -1,0 +1,190 @@
+"""ctypes front for the CPU oracle (oracle/liboracle.so).  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, as the
+checker.  The product (cuvslam_b200) never imports it.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+F = ctypes.c_float
+
+TEXTURE = 0
+EXACT = 1
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.or_level_sizes.argtypes = [I, I, I, P, P]
+        L.or_cast_u8.argtypes = [P, I, I, P]
+        L.or_gauss_downscale.argtypes = [P, I, I, P, I, I]
+        L.or_gradients.argtypes = [P, I, I, P, P]
+        L.or_gftt_response.argtypes = [P, P, I, I, P]
+        L.or_bins.argtypes = [P, I, I, P]
+        L.or_select.argtypes = [P, I, I, P, I, I, I, I, I, I, P, P, P, P, P, P, P, P]
+        L.or_select.restype = I
+        L.or_tex_sample.argtypes = [P, I, I, F, F, I]
+        L.or_tex_sample.restype = F
+        L.or_lk_track.argtypes = [I, P, P, P, P, P, P, P, I, I]
+        L.or_lk_track_horizontal.argtypes = [I, P, P, P, P, P, P, I, I]
+        L.or_lk_track_f64.argtypes = [I, P, P, P, P, P, P, P, I]
+        for name, args, res in _CPU_SIGS:
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = res
+        _LIB = L
+    return _LIB
+
+
+# CPU-semantics (cuVSLAM use_gpu=false) entry points, see cpu_tracker.c
+_CPU_SIGS = [
+    ("cpu_ctx_create", [I, I, I], P),
+    ("cpu_ctx_destroy", [P], None),
+    ("cpu_ctx_build", [P, P], I),
+    ("cpu_ctx_levels", [P], I),
+    ("cpu_ctx_level", [P, I, P, P, P], I),
+    ("cpu_track", [P, P, P, P, I, P, P, I], I),
+    ("cpu_select", [P, P, I, I, I, I, I, I, P], I),
+]
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def level_sizes(w, h, max_levels=10):
+    ws = np.zeros(10, np.int32)
+    hs = np.zeros(10, np.int32)
+    n = lib().or_level_sizes(w, h, max_levels, _p(ws), _p(hs))
+    return list(zip(ws[:n].tolist(), hs[:n].tolist()))
+
+
+def pyramid(img_u8, max_levels=10):
+    """[(level image, gx, gy)] for the reference GPU pyramid + gradient pyramid."""
+    img_u8 = np.ascontiguousarray(img_u8, np.uint8)
+    h, w = img_u8.shape
+    L = lib()
+    out = []
+    prev = np.zeros((h, w), np.float32)
+    L.or_cast_u8(_p(img_u8), w, h, _p(prev))
+    for i, (lw, lh) in enumerate(level_sizes(w, h, max_levels)):
+        if i > 0:
+            nxt = np.zeros((lh, lw), np.float32)
+            L.or_gauss_downscale(_p(prev), prev.shape[1], prev.shape[0], _p(nxt), lw, lh)
+            prev = nxt
+        gx = np.zeros_like(prev)
+        gy = np.zeros_like(prev)
+        L.or_gradients(_p(prev), lw, lh, _p(gx), _p(gy))
+        out.append((prev, gx, gy))
+    return out
+
+
+def pyramid_f32(img_f32, max_levels=10):
+    """Same as `pyramid` but from a float32 base level."""
+    prev = np.ascontiguousarray(img_f32, np.float32)
+    h, w = prev.shape
+    L = lib()
+    out = []
+    for i, (lw, lh) in enumerate(level_sizes(w, h, max_levels)):
+        if i > 0:
+            nxt = np.zeros((lh, lw), np.float32)
+            L.or_gauss_downscale(_p(prev), prev.shape[1], prev.shape[0], _p(nxt), lw, lh)
+            prev = nxt
+        gx = np.zeros_like(prev)
+        gy = np.zeros_like(prev)
+        L.or_gradients(_p(prev), lw, lh, _p(gx), _p(gy))
+        out.append((prev, gx, gy))
+    return out
+
+
+def gftt(gx, gy):
+    gx = np.ascontiguousarray(gx, np.float32)
+    gy = np.ascontiguousarray(gy, np.float32)
+    h, w = gx.shape
+    r = np.zeros((h, w), np.float32)
+    lib().or_gftt_response(_p(gx), _p(gy), w, h, _p(r))
+    return r
+
+
+def bins(resp):
+    resp = np.ascontiguousarray(resp, np.float32)
+    h, w = resp.shape
+    b = np.zeros(64, np.float32)
+    lib().or_bins(_p(resp), w, h, _p(b))
+    return b
+
+
+def select(resp, alive=None, num_desired=450, borders=(0, 0, 0, 0), mask=None):
+    resp = np.ascontiguousarray(resp, np.float32)
+    h, w = resp.shape
+    cw, ch = w // 8, h // 8
+    cap = max(cw * ch, 1)
+    alive = np.zeros((0, 2), np.float32) if alive is None else np.ascontiguousarray(alive, np.float32).reshape(-1, 2)
+    nms = np.zeros((h, w), np.float32)
+    cmax = np.zeros(cap, np.float32)
+    cidx = np.zeros(2 * cap, np.uint32)
+    kp = np.zeros(3 * cap, np.float32)
+    b = np.zeros(64, np.float32)
+    sel = np.zeros(2 * max(num_desired, 1), np.float32)
+    nkp = ctypes.c_int(0)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    n = lib().or_select(_p(resp), w, h, _p(alive), len(alive), num_desired, borders[0], borders[1], borders[2],
+                        borders[3], None if m is None else _p(m), _p(nms), _p(cmax), _p(cidx), _p(kp),
+                        ctypes.byref(nkp), _p(b), _p(sel))
+    return dict(nms=nms, cell_max=cmax[:cw * ch].reshape(ch, cw), cell_idx=cidx[:2 * cw * ch].reshape(ch, cw, 2),
+                kp=kp[:3 * nkp.value].reshape(-1, 3), bins=b, sel=sel[:2 * n].reshape(-1, 2))
+
+
+def tex_sample(img, xy, mode=TEXTURE):
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape
+    L = lib()
+    return np.array([L.or_tex_sample(_p(img), w, h, float(x), float(y), mode) for x, y in np.asarray(xy)],
+                    np.float32)
+
+
+def _level_ptrs(arrs):
+    arrs = [np.ascontiguousarray(a, np.float32) for a in arrs]
+    ptrs = (ctypes.c_void_p * 10)(*[a.ctypes.data for a in arrs])
+    return arrs, ptrs
+
+
+def lk(prev_pyr, cur_pyr, tracks, mode=TEXTURE, horizontal=False, f64=False):
+    """Run the LK oracle; prev_pyr/cur_pyr are lists of (img, gx, gy) per level.  Returns a copy of
+    `tracks` (TRACK_DTYPE records) updated as the reference kernel would."""
+    t = np.ascontiguousarray(tracks.copy())
+    levels = len(prev_pyr)
+    ws = np.array([p[0].shape[1] for p in prev_pyr] + [0] * (10 - levels), np.int32)
+    hs = np.array([p[0].shape[0] for p in prev_pyr] + [0] * (10 - levels), np.int32)
+    keep1, pgx = _level_ptrs([p[1] for p in prev_pyr])
+    keep2, pgy = _level_ptrs([p[2] for p in prev_pyr])
+    keep3, pim = _level_ptrs([p[0] for p in prev_pyr])
+    keep4, cim = _level_ptrs([p[0] for p in cur_pyr[:levels]])
+    L = lib()
+    if f64:
+        L.or_lk_track_f64(levels, _p(ws), _p(hs), pgx, pgy, pim, cim, _p(t), len(t))
+    elif horizontal:
+        L.or_lk_track_horizontal(levels, _p(ws), _p(hs), pgx, pim, cim, _p(t), len(t), mode)
+    else:
+        L.or_lk_track(levels, _p(ws), _p(hs), pgx, pgy, pim, cim, _p(t), len(t), mode)
+    del keep1, keep2, keep3, keep4
+    return t

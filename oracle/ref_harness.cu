@@ -1,0 +1,364 @@
+// Test-only harness around the reference's own CUDA kernels (cuVSLAM libs/cuda_modules/cuda_kernels).
+//
+// This file is oracle infrastructure: it is compiled together with the reference's unmodified
+// kernel sources (image_pyramid.cu, convolutions.cu, gftt.cu, selection_v2.cu, sort.cu,
+// lk_tracker.cu) by oracle/build_ref.sh into oracle/_ref/libcuvslam_ref.so.  Only tests and the
+// golden-fixture script load it; the product never does.
+//
+// It restates, in plain host code, the launch sequences of the reference host wrappers so that the
+// reference kernels run exactly as cuVSLAM's MonoSOFGPU drives them:
+//   - GPUImage<float> pitched storage + point/linear texture objects   (cuda_helper.h:297-300,402-431)
+//   - ImageCast::cast (u8 upload + cast_image)                          (image_cast.cpp:33-47)
+//   - GaussianGPUImagePyramid::build / prepare_levels                   (image_pyramid.h:81-98,136-151)
+//   - GPUGradientPyramid::set                                           (gradient_pyramid.cpp:83-118)
+//   - GPUSelection::computeGFTTAndSelectFeatures incl. host quota loop  (selection_v2.cpp:27-184)
+//   - GPULKFeatureTracker::track_points                                 (cuda_modules/lk_tracker.cpp:24-73)
+// Every entry point takes and returns HOST buffers and synchronises; it is a checker, not fast.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "cuda_modules/cuda_kernels/cuda_kernels.h"
+
+using namespace cuvslam::cuda;
+
+namespace {
+
+constexpr int kMaxLevels = 10;
+constexpr int kMinDim = 15;
+
+#define HCHECK(x)                         \
+  do {                                    \
+    cudaError_t e_ = (x);                 \
+    if (e_ != cudaSuccess) return (int)e_; \
+  } while (0)
+
+struct DevImage {
+  float* ptr = nullptr;
+  size_t pitch = 0;
+  int w = 0, h = 0;
+  cudaTextureObject_t tex_point = 0, tex_linear = 0;
+
+  cudaError_t alloc(int cols, int rows) {
+    w = cols;
+    h = rows;
+    cudaError_t e = cudaMallocPitch((void**)&ptr, &pitch, (size_t)cols * sizeof(float), rows);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = ptr;
+    rd.res.pitch2D.width = cols;
+    rd.res.pitch2D.height = rows;
+    rd.res.pitch2D.pitchInBytes = pitch;
+    rd.res.pitch2D.desc = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    // Same descriptors as the reference's GPUImage::prepare_texture.
+    td.addressMode[0] = cudaAddressModeMirror;
+    td.addressMode[1] = cudaAddressModeMirror;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&tex_point, &rd, &td, nullptr);
+    if (e != cudaSuccess) return e;
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    return cudaCreateTextureObject(&tex_linear, &rd, &td, nullptr);
+  }
+  ~DevImage() {
+    if (tex_point) cudaDestroyTextureObject(tex_point);
+    if (tex_linear) cudaDestroyTextureObject(tex_linear);
+    if (ptr) cudaFree(ptr);
+  }
+  cudaError_t upload(const float* host) {
+    return cudaMemcpy2D(ptr, pitch, host, (size_t)w * 4, (size_t)w * 4, h, cudaMemcpyHostToDevice);
+  }
+  cudaError_t download(float* host) const {
+    return cudaMemcpy2D(host, (size_t)w * 4, ptr, pitch, (size_t)w * 4, h, cudaMemcpyDeviceToHost);
+  }
+};
+
+int level_count(int w, int h, int max_levels) {
+  int n = 0;
+  while (n < max_levels) {
+    ++n;
+    h = (h + 1) / 2;
+    w = (w + 1) / 2;
+    if (h < kMinDim || w < kMinDim) break;
+  }
+  return n;
+}
+
+struct Pyr {
+  int n = 0;
+  std::unique_ptr<DevImage> img[kMaxLevels], gx[kMaxLevels], gy[kMaxLevels];
+};
+
+int init_tables() {
+  HCHECK(init_scaler());
+  HCHECK(init_conv_kernels());
+  HCHECK(init_gauss_coeffs());
+  HCHECK(init_gauss_square_kernel());
+  return 0;
+}
+
+// ImageCast::cast + GaussianGPUImagePyramid::build + GPUGradientPyramid::set.
+int build(const uint8_t* host_u8, int w, int h, int max_levels, Pyr& p, cudaStream_t s) {
+  p.n = level_count(w, h, max_levels);
+  int lw = w, lh = h;
+  for (int l = 0; l < p.n; ++l) {
+    p.img[l].reset(new DevImage);
+    p.gx[l].reset(new DevImage);
+    p.gy[l].reset(new DevImage);
+    HCHECK(p.img[l]->alloc(lw, lh));
+    HCHECK(p.gx[l]->alloc(lw, lh));
+    HCHECK(p.gy[l]->alloc(lw, lh));
+    lw = (lw + 1) / 2;
+    lh = (lh + 1) / 2;
+  }
+  uint8_t* d_u8 = nullptr;
+  size_t u8_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&d_u8, &u8_pitch, w, h));
+  HCHECK(cudaMemcpy2D(d_u8, u8_pitch, host_u8, w, w, h, cudaMemcpyHostToDevice));
+  DevImage cast;
+  HCHECK(cast.alloc(w, h));
+  HCHECK(cast_image(d_u8, u8_pitch, cast.ptr, cast.pitch, {(unsigned)w, (unsigned)h}, s));
+  HCHECK(cudaMemcpy2DAsync(p.img[0]->ptr, p.img[0]->pitch, cast.ptr, cast.pitch, (size_t)w * 4, h,
+                           cudaMemcpyDeviceToDevice, s));
+  for (int l = 0; l + 1 < p.n; ++l) {
+    const DevImage& a = *p.img[l];
+    DevImage& b = *p.img[l + 1];
+    HCHECK(gaussian_scaling(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, b.ptr, b.pitch,
+                            {(unsigned)b.w, (unsigned)b.h}, s));
+  }
+  for (int l = 0; l < p.n; ++l) {
+    const DevImage& a = *p.img[l];
+    HCHECK(conv_grad_x(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, p.gx[l]->ptr, p.gx[l]->pitch, s));
+    HCHECK(conv_grad_y(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, p.gy[l]->ptr, p.gy[l]->pitch, s));
+  }
+  HCHECK(cudaStreamSynchronize(s));
+  cudaFree(d_u8);
+  return 0;
+}
+
+Pyramid make_pyr(const Pyr& p, std::unique_ptr<DevImage> const* arr) {
+  Pyramid out;
+  memset(&out, 0, sizeof(out));
+  out.levels = p.n;
+  for (int l = 0; l < p.n; ++l) {
+    out.level_tex[l] = arr[l]->tex_linear;
+    out.level_sizes[l] = {arr[l]->w, arr[l]->h};
+  }
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_level_count(int w, int h, int max_levels) { return level_count(w, h, max_levels); }
+
+// Pyramid + gradient pyramid of one u8 image.  Outputs are packed level after level
+// (level l holds w_l*h_l floats, row-major, no padding).
+int ref_pyramid(const uint8_t* img, int w, int h, int max_levels, int* nlev, float* levels, float* gx, float* gy) {
+  int rc = init_tables();
+  if (rc) return rc;
+  Pyr p;
+  rc = build(img, w, h, max_levels, p, 0);
+  if (rc) return rc;
+  *nlev = p.n;
+  size_t off = 0;
+  for (int l = 0; l < p.n; ++l) {
+    HCHECK(p.img[l]->download(levels + off));
+    HCHECK(p.gx[l]->download(gx + off));
+    HCHECK(p.gy[l]->download(gy + off));
+    off += (size_t)p.img[l]->w * p.img[l]->h;
+  }
+  return 0;
+}
+
+// GPUSelection::computeGFTTAndSelectFeatures on level 0 of the pyramid of `img`.
+// Intermediate buffers are returned for stage-by-stage comparison:
+//   gftt[w*h], nms[w*h] (after filter_maximums), cell_max[cw*ch], cell_idx[cw*ch*2] (x,y),
+//   kp[cap*3] sorted keypoints (x,y,strength) with *n_kp entries, bins[64],
+//   sel[num_desired*2] selected features with *n_sel entries.
+int ref_select(const uint8_t* img, int w, int h, const float* alive_xy, int n_alive, int num_desired, int border_top,
+               int border_bottom, int border_left, int border_right, float* gftt, float* nms, float* cell_max,
+               uint32_t* cell_idx, float* kp_out, int* n_kp, float* bins_out, float* sel, int* n_sel) {
+  int rc = init_tables();
+  if (rc) return rc;
+  Pyr p;
+  rc = build(img, w, h, 1, p, 0);
+  if (rc) return rc;
+  cudaStream_t s = 0;
+  const uint2 size = {(unsigned)w, (unsigned)h};
+  const uint2 bin_size = {(unsigned)(w / 8), (unsigned)(h / 8)};
+  const uint2 num_bins = {8, 8};
+  const uint2 ds = {(unsigned)w / 8, (unsigned)h / 8};
+  const int max_tracks = (int)(ds.x * ds.y);
+
+  DevImage val, maxim, dsm;
+  HCHECK(val.alloc(w, h));
+  HCHECK(maxim.alloc(w, h));
+  HCHECK(dsm.alloc((int)ds.x, (int)ds.y));
+  uint2* idx = nullptr;
+  size_t idx_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&idx, &idx_pitch, ds.x * sizeof(uint2), ds.y));
+  Keypoint* kp = nullptr;
+  HCHECK(cudaMalloc((void**)&kp, sizeof(Keypoint) * (size_t)(max_tracks > 0 ? max_tracks : 1)));
+  float* bins = nullptr;  // [0]=kpCount, [1]=kpIndex (as int), [2..65]=bins
+  HCHECK(cudaMalloc((void**)&bins, sizeof(float) * 66));
+  HCHECK(cudaMemset(bins, 0, sizeof(float) * 66));
+  size_t tmp_bytes = sort_keypoints_get_temp_buffer_size((size_t)max_tracks);
+  void* tmp = nullptr;
+  HCHECK(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 1));
+
+  int n_old = n_alive < max_tracks ? n_alive : max_tracks;
+  std::vector<Keypoint> host_kp((size_t)(max_tracks > 0 ? max_tracks : 1));
+  for (int i = 0; i < n_old; ++i) host_kp[i] = {alive_xy[2 * i], alive_xy[2 * i + 1], 0.f};
+  if (n_old > 0) HCHECK(cudaMemcpy(kp, host_kp.data(), sizeof(Keypoint) * n_old, cudaMemcpyHostToDevice));
+
+  HCHECK(gftt_values(p.gx[0]->tex_point, p.gy[0]->tex_point, val.ptr, val.pitch, size, s));
+  HCHECK(accumulateGFTT(val.tex_point, size, bin_size, num_bins, bins + 2, s));
+  HCHECK(non_max_suppression(val.tex_point, size, maxim.ptr, maxim.pitch, s));
+  if (n_old > 0) HCHECK(filter_maximums(maxim.ptr, size, maxim.pitch, kp, (size_t)n_old, s));
+  int kp_count = 0;
+  std::vector<float> hb(66, 0.f);
+  if (max_tracks > 0) {
+    HCHECK(downsample_gftt_x8(maxim.ptr, maxim.pitch, dsm.ptr, ds, dsm.pitch, idx, idx_pitch, s));
+    HCHECK(select_features(val.ptr, size, val.pitch, dsm.ptr, ds, dsm.pitch, idx, idx_pitch, kp, (size_t)max_tracks,
+                           (int*)bins, (int*)bins + 1, s));
+  }
+  HCHECK(cudaMemcpy(hb.data(), bins, sizeof(float) * 66, cudaMemcpyDeviceToHost));
+  memcpy(&kp_count, hb.data(), sizeof(int));
+  if (kp_count > 0) sort_keypoints(kp, (size_t)kp_count, tmp, tmp_bytes, s);
+  HCHECK(cudaStreamSynchronize(s));
+  HCHECK(cudaGetLastError());
+
+  HCHECK(val.download(gftt));
+  HCHECK(maxim.download(nms));
+  if (max_tracks > 0) {
+    HCHECK(dsm.download(cell_max));
+    std::vector<uint2> hi((size_t)max_tracks);
+    HCHECK(cudaMemcpy2D(hi.data(), ds.x * sizeof(uint2), idx, idx_pitch, ds.x * sizeof(uint2), ds.y,
+                        cudaMemcpyDeviceToHost));
+    for (int i = 0; i < max_tracks; ++i) {
+      cell_idx[2 * i] = hi[i].x;
+      cell_idx[2 * i + 1] = hi[i].y;
+    }
+  }
+  if (kp_count > 0) HCHECK(cudaMemcpy(host_kp.data(), kp, sizeof(Keypoint) * kp_count, cudaMemcpyDeviceToHost));
+  *n_kp = kp_count;
+  for (int i = 0; i < kp_count; ++i) {
+    kp_out[3 * i] = host_kp[i].x;
+    kp_out[3 * i + 1] = host_kp[i].y;
+    kp_out[3 * i + 2] = host_kp[i].strength;
+  }
+  for (int i = 0; i < 64; ++i) bins_out[i] = hb[i + 2];
+
+  // Host quota loop of GPUSelection::computeGFTTAndSelectFeatures (selection_v2.cpp:108-183).
+  float sum = 0.f;
+  for (int i = 0; i < 64; ++i) sum += hb[i + 2];
+  size_t prev_cnt[64] = {0}, want[64] = {0}, added[64] = {0};
+  for (int i = 0; i < n_alive; ++i) {
+    unsigned bx = (unsigned)(alive_xy[2 * i] / (float)bin_size.x);
+    unsigned by = (unsigned)(alive_xy[2 * i + 1] / (float)bin_size.y);
+    if (bx < 8 && by < 8) prev_cnt[by * 8 + bx]++;
+  }
+  const size_t expected = (size_t)n_alive + (size_t)num_desired;
+  for (int i = 0; i < 64; ++i) {
+    // A zero strength sum makes the reference's quota a NaN cast (undefined); no quota here.
+    if (!(sum > 0.f)) break;
+    size_t e = (size_t)std::round((float)expected * hb[i + 2] / sum);
+    if (e > prev_cnt[i]) want[i] = e - prev_cnt[i];
+  }
+  int out_n = 0;
+  for (int i = 0; i < kp_count; ++i) {
+    float x = host_kp[i].x, y = host_kp[i].y;
+    if (x < border_left || x > (float)(w - 1 - border_right) || y < border_top || y > (float)(h - 1 - border_bottom))
+      continue;
+    unsigned bx = (unsigned)(x / (float)bin_size.x), by = (unsigned)(y / (float)bin_size.y);
+    if (bx < 8 && by < 8) {
+      unsigned b = by * 8 + bx;
+      if (added[b] < want[b]) {
+        added[b]++;
+        if (out_n < num_desired) {
+          sel[2 * out_n] = x;
+          sel[2 * out_n + 1] = y;
+          ++out_n;
+        } else {
+          break;
+        }
+      }
+    }
+  }
+  *n_sel = out_n;
+  cudaFree(idx);
+  cudaFree(kp);
+  cudaFree(bins);
+  cudaFree(tmp);
+  return 0;
+}
+
+// GPULKFeatureTracker::track_points (or GPULKTrackerHorizontal) between the pyramids of two u8
+// images.  `tracks` holds n reference TrackData records (80 bytes each), updated in place.
+int ref_lk(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int max_levels, void* tracks, int n,
+           int horizontal) {
+  int rc = init_tables();
+  if (rc) return rc;
+  if (sizeof(TrackData) != 80) return -1;
+  Pyr pp, cp;
+  rc = build(prev_img, w, h, max_levels, pp, 0);
+  if (rc) return rc;
+  rc = build(cur_img, w, h, max_levels, cp, 0);
+  if (rc) return rc;
+  TrackData* d = nullptr;
+  HCHECK(cudaMalloc((void**)&d, sizeof(TrackData) * (size_t)(n > 0 ? n : 1)));
+  HCHECK(cudaMemcpy(d, tracks, sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
+  Pyramid gx = make_pyr(pp, pp.gx), gy = make_pyr(pp, pp.gy), pi = make_pyr(pp, pp.img), ci = make_pyr(cp, cp.img);
+  if (n > 0) {
+    if (horizontal)
+      HCHECK(lk_track_horizontal(gx, pi, ci, d, n, 0));
+    else
+      HCHECK(lk_track(gx, gy, pi, ci, d, n, 0));
+  }
+  HCHECK(cudaDeviceSynchronize());
+  HCHECK(cudaMemcpy(tracks, d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return 0;
+}
+
+// Hardware bilinear texture sampling with the reference's linear texture descriptor
+// (cudaFilterModeLinear, unnormalised coordinates).  Used to pin the oracle's emulation of
+// the texture unit's 8-bit-fraction weights.
+__global__ void tex_probe_kernel(cudaTextureObject_t t, const float2* xy, int n, float* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = tex2D<float>(t, xy[i].x, xy[i].y);
+}
+
+int ref_tex_probe(const float* img, int w, int h, const float* xy, int n, float* out) {
+  DevImage im;
+  HCHECK(im.alloc(w, h));
+  HCHECK(im.upload(img));
+  float2* dxy = nullptr;
+  float* dout = nullptr;
+  HCHECK(cudaMalloc((void**)&dxy, sizeof(float2) * (size_t)n));
+  HCHECK(cudaMalloc((void**)&dout, sizeof(float) * (size_t)n));
+  HCHECK(cudaMemcpy(dxy, xy, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice));
+  tex_probe_kernel<<<(n + 255) / 256, 256>>>(im.tex_linear, dxy, n, dout);
+  HCHECK(cudaGetLastError());
+  HCHECK(cudaDeviceSynchronize());
+  HCHECK(cudaMemcpy(out, dout, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+  cudaFree(dxy);
+  cudaFree(dout);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+"""Generates the golden fixtures under tests/golden/.
+
+Step 1 (any machine, no GPU):   python tests/golden/make_golden.py inputs
+    Draws the seeded synthetic input frames and writes tests/golden/inputs.npz.
+Step 2 (a B200, after oracle/build_ref.sh built oracle/_ref/libcuvslam_ref.so):
+    python tests/golden/make_golden.py reference --out DIR
+    Runs the reference's own CUDA kernels (compiled unchanged from cuVSLAM by oracle/build_ref.sh)
+    on those inputs and writes DIR/reference.npz (compact: hashes of every pyramid/gradient level,
+    the sorted keypoints, the selected features, the LK results and a texture-sampling probe) and
+    DIR/reference_full.npz (every intermediate array, for debugging; not committed).
+The committed tests/golden/reference.npz is the step-2 output.
+"""
+
+import argparse
+import ctypes
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from cuvslam_b200 import synthetic  # noqa: E402
+from cuvslam_b200.types import TRACK_DTYPE, level_sizes, make_tracks  # noqa: E402
+
+# name -> (width, height, camera id)
+CASES = {
+    "c1": (752, 480, 0),  # the 752x480 stereo-pair configuration
+    "half": (376, 240, 1),
+    "odd": (97, 61, 2),
+    "tiny": (31, 17, 3),
+}
+
+
+def make_inputs(path):
+    arrays = {}
+    for name, (w, h, cam) in CASES.items():
+        prev, nxt, warp = synthetic.frame_pair(cam, w, h)
+        arrays[f"{name}/prev"] = prev
+        arrays[f"{name}/next"] = nxt
+        arrays[f"{name}/warp"] = np.array([warp.theta, warp.scale, warp.tx, warp.ty, warp.cx, warp.cy])
+    np.savez_compressed(path, **arrays)
+
+
+def _lib():
+    p = os.path.join(ROOT, "oracle", "_ref", "libcuvslam_ref.so")
+    lib = ctypes.CDLL(p)
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    lib.ref_pyramid.argtypes = [P, I, I, I, P, P, P, P]
+    lib.ref_select.argtypes = [P, I, I, P, I, I, I, I, I, I, P, P, P, P, P, P, P, P, P]
+    lib.ref_lk.argtypes = [P, P, I, I, I, P, I, I]
+    lib.ref_tex_probe.argtypes = [P, I, I, P, I, P]
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def ref_pyramid(lib, img, max_levels=10):
+    h, w = img.shape
+    sizes = level_sizes(w, h, max_levels)
+    total = sum(a * b for a, b in sizes)
+    lv, gx, gy = (np.zeros(total, np.float32) for _ in range(3))
+    n = ctypes.c_int(0)
+    img = np.ascontiguousarray(img)
+    rc = lib.ref_pyramid(_ptr(img), w, h, max_levels, ctypes.byref(n), _ptr(lv), _ptr(gx), _ptr(gy))
+    assert rc == 0 and n.value == len(sizes), (rc, n.value)
+    out, off = [], 0
+    for (a, b) in sizes:
+        out.append((lv[off:off + a * b].reshape(b, a), gx[off:off + a * b].reshape(b, a), gy[off:off + a * b].reshape(b, a)))
+        off += a * b
+    return out
+
+
+def ref_select(lib, img, alive, num_desired, borders=(0, 0, 0, 0)):
+    h, w = img.shape
+    cw, ch = w // 8, h // 8
+    cap = max(cw * ch, 1)
+    gftt = np.zeros((h, w), np.float32)
+    nms = np.zeros((h, w), np.float32)
+    cmax = np.zeros(cap, np.float32)
+    cidx = np.zeros(cap * 2, np.uint32)
+    kp = np.zeros(cap * 3, np.float32)
+    bins = np.zeros(64, np.float32)
+    sel = np.zeros(max(num_desired, 1) * 2, np.float32)
+    nkp, nsel = ctypes.c_int(0), ctypes.c_int(0)
+    alive = np.ascontiguousarray(alive, np.float32).reshape(-1, 2)
+    img = np.ascontiguousarray(img)
+    rc = lib.ref_select(_ptr(img), w, h, _ptr(alive), len(alive), num_desired, *borders, _ptr(gftt), _ptr(nms),
+                        _ptr(cmax), _ptr(cidx), _ptr(kp), ctypes.byref(nkp), _ptr(bins), _ptr(sel), ctypes.byref(nsel))
+    assert rc == 0, rc
+    return dict(gftt=gftt, nms=nms, cell_max=cmax[:cw * ch].reshape(ch, cw), cell_idx=cidx[:2 * cw * ch].reshape(ch, cw, 2),
+                kp=kp[:3 * nkp.value].reshape(-1, 3), bins=bins, sel=sel[:2 * nsel.value].reshape(-1, 2))
+
+
+def ref_lk(lib, prev, nxt, tracks, max_levels=10, horizontal=False):
+    h, w = prev.shape
+    t = np.ascontiguousarray(tracks.copy())
+    rc = lib.ref_lk(_ptr(np.ascontiguousarray(prev)), _ptr(np.ascontiguousarray(nxt)), w, h, max_levels, _ptr(t),
+                    len(t), int(horizontal))
+    assert rc == 0, rc
+    return t
+
+
+def ref_tex_probe(lib, img, xy):
+    h, w = img.shape
+    out = np.zeros(len(xy), np.float32)
+    rc = lib.ref_tex_probe(_ptr(np.ascontiguousarray(img, np.float32)), w, h, _ptr(np.ascontiguousarray(xy, np.float32)),
+                           len(xy), _ptr(out))
+    assert rc == 0, rc
+    return out
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def tex_probe_inputs():
+    rng = np.random.default_rng(99)
+    img = rng.uniform(-300.0, 300.0, (40, 48)).astype(np.float32)
+    # 1) fractional sweep across one texel step of a 0/1 image reveals the weight quantisation
+    step = np.zeros((40, 48), np.float32)
+    step[:, 25:] = 1.0
+    fr = (np.arange(8192, dtype=np.float64) / 8192.0)
+    sweep = np.stack([24.5 + fr, np.full_like(fr, 10.5)], 1).astype(np.float32)
+    # 2) random sub-texel coordinates on a random image, including clamped edges
+    xy = np.stack([rng.uniform(-1.0, 49.0, 20000), rng.uniform(-1.0, 41.0, 20000)], 1).astype(np.float32)
+    return img, step, sweep, xy
+
+
+def make_reference(out_dir):
+    lib = _lib()
+    inp = np.load(os.path.join(HERE, "inputs.npz"))
+    compact, full = {}, {}
+    for name in CASES:
+        prev, nxt = inp[f"{name}/prev"], inp[f"{name}/next"]
+        for tag, img in (("prev", prev), ("next", nxt)):
+            for l, (lv, gx, gy) in enumerate(ref_pyramid(lib, img)):
+                for q, arr in (("img", lv), ("gx", gx), ("gy", gy)):
+                    compact[f"{name}/{tag}/L{l}/{q}/sha"] = np.array(_sha(arr))
+                    full[f"{name}/{tag}/L{l}/{q}"] = arr
+        # 4-level pyramids (BASELINE config 1 caps levels at 4)
+        for l, (lv, gx, gy) in enumerate(ref_pyramid(lib, prev, 4)):
+            compact[f"{name}/prev4/L{l}/img/sha"] = np.array(_sha(lv))
+        h, w = prev.shape
+        s1 = ref_select(lib, prev, np.zeros((0, 2), np.float32), 450)
+        alive = s1["sel"][::2].copy()
+        s2 = ref_select(lib, prev, alive, 450 - len(alive), borders=(3, 4, 5, 6))
+        for tag, s in (("sel0", s1), ("sel1", s2)):
+            compact[f"{name}/{tag}/kp"] = s["kp"]
+            compact[f"{name}/{tag}/sel"] = s["sel"]
+            compact[f"{name}/{tag}/bins"] = s["bins"]
+            compact[f"{name}/{tag}/gftt/sha"] = np.array(_sha(s["gftt"]))
+            compact[f"{name}/{tag}/nms/sha"] = np.array(_sha(s["nms"]))
+            for k, v in s.items():
+                full[f"{name}/{tag}/{k}"] = v
+        compact[f"{name}/sel1/alive"] = alive
+        pts = s1["sel"]
+        if len(pts) == 0:
+            continue
+        wp = inp[f"{name}/warp"]
+        warp = synthetic.Similarity(*[float(v) for v in wp])
+        gt = synthetic.flow_texture(warp, pts.astype(np.float64)).astype(np.float32)
+        rng = np.random.default_rng(5)
+        pred = gt + rng.normal(0.0, 0.7, gt.shape).astype(np.float32)
+        runs = {
+            "lk_zero": make_tracks(pts, None, float(w), 0.8),
+            "lk_pred": make_tracks(pts, pred - pts, float(w), 0.8),
+            "lk_retrack": make_tracks(pts, None, float(w), 0.85),
+        }
+        for tag, t in runs.items():
+            out = ref_lk(lib, prev, nxt, t)
+            compact[f"{name}/{tag}/in"] = t
+            compact[f"{name}/{tag}/out"] = out
+        out4 = ref_lk(lib, prev, nxt, runs["lk_pred"], max_levels=4)
+        compact[f"{name}/lk_pred4/out"] = out4
+        outh = ref_lk(lib, prev, nxt, runs["lk_zero"], horizontal=True)
+        compact[f"{name}/lk_horiz/out"] = outh
+        compact[f"{name}/gt"] = gt
+    img, step, sweep, xy = tex_probe_inputs()
+    compact["tex/sweep"] = ref_tex_probe(lib, step, sweep)
+    compact["tex/random"] = ref_tex_probe(lib, img, xy)
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "reference.npz"), **compact)
+    np.savez_compressed(os.path.join(out_dir, "reference_full.npz"), **full)
+    print("wrote", out_dir)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("step", choices=["inputs", "reference"])
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    if a.step == "inputs":
+        make_inputs(os.path.join(HERE, "inputs.npz"))
+    else:
+        make_reference(a.out)
