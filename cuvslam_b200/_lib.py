@@ -1,0 +1,102 @@
+"""ctypes binding of libcuvslam_fe.so (the C ABI declared in include/cuvslam_fe.h).
+
+The shared library is built in-tree by cuvslam_b200/csrc/Makefile (see cuvslam_b200.build).
+There is no fallback: if the library is missing or fails to load, importing the front-end raises.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcuvslam_fe.so")
+MAX_LEVELS = 10
+
+FE_OK = 0
+FE_SAMPLE_TEXTURE = 0
+FE_SAMPLE_EXACT = 1
+
+
+class FePyramid(ctypes.Structure):
+    _fields_ = [
+        ("levels", ctypes.c_int32),
+        ("width", ctypes.c_int32 * MAX_LEVELS),
+        ("height", ctypes.c_int32 * MAX_LEVELS),
+        ("pitch_bytes", ctypes.c_int64 * MAX_LEVELS),
+        ("image", ctypes.c_void_p * MAX_LEVELS),
+        ("grad_x", ctypes.c_void_p * MAX_LEVELS),
+        ("grad_y", ctypes.c_void_p * MAX_LEVELS),
+    ]
+
+
+class FeCameraFrame(ctypes.Structure):
+    _fields_ = [
+        ("image", ctypes.c_void_p),
+        ("image_pitch_bytes", ctypes.c_int64),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("prev", ctypes.POINTER(FePyramid)),
+        ("cur", ctypes.POINTER(FePyramid)),
+        ("tracks", ctypes.c_void_p),
+        ("n_tracks", ctypes.c_int32),
+        ("num_desired", ctypes.c_int32),
+        ("new_xy", ctypes.c_void_p),
+        ("new_count", ctypes.c_void_p),
+        ("border", ctypes.c_int32 * 4),
+    ]
+
+
+class FeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_SIGS = {
+    "fe_abi_version": (_I, []),
+    "fe_status_string": (ctypes.c_char_p, [_I]),
+    "fe_last_cuda_error": (_I, []),
+    "fe_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "fe_destroy": (_I, [_P]),
+    "fe_pyramid_levels": (_I, [_I, _I, _I]),
+    "fe_pyramid_bytes": (_I64, [_I, _I, _I]),
+    "fe_pyramid_init": (_I, [_P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid)]),
+    "fe_build_pyramid": (_I, [_P, _P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid), _P]),
+    "fe_build_pyramid_f32": (_I, [_P, _P, _I64, _I, _I, ctypes.POINTER(FePyramid), _P]),
+    "fe_select": (_I, [_P, ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
+    "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
+    "fe_track": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _P]),
+    "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),
+    "fe_batch_run": (_I, [_P, _P]),
+    "fe_batch_run_plain": (_I, [_P, _P]),
+    "fe_batch_run_part": (_I, [_P, _I, _P]),
+    "fe_batch_kernel_count": (_I, [_P]),
+    "fe_batch_destroy": (_I, [_P]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+
+def load():
+    """Loads libcuvslam_fe.so; raises if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -c 'import cuvslam_b200.build as b; b.build()'`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(rc, what=""):
+    if rc != FE_OK:
+        lib = load()
+        msg = lib.fe_status_string(rc).decode()
+        raise FeError(f"{what}: {msg} (status {rc}, cuda error {lib.fe_last_cuda_error()})")

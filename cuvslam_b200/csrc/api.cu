@@ -1,0 +1,726 @@
+// C ABI of the front-end (include/cuvslam_fe.h): argument checking, scratch management, launch
+// planning for single cameras and batches, and CUDA-graph capture of batched frame steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cuvslam_fe.h"
+#include "fe_common.cuh"
+#include "fe_internal.h"
+
+static_assert(sizeof(fe_track_data) == 80, "fe_track_data must match cuvslam::cuda::TrackData");
+static_assert(offsetof(fe_track_data, track_status) == 32, "TrackData layout");
+static_assert(offsetof(fe_track_data, initial_guess_map) == 48, "TrackData layout");
+static_assert(offsetof(fe_track_data, search_radius_px) == 64, "TrackData layout");
+static_assert(offsetof(fe_track_data, ncc) == 72, "TrackData layout");
+
+namespace {
+
+thread_local int g_last_cuda_error = 0;
+
+int cuda_fail(cudaError_t e) {
+  g_last_cuda_error = (int)e;
+  return e == cudaErrorMemoryAllocation ? FE_ERR_OUT_OF_MEMORY : FE_ERR_CUDA;
+}
+
+#define FE_CUDA(x)                                  \
+  do {                                              \
+    cudaError_t e_ = (x);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_);    \
+  } while (0)
+
+constexpr int64_t kAlign = 256;
+int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+int next_pow2(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+int level_sizes(int w, int h, int max_levels, int* ws, int* hs) {
+  if (w <= 0 || h <= 0 || max_levels <= 0) return 0;
+  max_levels = std::min(max_levels, FE_MAX_LEVELS);
+  int n = 0;
+  while (n < max_levels) {
+    ws[n] = w;
+    hs[n] = h;
+    ++n;
+    w = (w + 1) / 2;
+    h = (h + 1) / 2;
+    if (w < fe::kMinLevelDim || h < fe::kMinLevelDim) break;
+  }
+  return n;
+}
+
+bool valid_pyramid(const fe_pyramid* p) {
+  if (!p || p->levels <= 0 || p->levels > FE_MAX_LEVELS) return false;
+  for (int l = 0; l < p->levels; ++l) {
+    if (!p->image[l] || !p->grad_x[l] || p->width[l] <= 0 || p->height[l] <= 0) return false;
+    if (p->pitch_bytes[l] % 16 != 0 || p->pitch_bytes[l] < (int64_t)p->width[l] * 4) return false;
+    if (l > 0 && (p->width[l] != (p->width[l - 1] + 1) / 2 || p->height[l] != (p->height[l - 1] + 1) / 2)) return false;
+  }
+  return true;
+}
+
+fe::Pyr to_pyr(const fe_pyramid& p) {
+  fe::Pyr r;
+  memset(&r, 0, sizeof(r));
+  r.levels = p.levels;
+  for (int l = 0; l < p.levels; ++l) {
+    r.lv[l].img = p.image[l];
+    r.lv[l].gx = p.grad_x[l];
+    r.lv[l].gy = p.grad_y[l];
+    r.lv[l].w = p.width[l];
+    r.lv[l].h = p.height[l];
+    r.lv[l].pitch = (int)(p.pitch_bytes[l] / 4);
+  }
+  return r;
+}
+
+// ------------------------------------------------------------------ pyramid planning
+// Launches of one stage index that share the source kind and the number of produced levels.
+struct StageGroup {
+  bool u8;
+  int nl;
+  int tiles;
+  fe::StageBatch batch;
+};
+using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
+
+// Appends the stages of one camera's pyramid build: stage 0 reads the frame (uint8 or FP32) and
+// writes levels 0..2; each later stage reads the deepest level of the previous one and writes up
+// to two more.
+int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan) {
+  const fe::Pyr pyr = to_pyr(p);
+  const int T = fe::stage_tile();
+  int s = 0;
+  for (int stage = 0;; ++stage) {
+    const int nl = std::min(2, pyr.levels - 1 - s);
+    if (stage > 0 && nl <= 0) break;
+    fe::StageJob job;
+    memset(&job, 0, sizeof(job));
+    job.src = stage == 0 ? src : (const void*)pyr.lv[s].img;
+    job.src_pitch_bytes = stage == 0 ? src_pitch : (int64_t)pyr.lv[s].pitch * 4;
+    job.write_level0 = stage == 0 ? 1 : 0;
+    job.src_w = pyr.lv[s].w;
+    job.src_h = pyr.lv[s].h;
+    for (int k = 0; k <= nl; ++k) job.out[k] = pyr.lv[s + k];
+    const fe::Level& deep = pyr.lv[s + nl];
+    job.tiles_x = (deep.w + T - 1) / T;
+    job.tiles_y = (deep.h + T - 1) / T;
+    const bool kind_u8 = stage == 0 && u8;
+    if ((int)plan.size() <= stage) plan.resize(stage + 1);
+    StageGroup* g = nullptr;
+    for (auto& gg : plan[stage])
+      if (gg.u8 == kind_u8 && gg.nl == nl) g = &gg;
+    if (!g) {
+      plan[stage].emplace_back();
+      g = &plan[stage].back();
+      memset(&g->batch, 0, sizeof(g->batch));
+      g->u8 = kind_u8;
+      g->nl = nl;
+      g->tiles = 0;
+    }
+    if (g->batch.njobs >= fe::kMaxCams) return FE_ERR_CAPACITY;
+    job.tile_begin = g->tiles;
+    g->batch.job[g->batch.njobs++] = job;
+    g->tiles += job.tiles_x * job.tiles_y;
+    if (nl <= 0) break;
+    s += nl;
+  }
+  return FE_OK;
+}
+
+int run_plan(const StagePlan& plan, cudaStream_t st) {
+  for (const auto& stage : plan)
+    for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, st));
+  return FE_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ context
+struct SelectScratch {
+  int w = 0, h = 0, n_alive_cap = 0, q_cap = 0;
+  void* mem = nullptr;
+  size_t bytes = 0;
+  float* resp = nullptr;  // debug maps, allocated on demand
+  float* nms = nullptr;
+  uint32_t* burn = nullptr;
+  float* cell_m = nullptr;
+  float2* cell_xy = nullptr;
+  float* sub_sum = nullptr;
+  int* bin_want = nullptr;
+  int* stats = nullptr;
+  uint64_t* q_keys = nullptr;
+  float* alive_xy = nullptr;
+  size_t burn_bytes = 0, zero_bytes = 0;  // bytes to clear per run (burn + stats)
+};
+
+struct fe_context {
+  int device = 0;
+  SelectScratch sel;
+  bool debug = false;
+};
+
+namespace {
+
+struct ScratchLayout {
+  size_t burn, cell_m, cell_xy, sub_sum, bin_want, stats, q_keys, alive, total, burn_bytes;
+};
+
+ScratchLayout scratch_layout(int w, int h, int n_alive_cap, int q_cap) {
+  ScratchLayout L;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = (size_t)align_up((int64_t)(o + bytes), kAlign);
+    return at;
+  };
+  const size_t words = (size_t)((w + 31) / 32) * h;
+  const size_t cells = (size_t)(w / 8) * (h / 8);
+  const size_t subs = (size_t)((w + 15) / 16) * ((h + 15) / 16);
+  L.stats = take(16 * sizeof(int));  // first so one memset clears stats + burn
+  L.burn = take(words * 4);
+  L.burn_bytes = L.burn + words * 4;
+  L.cell_m = take(std::max<size_t>(cells, 1) * 4);
+  L.cell_xy = take(std::max<size_t>(cells, 1) * 8);
+  L.sub_sum = take(subs * 4);
+  L.bin_want = take(128 * 4);
+  L.q_keys = take((size_t)std::max(q_cap, 1) * 8);
+  L.alive = take((size_t)std::max(n_alive_cap, 1) * 8);
+  L.total = o;
+  return L;
+}
+
+// Shared-memory key capacities of bin_kernel (largest candidate-cell rectangle of a bin) and
+// final_kernel (kept candidates), and the kept-candidate buffer size.
+int sel_caps(int w, int h, int n_alive, int num_desired, int* bin_key_cap, int* final_key_cap, int* q_cap) {
+  const int cw = w / 8, ch = h / 8, bw = w / 8, bh = h / 8;
+  int mx = 1;
+  if (bw > 0 && bh > 0) {
+    int mxx = 1, mxy = 1;
+    for (int b = 0; b < 8; ++b) {
+      mxx = std::max(mxx, std::min(((b + 1) * bw) / 8, cw - 1) - std::max((b * bw - 1) / 8, 0) + 1);
+      mxy = std::max(mxy, std::min(((b + 1) * bh) / 8, ch - 1) - std::max((b * bh - 1) / 8, 0) + 1);
+    }
+    mx = mxx * mxy;
+  }
+  *bin_key_cap = next_pow2(mx);
+  const int cells = std::max(cw * ch, 1);
+  *q_cap = std::min(cells, std::max(n_alive, 0) + num_desired + 64);
+  *final_key_cap = next_pow2(*q_cap);
+  if (*bin_key_cap > 16384 || *final_key_cap > 16384) return FE_ERR_CAPACITY;
+  return FE_OK;
+}
+
+int ensure_select_scratch(fe_context* ctx, int w, int h, int n_alive_cap, int q_cap) {
+  SelectScratch& s = ctx->sel;
+  if (s.mem && s.w == w && s.h == h && s.n_alive_cap >= n_alive_cap && s.q_cap >= q_cap) return FE_OK;
+  const int na = std::max(n_alive_cap, s.w == w && s.h == h ? s.n_alive_cap : 0);
+  const int qc = std::max(q_cap, s.w == w && s.h == h ? s.q_cap : 0);
+  ScratchLayout L = scratch_layout(w, h, na, qc);
+  if (s.mem) cudaFree(s.mem);
+  s.mem = nullptr;
+  FE_CUDA(cudaMalloc(&s.mem, L.total));
+  char* base = (char*)s.mem;
+  s.w = w;
+  s.h = h;
+  s.n_alive_cap = na;
+  s.q_cap = qc;
+  s.bytes = L.total;
+  s.stats = (int*)(base + L.stats);
+  s.burn = (uint32_t*)(base + L.burn);
+  s.cell_m = (float*)(base + L.cell_m);
+  s.cell_xy = (float2*)(base + L.cell_xy);
+  s.sub_sum = (float*)(base + L.sub_sum);
+  s.bin_want = (int*)(base + L.bin_want);
+  s.q_keys = (uint64_t*)(base + L.q_keys);
+  s.alive_xy = (float*)(base + L.alive);
+  s.zero_bytes = L.burn_bytes;
+  if (s.resp) cudaFree(s.resp);
+  if (s.nms) cudaFree(s.nms);
+  s.resp = s.nms = nullptr;
+  return FE_OK;
+}
+
+void fill_select_cam(fe::SelectCam& c, const SelectScratch& s, const fe_pyramid& p, int q_cap) {
+  memset(&c, 0, sizeof(c));
+  c.gx = p.grad_x[0];
+  c.gy = p.grad_y[0];
+  c.w = p.width[0];
+  c.h = p.height[0];
+  c.pitch = (int)(p.pitch_bytes[0] / 4);
+  c.resp = s.resp;
+  c.nms = s.nms;
+  c.burn = s.burn;
+  c.cell_m = s.cell_m;
+  c.cell_xy = s.cell_xy;
+  c.sub_sum = s.sub_sum;
+  c.bin_want = s.bin_want;
+  c.stats = s.stats;
+  c.q_keys = s.q_keys;
+  c.q_cap = q_cap;
+  const int T = fe::select_tile();
+  c.tiles_x = (c.w + T - 1) / T;
+  c.tiles_y = (c.h + T - 1) / T;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fe_abi_version(void) { return FE_ABI_VERSION; }
+
+const char* fe_status_string(int status) {
+  switch (status) {
+    case FE_OK: return "ok";
+    case FE_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FE_ERR_CUDA: return "CUDA error";
+    case FE_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case FE_ERR_CAPACITY: return "size limit exceeded";
+    case FE_ERR_DEVICE_FAULT: return "device-side error flag";
+    default: return "unknown status";
+  }
+}
+
+int fe_last_cuda_error(void) { return g_last_cuda_error; }
+
+int fe_create(int device, fe_context** out) {
+  if (!out) return FE_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  FE_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return FE_ERR_INVALID_ARGUMENT;
+  FE_CUDA(cudaSetDevice(device));
+  FE_CUDA(fe::pyramid_init());
+  FE_CUDA(fe::select_init());
+  fe_context* c = new (std::nothrow) fe_context;
+  if (!c) return FE_ERR_OUT_OF_MEMORY;
+  c->device = device;
+  c->debug = getenv("CUVSLAM_FE_DEBUG_MAPS") != nullptr;
+  *out = c;
+  return FE_OK;
+}
+
+int fe_destroy(fe_context* ctx) {
+  if (!ctx) return FE_ERR_INVALID_ARGUMENT;
+  if (ctx->sel.mem) cudaFree(ctx->sel.mem);
+  if (ctx->sel.resp) cudaFree(ctx->sel.resp);
+  if (ctx->sel.nms) cudaFree(ctx->sel.nms);
+  delete ctx;
+  return FE_OK;
+}
+
+int fe_pyramid_levels(int width, int height, int max_levels) {
+  int ws[FE_MAX_LEVELS], hs[FE_MAX_LEVELS];
+  return level_sizes(width, height, max_levels, ws, hs);
+}
+
+int64_t fe_pyramid_bytes(int width, int height, int max_levels) {
+  int ws[FE_MAX_LEVELS], hs[FE_MAX_LEVELS];
+  const int n = level_sizes(width, height, max_levels, ws, hs);
+  int64_t total = 0;
+  for (int l = 0; l < n; ++l) total += 3 * align_up(align_up((int64_t)ws[l] * 4, kAlign) * hs[l], kAlign);
+  return total;
+}
+
+int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int height, int max_levels, fe_pyramid* out) {
+  if (!device_memory || !out || ((uintptr_t)device_memory % kAlign) != 0) return FE_ERR_INVALID_ARGUMENT;
+  int ws[FE_MAX_LEVELS], hs[FE_MAX_LEVELS];
+  const int n = level_sizes(width, height, max_levels, ws, hs);
+  if (n == 0) return FE_ERR_INVALID_ARGUMENT;
+  if (bytes < fe_pyramid_bytes(width, height, max_levels)) return FE_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->levels = n;
+  char* p = (char*)device_memory;
+  for (int l = 0; l < n; ++l) {
+    const int64_t pitch = align_up((int64_t)ws[l] * 4, kAlign);
+    const int64_t plane = align_up(pitch * hs[l], kAlign);
+    out->width[l] = ws[l];
+    out->height[l] = hs[l];
+    out->pitch_bytes[l] = pitch;
+    out->image[l] = (float*)p;
+    out->grad_x[l] = (float*)(p + plane);
+    out->grad_y[l] = (float*)(p + 2 * plane);
+    p += 3 * plane;
+  }
+  return FE_OK;
+}
+
+int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
+                     int box3, const fe_pyramid* pyr, fe_stream stream) {
+  if (!ctx || !image || !valid_pyramid(pyr) || box3 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (pyr->width[0] != width || pyr->height[0] != height || image_pitch_bytes < width) return FE_ERR_INVALID_ARGUMENT;
+  if (!pyr->grad_y[0]) return FE_ERR_INVALID_ARGUMENT;
+  StagePlan plan;
+  int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan);
+  if (rc) return rc;
+  return run_plan(plan, (cudaStream_t)stream);
+}
+
+int fe_build_pyramid_f32(fe_context* ctx, const float* image, int64_t image_pitch_bytes, int width, int height,
+                         const fe_pyramid* pyr, fe_stream stream) {
+  if (!ctx || !image || !valid_pyramid(pyr)) return FE_ERR_INVALID_ARGUMENT;
+  if (pyr->width[0] != width || pyr->height[0] != height || image_pitch_bytes < (int64_t)width * 4 ||
+      image_pitch_bytes % 4 != 0)
+    return FE_ERR_INVALID_ARGUMENT;
+  StagePlan plan;
+  int rc = plan_pyramid(image, image_pitch_bytes, false, *pyr, plan);
+  if (rc) return rc;
+  return run_plan(plan, (cudaStream_t)stream);
+}
+
+int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int border_bottom, int border_left,
+              int border_right, const uint8_t* mask, int64_t mask_pitch_bytes, const float* alive_xy, int n_alive,
+              int num_desired, float* out_xy, int32_t* out_count, fe_stream stream) {
+  if (!ctx || !valid_pyramid(pyr) || !pyr->grad_y[0] || !out_count || n_alive < 0 || num_desired < 0)
+    return FE_ERR_INVALID_ARGUMENT;
+  if ((n_alive > 0 && !alive_xy) || (num_desired > 0 && !out_xy)) return FE_ERR_INVALID_ARGUMENT;
+  const int w = pyr->width[0], h = pyr->height[0];
+  if (w > 4096 || h > 4096 || num_desired > 16384) return FE_ERR_CAPACITY;
+  if (mask && mask_pitch_bytes < w) return FE_ERR_INVALID_ARGUMENT;
+  int bin_cap, final_cap, q_cap;
+  int rc = sel_caps(w, h, n_alive, num_desired, &bin_cap, &final_cap, &q_cap);
+  if (rc) return rc;
+  rc = ensure_select_scratch(ctx, w, h, 0, q_cap);
+  if (rc) return rc;
+  SelectScratch& s = ctx->sel;
+  if (ctx->debug && !s.resp) {
+    FE_CUDA(cudaMalloc((void**)&s.resp, (size_t)w * h * 4));
+    FE_CUDA(cudaMalloc((void**)&s.nms, (size_t)w * h * 4));
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  FE_CUDA(cudaMemsetAsync(s.mem, 0, s.zero_bytes, st));
+  static thread_local fe::SelectBatch b;  // large: keep off the stack
+  memset(&b, 0, sizeof(b));
+  b.ncams = 1;
+  b.debug = ctx->debug ? 1 : 0;
+  fe::SelectCam& c = b.cam[0];
+  fill_select_cam(c, s, *pyr, q_cap);
+  c.mask = mask;
+  c.mask_pitch = mask_pitch_bytes;
+  c.alive_xy = alive_xy;
+  c.n_alive = n_alive;
+  c.num_desired = num_desired;
+  c.border[0] = border_top;
+  c.border[1] = border_bottom;
+  c.border[2] = border_left;
+  c.border[3] = border_right;
+  c.out_xy = out_xy;
+  c.out_count = out_count;
+  c.tile_begin = 0;
+  FE_CUDA(fe::launch_select(b, c.tiles_x * c.tiles_y, bin_cap, final_cap, st));
+  return FE_OK;
+}
+
+int fe_select_debug(fe_context* ctx, const float** response, const float** nms) {
+  if (!ctx || !response || !nms) return FE_ERR_INVALID_ARGUMENT;
+  *response = ctx->sel.resp;
+  *nms = ctx->sel.nms;
+  return ctx->debug ? FE_OK : FE_ERR_INVALID_ARGUMENT;
+}
+
+int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks, int n,
+             int horizontal, int sampling, fe_stream stream) {
+  if (!ctx || !valid_pyramid(prev) || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
+  if (cur->levels < prev->levels) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  if (!horizontal)
+    for (int l = 0; l < prev->levels; ++l)
+      if (!prev->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
+  if ((uintptr_t)tracks % 16 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FE_OK;
+  fe::LkLaunch p;
+  memset(&p, 0, sizeof(p));
+  p.cams = nullptr;
+  p.ncams = 1;
+  p.total = n;
+  p.horizontal = horizontal ? 1 : 0;
+  p.sampling = sampling;
+  p.single.prev = to_pyr(*prev);
+  p.single.cur = to_pyr(*cur);
+  p.single.tracks = tracks;
+  p.single.n = n;
+  p.single.begin = 0;
+  FE_CUDA(fe::launch_lk(p, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batched frame step
+struct fe_batch {
+  fe_context* ctx = nullptr;
+  int ncams = 0;
+  int sampling = FE_SAMPLE_TEXTURE;
+  std::vector<fe_camera_frame> cams;
+  std::vector<fe_pyramid> prev, cur;
+  std::vector<char> has_prev;
+  StagePlan plan;
+  fe::LkCam* d_lk = nullptr;
+  fe::LkLaunch lk;
+  fe::SelectBatch* sel = nullptr;  // heap: large
+  int sel_tiles = 0, bin_cap = 1, final_cap = 1;
+  void* sel_mem = nullptr;
+  size_t zero_bytes = 0;
+  bool any_select = false;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int enqueue_batch(fe_batch* b, cudaStream_t st) {
+  int rc = run_plan(b->plan, st);
+  if (rc) return rc;
+  if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
+  if (b->any_select) {
+    FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
+    FE_CUDA(fe::launch_select(*b->sel, b->sel_tiles, b->bin_cap, b->final_cap, st));
+  }
+  return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int sampling, fe_batch** out) {
+  if (!ctx || !cams || !out || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
+  if (ncams > fe::kMaxCams) return FE_ERR_CAPACITY;
+  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  fe_batch* b = new (std::nothrow) fe_batch;
+  if (!b) return FE_ERR_OUT_OF_MEMORY;
+  b->ctx = ctx;
+  b->ncams = ncams;
+  b->sampling = sampling;
+  b->cams.assign(cams, cams + ncams);
+  b->prev.resize(ncams);
+  b->cur.resize(ncams);
+  b->has_prev.assign(ncams, 0);
+  b->sel = new (std::nothrow) fe::SelectBatch;
+  if (!b->sel) {
+    delete b;
+    return FE_ERR_OUT_OF_MEMORY;
+  }
+  memset(b->sel, 0, sizeof(*b->sel));
+  auto fail = [&](int rc) {
+    fe_batch_destroy(b);
+    return rc;
+  };
+  // validate and copy descriptors; plan the pyramid stages
+  std::vector<fe::LkCam> lk;
+  int total = 0;
+  for (int i = 0; i < ncams; ++i) {
+    const fe_camera_frame& c = cams[i];
+    if (!c.image || !valid_pyramid(c.cur) || !c.cur->grad_y[0] || c.cur->width[0] != c.width ||
+        c.cur->height[0] != c.height || c.image_pitch_bytes < c.width || c.n_tracks < 0 || c.num_desired < 0)
+      return fail(FE_ERR_INVALID_ARGUMENT);
+    b->cur[i] = *c.cur;
+    int rc = plan_pyramid(c.image, c.image_pitch_bytes, true, b->cur[i], b->plan);
+    if (rc) return fail(rc);
+    if (c.prev && c.n_tracks > 0) {
+      if (!valid_pyramid(c.prev) || !c.tracks || c.cur->levels < c.prev->levels || (uintptr_t)c.tracks % 16)
+        return fail(FE_ERR_INVALID_ARGUMENT);
+      b->prev[i] = *c.prev;
+      b->has_prev[i] = 1;
+      fe::LkCam lc;
+      memset(&lc, 0, sizeof(lc));
+      lc.prev = to_pyr(b->prev[i]);
+      lc.cur = to_pyr(b->cur[i]);
+      lc.tracks = c.tracks;
+      lc.n = c.n_tracks;
+      lc.begin = total;
+      total += c.n_tracks;
+      lk.push_back(lc);
+    }
+  }
+  memset(&b->lk, 0, sizeof(b->lk));
+  if (!lk.empty()) {
+    cudaError_t e = cudaMalloc((void**)&b->d_lk, sizeof(fe::LkCam) * lk.size());
+    if (e != cudaSuccess) return fail(cuda_fail(e));
+    e = cudaMemcpy(b->d_lk, lk.data(), sizeof(fe::LkCam) * lk.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_fail(e));
+    b->lk.cams = b->d_lk;
+    b->lk.ncams = (int)lk.size();
+    b->lk.total = total;
+    b->lk.horizontal = 0;
+    b->lk.sampling = sampling;
+  }
+  // selection scratch: all cameras' [stats | burn] regions first (one memset), then the rest
+  std::vector<ScratchLayout> lay(ncams);
+  size_t zero = 0, rest = 0;
+  std::vector<int> qcaps(ncams);
+  for (int i = 0; i < ncams; ++i) {
+    const fe_camera_frame& c = cams[i];
+    if (c.num_desired <= 0) continue;
+    if (!c.new_xy || !c.new_count) return fail(FE_ERR_INVALID_ARGUMENT);
+    if (c.width > 4096 || c.height > 4096 || c.num_desired > 16384) return fail(FE_ERR_CAPACITY);
+    int bc, fc, qc;
+    const int n_alive = b->has_prev[i] ? c.n_tracks : 0;
+    int rc = sel_caps(c.width, c.height, n_alive, c.num_desired, &bc, &fc, &qc);
+    if (rc) return fail(rc);
+    b->bin_cap = std::max(b->bin_cap, bc);
+    b->final_cap = std::max(b->final_cap, fc);
+    qcaps[i] = qc;
+    lay[i] = scratch_layout(c.width, c.height, 0, qc);
+    zero += (size_t)align_up((int64_t)lay[i].burn_bytes, kAlign);
+    rest += lay[i].total - lay[i].cell_m;
+    b->any_select = true;
+  }
+  if (b->any_select) {
+    cudaError_t e = cudaMalloc(&b->sel_mem, zero + rest);
+    if (e != cudaSuccess) return fail(cuda_fail(e));
+    b->zero_bytes = zero;
+    char* zp = (char*)b->sel_mem;
+    char* rp = (char*)b->sel_mem + zero;
+    fe::SelectBatch& sb = *b->sel;
+    sb.ncams = 0;
+    sb.debug = 0;
+    for (int i = 0; i < ncams; ++i) {
+      const fe_camera_frame& c = cams[i];
+      if (c.num_desired <= 0) continue;
+      const ScratchLayout& L = lay[i];
+      SelectScratch s;
+      s.stats = (int*)(zp + L.stats);
+      s.burn = (uint32_t*)(zp + L.burn);
+      zp += align_up((int64_t)L.burn_bytes, kAlign);
+      s.cell_m = (float*)(rp + (L.cell_m - L.cell_m));
+      s.cell_xy = (float2*)(rp + (L.cell_xy - L.cell_m));
+      s.sub_sum = (float*)(rp + (L.sub_sum - L.cell_m));
+      s.bin_want = (int*)(rp + (L.bin_want - L.cell_m));
+      s.q_keys = (uint64_t*)(rp + (L.q_keys - L.cell_m));
+      rp += L.total - L.cell_m;
+      fe::SelectCam& sc = sb.cam[sb.ncams++];
+      fill_select_cam(sc, s, b->cur[i], qcaps[i]);
+      sc.alive_tracks = b->has_prev[i] ? c.tracks : nullptr;
+      sc.n_alive = b->has_prev[i] ? c.n_tracks : 0;
+      sc.num_desired = c.num_desired;
+      sc.target_total = c.num_desired;
+      for (int k = 0; k < 4; ++k) sc.border[k] = c.border[k];
+      sc.out_xy = c.new_xy;
+      sc.out_count = c.new_count;
+      sc.tile_begin = b->sel_tiles;
+      b->sel_tiles += sc.tiles_x * sc.tiles_y;
+    }
+  }
+  // capture the step into a graph
+  cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  int rc = enqueue_batch(b, b->cap_stream);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->cap_stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return fail(rc);
+  }
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  *out = b;
+  return FE_OK;
+}
+
+int fe_batch_run(fe_batch* b, fe_stream stream) {
+  if (!b || !b->exec) return FE_ERR_INVALID_ARGUMENT;
+  FE_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_batch_run_part(fe_batch* b, int part, fe_stream stream) {
+  if (!b) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (part) {
+    case FE_PART_PYRAMID:
+      return run_plan(b->plan, st);
+    case FE_PART_TRACK:
+      if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
+      return FE_OK;
+    case FE_PART_SELECT:
+      if (b->any_select) {
+        FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
+        FE_CUDA(fe::launch_select(*b->sel, b->sel_tiles, b->bin_cap, b->final_cap, st));
+      }
+      return FE_OK;
+    default:
+      return FE_ERR_INVALID_ARGUMENT;
+  }
+}
+
+int fe_batch_kernel_count(fe_batch* b) {
+  if (!b || !b->graph) return -1;
+  size_t n = 0;
+  if (cudaGraphGetNodes(b->graph, nullptr, &n) != cudaSuccess) return -1;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n && cudaGraphGetNodes(b->graph, nodes.data(), &n) != cudaSuccess) return -1;
+  int k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+int fe_batch_run_plain(fe_batch* b, fe_stream stream) {
+  if (!b) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  fe_context* ctx = b->ctx;
+  for (int i = 0; i < b->ncams; ++i) {
+    const fe_camera_frame& c = b->cams[i];
+    int rc = fe_build_pyramid(ctx, c.image, c.image_pitch_bytes, c.width, c.height, 0, &b->cur[i], stream);
+    if (rc) return rc;
+    if (b->has_prev[i]) {
+      rc = fe_track(ctx, &b->prev[i], &b->cur[i], c.tracks, c.n_tracks, 0, b->sampling, stream);
+      if (rc) return rc;
+    }
+    if (c.num_desired > 0) {
+      // same selection as the batch, one camera at a time on the context's scratch
+      int bc, fc, qc;
+      const int n_alive = b->has_prev[i] ? c.n_tracks : 0;
+      rc = sel_caps(c.width, c.height, n_alive, c.num_desired, &bc, &fc, &qc);
+      if (rc) return rc;
+      rc = ensure_select_scratch(ctx, c.width, c.height, 0, qc);
+      if (rc) return rc;
+      SelectScratch& s = ctx->sel;
+      FE_CUDA(cudaMemsetAsync(s.mem, 0, s.zero_bytes, st));
+      static thread_local fe::SelectBatch sb;
+      memset(&sb, 0, sizeof(sb));
+      sb.ncams = 1;
+      fe::SelectCam& sc = sb.cam[0];
+      fill_select_cam(sc, s, b->cur[i], qc);
+      sc.alive_tracks = b->has_prev[i] ? c.tracks : nullptr;
+      sc.n_alive = n_alive;
+      sc.num_desired = c.num_desired;
+      sc.target_total = c.num_desired;
+      for (int k = 0; k < 4; ++k) sc.border[k] = c.border[k];
+      sc.out_xy = c.new_xy;
+      sc.out_count = c.new_count;
+      FE_CUDA(fe::launch_select(sb, sc.tiles_x * sc.tiles_y, bc, fc, st));
+    }
+  }
+  return FE_OK;
+}
+
+int fe_batch_destroy(fe_batch* b) {
+  if (!b) return FE_ERR_INVALID_ARGUMENT;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->d_lk) cudaFree(b->d_lk);
+  if (b->sel_mem) cudaFree(b->sel_mem);
+  delete b->sel;
+  delete b;
+  return FE_OK;
+}
+
+}  // extern "C"

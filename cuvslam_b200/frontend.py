@@ -1,0 +1,271 @@
+"""Host-side mirror of the cuVSLAM GPU front-end interface over the C ABI.
+
+The classes keep the method names, argument meaning and error behaviour of the reference host
+wrappers that MonoSOFGPU calls (libs/cuda_modules):
+  ImagePyramid.build                         GaussianGPUImagePyramid::build (image_pyramid.h:81-98)
+                                             + GPUGradientPyramid::set (gradient_pyramid.cpp:83-118)
+  Selection.compute_gftt_and_select_features GPUSelection::computeGFTTAndSelectFeatures
+                                             (selection_v2.cpp:27-184)
+  LKFeatureTracker.track_points              GPULKFeatureTracker::track_points (lk_tracker.cpp:24-73)
+Device memory comes from PyTorch (plumbing only); every computation runs in libcuvslam_fe.so.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .types import TRACK_DTYPE
+
+
+def _stream_handle(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """Owns the library's per-device scratch (fe_create / fe_destroy)."""
+
+    def __init__(self, device=0):
+        self.lib = _lib.load()
+        self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+        torch.cuda.set_device(self.device)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.fe_create(self.device.index or 0, ctypes.byref(h)), "fe_create")
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.fe_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ImagePyramid:
+    """Image pyramid + gradient pyramid in one device buffer (fe_pyramid)."""
+
+    def __init__(self, width, height, max_levels=10, device="cuda"):
+        lib = _lib.load()
+        self.width, self.height = int(width), int(height)
+        nbytes = lib.fe_pyramid_bytes(self.width, self.height, max_levels)
+        if nbytes <= 0:
+            raise ValueError(f"bad pyramid size {width}x{height}")
+        self.storage = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        self.desc = _lib.FePyramid()
+        _lib.check(lib.fe_pyramid_init(_ptr(self.storage), nbytes, self.width, self.height, max_levels,
+                                       ctypes.byref(self.desc)), "fe_pyramid_init")
+        self._f32 = self.storage.view(torch.float32)
+
+    @property
+    def levels(self):
+        return self.desc.levels
+
+    def level_size(self, l):
+        return self.desc.width[l], self.desc.height[l]
+
+    def _plane(self, ptr, l):
+        off = (ptr - self.storage.data_ptr()) // 4
+        w, h = self.desc.width[l], self.desc.height[l]
+        return self._f32.as_strided((h, w), (self.desc.pitch_bytes[l] // 4, 1), off)
+
+    def image(self, l):
+        return self._plane(self.desc.image[l], l)
+
+    def grad_x(self, l):
+        return self._plane(self.desc.grad_x[l], l)
+
+    def grad_y(self, l):
+        return self._plane(self.desc.grad_y[l], l)
+
+    def build(self, ctx, image_u8, blur_filter=False, stream=None):
+        """Builds all levels and gradients from a (height, width) uint8 CUDA tensor."""
+        if blur_filter:
+            raise NotImplementedError("box3 prefilter is not part of this build")
+        img = image_u8
+        if img.dtype != torch.uint8 or img.dim() != 2 or not img.is_cuda:
+            raise ValueError("image must be a 2-D uint8 CUDA tensor")
+        if img.stride(1) != 1:
+            img = img.contiguous()
+        h, w = img.shape
+        _lib.check(ctx.lib.fe_build_pyramid(ctx.handle, _ptr(img), img.stride(0), w, h, 0, ctypes.byref(self.desc),
+                                            _stream_handle(stream)), "fe_build_pyramid")
+        return self
+
+    def build_f32(self, ctx, image_f32, stream=None):
+        img = image_f32
+        if img.dtype != torch.float32 or img.dim() != 2 or not img.is_cuda:
+            raise ValueError("image must be a 2-D float32 CUDA tensor")
+        if img.stride(1) != 1:
+            img = img.contiguous()
+        h, w = img.shape
+        _lib.check(ctx.lib.fe_build_pyramid_f32(ctx.handle, _ptr(img), img.stride(0) * 4, w, h,
+                                                ctypes.byref(self.desc), _stream_handle(stream)),
+                   "fe_build_pyramid_f32")
+        return self
+
+    def to_numpy(self):
+        """[(image, grad_x, grad_y)] per level as host arrays."""
+        return [(self.image(l).cpu().numpy(), self.grad_x(l).cpu().numpy(), self.grad_y(l).cpu().numpy())
+                for l in range(self.levels)]
+
+
+def tracks_to_device(tracks, device="cuda"):
+    """TRACK_DTYPE records -> (n, 80) uint8 CUDA tensor (the TrackData array the kernels update)."""
+    arr = np.ascontiguousarray(tracks, dtype=TRACK_DTYPE)
+    return torch.from_numpy(arr.view(np.uint8).reshape(len(arr), 80).copy()).to(device)
+
+
+def tracks_from_device(t):
+    return t.cpu().numpy().reshape(-1).view(TRACK_DTYPE).copy()
+
+
+class LKFeatureTracker:
+    """GPULKFeatureTracker (horizontal=False) / GPULKTrackerHorizontal (horizontal=True)."""
+
+    def __init__(self, ctx, horizontal=False, sampling=_lib.FE_SAMPLE_TEXTURE):
+        self.ctx = ctx
+        self.horizontal = bool(horizontal)
+        self.sampling = sampling
+
+    def track_points(self, previous_image_pyramid, current_image_pyramid, track_data, num_tracks=None,
+                     stream=None):
+        """Advances `track_data` ((n, 80) uint8 CUDA tensor of TrackData) in place; asynchronous."""
+        n = track_data.shape[0] if num_tracks is None else int(num_tracks)
+        if n == 0:
+            return True
+        if track_data.dtype != torch.uint8 or track_data.dim() != 2 or track_data.shape[1] != 80:
+            raise ValueError("track_data must be an (n, 80) uint8 tensor of TrackData records")
+        _lib.check(self.ctx.lib.fe_track(self.ctx.handle, ctypes.byref(previous_image_pyramid.desc),
+                                         ctypes.byref(current_image_pyramid.desc), _ptr(track_data), n,
+                                         int(self.horizontal), int(self.sampling), _stream_handle(stream)),
+                   "fe_track")
+        return True
+
+
+class Selection:
+    """GPUSelection: Shi-Tomasi response + deterministic feature selection on pyramid level 0."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self._count = torch.zeros(1, dtype=torch.int32, device=ctx.device)
+
+    def select_async(self, pyramid, border_top, border_bottom, border_left, border_right, mask, alive_features,
+                     num_desired, stream=None):
+        """Enqueues selection; returns (xy (num_desired, 2) tensor, count (1,) int32 tensor)."""
+        out = torch.empty((max(int(num_desired), 1), 2), dtype=torch.float32, device=self.ctx.device)
+        count = torch.zeros(1, dtype=torch.int32, device=self.ctx.device)
+        alive = None
+        n_alive = 0
+        if alive_features is not None and len(alive_features) > 0:
+            alive = torch.as_tensor(alive_features, dtype=torch.float32).reshape(-1, 2).to(self.ctx.device).contiguous()
+            n_alive = alive.shape[0]
+        m = None
+        if mask is not None:
+            m = torch.as_tensor(mask, dtype=torch.uint8).to(self.ctx.device).contiguous()
+        _lib.check(self.ctx.lib.fe_select(self.ctx.handle, ctypes.byref(pyramid.desc), int(border_top),
+                                          int(border_bottom), int(border_left), int(border_right),
+                                          None if m is None else _ptr(m), 0 if m is None else m.stride(0),
+                                          None if alive is None else _ptr(alive), n_alive, int(num_desired),
+                                          _ptr(out), _ptr(count), _stream_handle(stream)), "fe_select")
+        self._keep = (alive, m)
+        return out, count
+
+    def compute_gftt_and_select_features(self, pyramid, border_top, border_bottom, border_left, border_right,
+                                         input_mask, alive_features, num_desired_new_features, stream=None):
+        """Blocking form with the reference's signature: returns the new features as an (k, 2) tensor."""
+        out, count = self.select_async(pyramid, border_top, border_bottom, border_left, border_right, input_mask,
+                                       alive_features, num_desired_new_features, stream)
+        (stream or torch.cuda.current_stream()).synchronize()
+        return out[: int(count.item())]
+
+    def debug_maps(self, width, height):
+        """(response, nms) maps of the last selection as (height, width) float32 CUDA tensors; the
+        context must have been created with CUVSLAM_FE_DEBUG_MAPS set in the environment."""
+        r, n = ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(self.ctx.lib.fe_select_debug(self.ctx.handle, ctypes.byref(r), ctypes.byref(n)), "fe_select_debug")
+        return (torch.as_tensor(_DeviceArray(r.value, (height, width)), device=self.ctx.device),
+                torch.as_tensor(_DeviceArray(n.value, (height, width)), device=self.ctx.device))
+
+
+class _DeviceArray:
+    """A float32 device buffer owned by the library, exposed through __cuda_array_interface__."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), False),
+                                         "version": 2, "strides": None}
+
+
+class CameraFrame:
+    """One camera of a batched frame step (fe_camera_frame)."""
+
+    def __init__(self, image_u8, cur, prev=None, tracks=None, num_desired=0, border=(0, 0, 0, 0)):
+        self.image = image_u8.contiguous()
+        self.cur = cur
+        self.prev = prev
+        self.tracks = tracks
+        self.num_desired = int(num_desired)
+        self.border = tuple(int(b) for b in border)
+        dev = image_u8.device
+        self.new_xy = torch.zeros((max(self.num_desired, 1), 2), dtype=torch.float32, device=dev)
+        self.new_count = torch.zeros(1, dtype=torch.int32, device=dev)
+
+
+class Batch:
+    """Batched multi-camera frame step captured in a CUDA graph (fe_batch_*)."""
+
+    def __init__(self, ctx, frames, sampling=_lib.FE_SAMPLE_TEXTURE):
+        self.ctx = ctx
+        self.frames = list(frames)
+        arr = (_lib.FeCameraFrame * len(self.frames))()
+        for i, f in enumerate(self.frames):
+            a = arr[i]
+            a.image = f.image.data_ptr()
+            a.image_pitch_bytes = f.image.stride(0)
+            a.height, a.width = f.image.shape
+            a.prev = ctypes.pointer(f.prev.desc) if f.prev is not None else None
+            a.cur = ctypes.pointer(f.cur.desc)
+            a.tracks = f.tracks.data_ptr() if f.tracks is not None else None
+            a.n_tracks = f.tracks.shape[0] if f.tracks is not None else 0
+            a.num_desired = f.num_desired
+            a.new_xy = f.new_xy.data_ptr()
+            a.new_count = f.new_count.data_ptr()
+            for k in range(4):
+                a.border[k] = f.border[k]
+        h = ctypes.c_void_p()
+        _lib.check(ctx.lib.fe_batch_create(ctx.handle, arr, len(self.frames), int(sampling), ctypes.byref(h)),
+                   "fe_batch_create")
+        self.handle = h
+
+    def run(self, stream=None):
+        _lib.check(self.ctx.lib.fe_batch_run(self.handle, _stream_handle(stream)), "fe_batch_run")
+
+    def run_part(self, part, stream=None):
+        """part: 0 pyramids, 1 LK, 2 selection (enqueued directly, no graph)."""
+        _lib.check(self.ctx.lib.fe_batch_run_part(self.handle, int(part), _stream_handle(stream)), "fe_batch_run_part")
+
+    def kernel_count(self):
+        return self.ctx.lib.fe_batch_kernel_count(self.handle)
+
+    def run_plain(self, stream=None):
+        _lib.check(self.ctx.lib.fe_batch_run_plain(self.handle, _stream_handle(stream)), "fe_batch_run_plain")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.fe_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

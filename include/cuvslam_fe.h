@@ -1,0 +1,211 @@
+/* cuvslam_fe.h - C ABI of the B200-native visual-tracking front-end.
+ *
+ * The library replaces the hot path that cuVSLAM's MonoSOFGPU drives through four host wrappers
+ * and the C-style kernel launchers of libs/cuda_modules:
+ *   Gaussian image pyramid + gradient pyramid, Shi-Tomasi (GFTT) response and feature selection,
+ *   and pyramidal Lucas-Kanade tracking,
+ * with results equal to the reference GPU path (see each entry point).  All entry points:
+ *   - take device pointers, sizes in elements/pixels and pitches in BYTES;
+ *   - enqueue work on the caller's stream and return without synchronising, unless stated;
+ *   - return an fe_status code and never throw across the ABI.
+ * Citations are to cuVSLAM 18.0.0 (libs/...).
+ */
+#ifndef CUVSLAM_FE_H
+#define CUVSLAM_FE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FE_API __attribute__((visibility("default")))
+#else
+#define FE_API
+#endif
+
+#define FE_MAX_LEVELS 10 /* PYRAMID_LEVELS, cuda_kernels.h:29 */
+#define FE_ABI_VERSION 1
+
+typedef enum {
+  FE_OK = 0,
+  FE_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, misaligned pitch, ... */
+  FE_ERR_CUDA = 2,             /* a CUDA runtime call failed; see fe_last_cuda_error() */
+  FE_ERR_OUT_OF_MEMORY = 3,
+  FE_ERR_CAPACITY = 4,         /* a documented size limit was exceeded */
+  FE_ERR_DEVICE_FAULT = 5,     /* a kernel reported a bounded wait that ran out or a bad work item */
+} fe_status;
+
+typedef struct CUstream_st* fe_stream; /* identical to cudaStream_t */
+typedef struct fe_context fe_context;
+typedef struct fe_batch fe_batch;
+
+/* One image pyramid and its gradient pyramid in device memory.  Level l has width[l] x height[l]
+ * FP32 pixels for image, grad_x and grad_y, rows pitch_bytes[l] apart (a multiple of 16).
+ * Level sizes follow the reference: (d+1)/2 while both sides stay >= 15, at most FE_MAX_LEVELS
+ * (GPUImagePyramid::prepare_levels, image_pyramid.h:136-151; ScaleDownDim, image_pyramid.cpp:24).
+ * Replaces GaussianGPUImagePyramid + GPUGradientPyramid (image_pyramid.h:56-162,
+ * gradient_pyramid.h:30-59). */
+typedef struct {
+  int32_t levels;
+  int32_t width[FE_MAX_LEVELS];
+  int32_t height[FE_MAX_LEVELS];
+  int64_t pitch_bytes[FE_MAX_LEVELS];
+  float* image[FE_MAX_LEVELS];
+  float* grad_x[FE_MAX_LEVELS];
+  float* grad_y[FE_MAX_LEVELS];
+} fe_pyramid;
+
+/* cuvslam::cuda::TrackData, byte-for-byte (cuda_kernels.h:76-87): 80 bytes, 16-byte aligned.
+ * Inputs: track (previous position, texture coordinates), offset (predicted motion),
+ * search_radius_px (< 0 disables the track), ncc_threshold.  Outputs: track (new position, only
+ * written when tracked), track_status, info (= diag(1/9)).  Other fields are not touched. */
+typedef struct {
+  float track[2];
+  float offset[2];
+  float info[4];
+  uint8_t track_status;
+  uint8_t reserved0[3];
+  int32_t cache_index;
+  float reserved1[2];
+  float initial_guess_map[4];
+  float search_radius_px;
+  float ncc_threshold;
+  float ncc;
+  float reserved2;
+} fe_track_data;
+
+/* Bilinear sampling of LK patches. */
+typedef enum {
+  FE_SAMPLE_TEXTURE = 0, /* cudaFilterModeLinear's 8-bit-fraction weights: matches the reference */
+  FE_SAMPLE_EXACT = 1,   /* exact FP32 weights (differentiable; used by the adjoint) */
+} fe_sampling;
+
+/* ---------------------------------------------------------------------------------------- */
+/* Library                                                                                   */
+/* ---------------------------------------------------------------------------------------- */
+
+FE_API int fe_abi_version(void);
+FE_API const char* fe_status_string(int status);
+/* The CUDA error behind the last FE_ERR_CUDA on this thread (0 if none). */
+FE_API int fe_last_cuda_error(void);
+
+/* Context: owns the scratch memory of selection and batching on one device.  The device must be
+ * current on the calling thread for every call that takes the context.
+ * Replaces the per-wrapper state of GPUSelection / GPULKFeatureTracker (selection_v2.h:28-58,
+ * lk_tracker.h:27-37) and the lazy init_* constant uploads (image_pyramid.cu:33-54, ...). */
+FE_API int fe_create(int device, fe_context** out);
+FE_API int fe_destroy(fe_context* ctx);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Pyramid                                                                                   */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Number of levels of a width x height pyramid capped at max_levels (0 on bad arguments). */
+FE_API int fe_pyramid_levels(int width, int height, int max_levels);
+/* Bytes of device memory one pyramid (image + grad_x + grad_y, all levels) needs in this
+ * library's layout (each plane 256-byte aligned, rows padded to 256 bytes). */
+FE_API int64_t fe_pyramid_bytes(int width, int height, int max_levels);
+/* Lays a pyramid out in caller-provided device memory of at least fe_pyramid_bytes() bytes
+ * (256-byte aligned).  Host-only; allocates nothing. */
+FE_API int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int height, int max_levels, fe_pyramid* out);
+
+/* Builds every level and both gradient images of `pyr` from a uint8 grayscale image in device
+ * memory.  Results are bit-identical to the reference's
+ *   cast_image (image_cast.cu:24-36) + GaussianGPUImagePyramid::build (image_pyramid.h:81-98,
+ *   gaussian_scaling_kernel image_pyramid.cu:56-102) + GPUGradientPyramid::set
+ *   (gradient_pyramid.cpp:83-118, conv_grad_x/y convolutions.cu:74-139).
+ * `pyr` must describe width x height at level 0.  box3 must be 0 (box prefilter not built). */
+FE_API int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
+                     int box3, const fe_pyramid* pyr, fe_stream stream);
+/* Same from an FP32 level-0 image (rows pitch_bytes apart). */
+FE_API int fe_build_pyramid_f32(fe_context* ctx, const float* image, int64_t image_pitch_bytes, int width, int height,
+                         const fe_pyramid* pyr, fe_stream stream);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Selection                                                                                 */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Shi-Tomasi response on level 0 of `pyr`, 3x3 non-maximum suppression, 9x9 suppression around
+ * the n_alive alive features, one candidate per 8x8 cell above 1e-2 refined to sub-pixel, and the
+ * per-bin (8x8 bins) quota apportioned by response strength; writes at most num_desired new
+ * features (x, y pairs) to out_xy and their number to *out_count (both device memory).
+ * Equals GPUSelection::computeGFTTAndSelectFeatures (selection_v2.cpp:27-184) with a total order
+ * where the reference is nondeterministic: keypoints are ordered by strength, ties by cell raster
+ * index, and each bin sum adds its 16x16 sub-tile sums row by row (left to right within a row,
+ * then the row sums top to bottom).
+ * mask (optional, device, width x height, non-zero = masked) and alive_xy (device, n_alive
+ * x,y pairs) may be NULL.  Asynchronous; no host synchronisation.
+ * One context runs one selection at a time: calls on different streams must use different contexts.
+ * Limits: width, height <= 4096; num_desired <= 16384. */
+FE_API int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int border_bottom, int border_left,
+              int border_right, const uint8_t* mask, int64_t mask_pitch_bytes, const float* alive_xy, int n_alive,
+              int num_desired, float* out_xy, int32_t* out_count, fe_stream stream);
+
+/* Diagnostic outputs of the last fe_select on this context (device pointers, valid until the
+ * next fe_select): the response map (level-0 size, pitch = width*4) and the NMS map. */
+FE_API int fe_select_debug(fe_context* ctx, const float** response, const float** nms);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Lucas-Kanade                                                                              */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Pyramidal LK of n tracks from `prev` (image + gradients) to `cur` (image), updating `tracks`
+ * in place (device memory).  One warp per track.  With FE_SAMPLE_TEXTURE the results agree with
+ * the reference's lk_track_kernel (lk_tracker.cu:69-379, launched by
+ * GPULKFeatureTracker::track_points, cuda_modules/lk_tracker.cpp:24-73) to well under 0.01 px;
+ * horizontal != 0 selects lk_track_horizontal_kernel (lk_tracker.cu:381-665). */
+FE_API int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks, int n,
+             int horizontal, int sampling, fe_stream stream);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Batched multi-camera frame step                                                           */
+/* ---------------------------------------------------------------------------------------- */
+
+/* One camera of a batched frame step.  All pointers are device memory except `prev`/`cur`,
+ * which point to host descriptors. */
+typedef struct {
+  const uint8_t* image; /* current frame, uint8 grayscale */
+  int64_t image_pitch_bytes;
+  int32_t width, height;
+  const fe_pyramid* prev; /* previous frame's pyramid (may be NULL on a first frame) */
+  const fe_pyramid* cur;  /* pyramid to build from `image` */
+  fe_track_data* tracks;  /* tracks to advance prev -> cur */
+  int32_t n_tracks;
+  int32_t num_desired;    /* tracks to maintain (num_desired_tracks): after LK, selection adds
+                             max(0, num_desired - tracks LK kept) features (0 = no selection) */
+  float* new_xy;          /* out: selected features, capacity num_desired */
+  int32_t* new_count;     /* out */
+  int32_t border[4];      /* top, bottom, left, right */
+} fe_camera_frame;
+
+/* Plans a batched frame step over ncams cameras: the pyramids of all cameras, LK of all tracks,
+ * and selection on all cameras (alive features = tracks that LK kept), as a few launches over
+ * flattened (camera, tile) and (camera, track) work lists, captured once into a CUDA graph.
+ * The descriptors are copied; the device buffers they name must stay valid while the batch
+ * lives.  sampling as in fe_track. */
+FE_API int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int sampling, fe_batch** out);
+/* Launches the planned step on `stream` (graph launch). */
+FE_API int fe_batch_run(fe_batch* batch, fe_stream stream);
+
+/* Parts of a batched step, for pipelining and measurement. */
+typedef enum {
+  FE_PART_PYRAMID = 0, /* pyramids of all cameras */
+  FE_PART_TRACK = 1,   /* LK of all tracks (needs the pyramids) */
+  FE_PART_SELECT = 2,  /* selection on all cameras (needs pyramids and LK) */
+} fe_batch_part;
+/* Enqueues one part of the planned step directly (no graph). */
+FE_API int fe_batch_run_part(fe_batch* batch, int part, fe_stream stream);
+/* Number of kernel launches in one fe_batch_run (kernel nodes of the captured graph). */
+FE_API int fe_batch_kernel_count(fe_batch* batch);
+/* The same step as a plain per-camera sequence of fe_build_pyramid / fe_track / fe_select
+ * (the drop-in launch pattern), for comparison. */
+FE_API int fe_batch_run_plain(fe_batch* batch, fe_stream stream);
+FE_API int fe_batch_destroy(fe_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUVSLAM_FE_H */

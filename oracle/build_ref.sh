@@ -14,6 +14,10 @@ if [ ! -d "$K" ]; then
   exit 0
 fi
 mkdir -p "$HERE/_ref"
+OUT="$HERE/_ref/libcuvslam_ref.so"
+if [ -f "$OUT" ] && [ "$OUT" -nt "$HERE/ref_harness.cu" ] && [ "$OUT" -nt "$K/lk_tracker.cu" ]; then
+  exit 0
+fi
 nvcc -gencode arch=compute_100a,code=sm_100a -O3 -DNDEBUG -std=c++17 -lineinfo \
   -Xcompiler -fPIC -shared -I "$REF/libs" \
   "$K/image_cast.cu" "$K/image_pyramid.cu" "$K/convolutions.cu" "$K/gftt.cu" \

@@ -167,12 +167,13 @@ static float butterfly(float* v, int levels) {
 /* Per-bin strength sums.  accumulateGFTT_kernel (cuda_kernels/selection_v2.cu:39-92) sums each
  * 16x16 sub-tile (warp butterfly over 2 rows x 16 columns, then a 3-level butterfly over the 8
  * warps) and adds the sub-tile into the 8x8 bin containing its centre with a float atomicAdd, in
- * arbitrary order.  Here the sub-tile sums are added in raster order of the sub-tile grid, the
- * deterministic order the CUDA kernels use. */
+ * arbitrary order.  Here the order is fixed as the CUDA kernels fix it: a bin adds its sub-tiles
+ * row by row (left to right), then adds the row sums top to bottom. */
 void or_bins(const float* resp, int w, int h, float* bins64) {
   const int bw = w / 8, bh = h / 8;
   memset(bins64, 0, sizeof(float) * 64);
   const int tw = (w + 15) / 16, th = (h + 15) / 16;
+  float* sub = (float*)malloc(sizeof(float) * (size_t)(tw > 0 ? tw : 1) * (th > 0 ? th : 1));
   for (int ty = 0; ty < th; ++ty) {
     for (int tx = 0; tx < tw; ++tx) {
       float part[32] = {0};
@@ -184,12 +185,24 @@ void or_bins(const float* resp, int w, int h, float* bins64) {
         }
         part[wp] = butterfly(lanes, 5);
       }
-      float s = butterfly(part, 3);
-      if (bw <= 0 || bh <= 0) continue;
-      unsigned bx = (unsigned)(tx * 16 + 8) / (unsigned)bw, by = (unsigned)(ty * 16 + 8) / (unsigned)bh;
-      if (bx < 8 && by < 8) bins64[by * 8 + bx] += s;
+      sub[ty * tw + tx] = butterfly(part, 3);
     }
   }
+  if (bw > 0 && bh > 0) {
+    for (int b = 0; b < 64; ++b) {
+      const unsigned bx = (unsigned)(b & 7), by = (unsigned)(b >> 3);
+      float acc = 0.f;
+      for (int ty = 0; ty < th; ++ty) {
+        if ((unsigned)(ty * 16 + 8) / (unsigned)bh != by) continue;
+        float row = 0.f;
+        for (int tx = 0; tx < tw; ++tx)
+          if ((unsigned)(tx * 16 + 8) / (unsigned)bw == bx) row += sub[ty * tw + tx];
+        acc += row;
+      }
+      bins64[b] = acc;
+    }
+  }
+  free(sub);
 }
 
 static int rint_even(float v) { return (int)nearbyintf(v); }
@@ -499,7 +512,7 @@ static void lk_one(int levels, const int* ws, const int* hs, const float* const*
     const int W = ws[level], H = hs[level];
     float xmin = sx + (0.5f - 4.5f), xmax = sx + (0.5f - 4.5f + 9.f);
     float ymin = sy + (0.5f - 4.5f), ymax = sy + (0.5f - 4.5f + 9.f);
-    int good = !(xmin < 0 || xmax >= (float)W || ymin < 0 || ymax >= (float)H);
+    int good = xmin >= 0 && xmax < (float)W && ymin >= 0 && ymax < (float)H;
     if (good) {
       for (int e = 0; e < NE; ++e)
         for (int l = 0; l < 32; ++l) {
@@ -565,7 +578,7 @@ static void lk_one(int levels, const int* ws, const int* hs, const float* const*
         xmax = cx + (0.5f - 4.5f + 9.f);
         ymin = cy + (0.5f - 4.5f);
         ymax = cy + (0.5f - 4.5f + 9.f);
-        if (xmin < 0 || xmax >= (float)W || ymin < 0 || ymax >= (float)H) good = 0;
+        if (!(xmin >= 0 && xmax < (float)W && ymin >= 0 && ymax < (float)H)) good = 0;
         if (!good) break;
         for (int e = 0; e < NE; ++e)
           for (int l = 0; l < 32; ++l) {

@@ -57,13 +57,14 @@ def lib():
 
 # CPU-semantics (cuVSLAM use_gpu=false) entry points, see cpu_tracker.c
 _CPU_SIGS = [
-    ("cpu_ctx_create", [I, I, I], P),
-    ("cpu_ctx_destroy", [P], None),
-    ("cpu_ctx_build", [P, P], I),
-    ("cpu_ctx_levels", [P], I),
-    ("cpu_ctx_level", [P, I, P, P, P], I),
-    ("cpu_track", [P, P, P, P, I, P, P, I], I),
-    ("cpu_select", [P, P, I, I, I, I, I, I, P], I),
+    ("cpu_cam_create", [I, I], P),
+    ("cpu_cam_destroy", [P], None),
+    ("cpu_cam_build", [P, P], None),
+    ("cpu_cam_levels", [P], I),
+    ("cpu_cam_level", [P, I, P, P, P, P, P], None),
+    ("cpu_cam_track", [P, P, P, P, I, P, P], I),
+    ("cpu_cam_select", [P, P, I, I, I, I, I, I, P], I),
+    ("cpu_frame_step", [P, P, P, P, P, P, P, P, P, P, P, I, I], I),
 ]
 
 
@@ -188,3 +189,69 @@ def lk(prev_pyr, cur_pyr, tracks, mode=TEXTURE, horizontal=False, f64=False):
         L.or_lk_track(levels, _p(ws), _p(hs), pgx, pgy, pim, cim, _p(t), len(t), mode)
     del keep1, keep2, keep3, keep4
     return t
+
+
+class CpuCamera:
+    """One camera of the restated reference CPU tracker (cpu_tracker.c)."""
+
+    def __init__(self, width, height):
+        self.w, self.h = int(width), int(height)
+        self.h_ = lib().cpu_cam_create(self.w, self.h)
+
+    def build(self, img_u8):
+        img = np.ascontiguousarray(img_u8, np.uint8)
+        assert img.shape == (self.h, self.w)
+        lib().cpu_cam_build(self.h_, _p(img))
+        return self
+
+    def levels(self):
+        return lib().cpu_cam_levels(self.h_)
+
+    def level(self, l):
+        w, h = ctypes.c_int(), ctypes.c_int()
+        lib().cpu_cam_level(self.h_, l, ctypes.byref(w), ctypes.byref(h), None, None, None)
+        out = [np.zeros((h.value, w.value), np.float32) for _ in range(3)]
+        lib().cpu_cam_level(self.h_, l, ctypes.byref(w), ctypes.byref(h), _p(out[0]), _p(out[1]), _p(out[2]))
+        return out
+
+    def track_from(self, prev, xy, pred=None):
+        xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+        out = np.zeros_like(xy)
+        st = np.zeros(len(xy), np.uint8)
+        pr = None if pred is None else np.ascontiguousarray(pred, np.float32).reshape(-1, 2)
+        lib().cpu_cam_track(prev.h_, self.h_, _p(xy), None if pr is None else _p(pr), len(xy), _p(out), _p(st))
+        return out, st
+
+    def select(self, alive=None, num_desired=450, borders=(0, 0, 0, 0)):
+        alive = np.zeros((0, 2), np.float32) if alive is None else np.ascontiguousarray(alive, np.float32).reshape(-1, 2)
+        out = np.zeros((max(num_desired, 1), 2), np.float32)
+        n = lib().cpu_cam_select(self.h_, _p(alive), len(alive), num_desired, *borders, _p(out))
+        return out[:n]
+
+    def __del__(self):
+        try:
+            lib().cpu_cam_destroy(self.h_)
+        except Exception:
+            pass
+
+
+def cpu_frame_step(prev_cams, cur_cams, images, xy, pred, num_desired, nthreads):
+    """One multi-camera frame step of the restated CPU tracker on `nthreads` threads.
+    Returns (tracked positions, status, new features) per camera."""
+    n = len(cur_cams)
+    PA = ctypes.c_void_p * n
+    imgs = [np.ascontiguousarray(i, np.uint8) for i in images]
+    xys = [np.ascontiguousarray(a, np.float32).reshape(-1, 2) for a in xy]
+    preds = None if pred is None else [np.ascontiguousarray(a, np.float32).reshape(-1, 2) for a in pred]
+    outs = [np.zeros_like(a) for a in xys]
+    sts = [np.zeros(len(a), np.uint8) for a in xys]
+    news = [np.zeros((max(int(k), 1), 2), np.float32) for k in num_desired]
+    counts = np.zeros(n, np.int32)
+    ns = np.array([len(a) for a in xys], np.int32)
+    nd = np.array(num_desired, np.int32)
+    lib().cpu_frame_step(PA(*[c.h_ for c in prev_cams]) if prev_cams is not None else None, PA(*[c.h_ for c in cur_cams]),
+                         PA(*[i.ctypes.data for i in imgs]), PA(*[a.ctypes.data for a in xys]),
+                         None if preds is None else PA(*[a.ctypes.data for a in preds]), _p(ns), _p(nd),
+                         PA(*[a.ctypes.data for a in outs]), PA(*[a.ctypes.data for a in sts]),
+                         PA(*[a.ctypes.data for a in news]), _p(counts), n, nthreads)
+    return outs, sts, [a[:c] for a, c in zip(news, counts)]
