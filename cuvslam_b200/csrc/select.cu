@@ -282,22 +282,39 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
 }
 
 // ---------------------------------------------------------------- quotas
-__global__ void quota_kernel(const __grid_constant__ SelectBatch b) {
+// Sub-tile index range [lo, hi) whose centres (16 t + 8) fall in bin b of size `bin_px`.
+__device__ __forceinline__ int2 bin_range(int b, int bin_px, int n) {
+  const int lo = max(0, (b * bin_px - 8 + 15) / 16);
+  const int hi = min(n, ((b + 1) * bin_px - 8 + 15) / 16);
+  return make_int2(lo, max(hi, lo));
+}
+
+constexpr int kMaxBinRows = 40;  // sub-tile rows per bin for heights <= 4096
+
+__global__ void __launch_bounds__(512) quota_kernel(const __grid_constant__ SelectBatch b) {
   const SelectCam& c = b.cam[blockIdx.x];
+  __shared__ float rows[64][kMaxBinRows];
   __shared__ float bins[64];
   const int bw = c.w / 8, bh = c.h / 8;
   const int sw = (c.w + 15) / 16, sh = (c.h + 15) / 16;
+  if (bw > 0 && bh > 0) {
+    // row sums: one (bin column, sub-tile row) per thread, left to right
+    for (int i = threadIdx.x; i < 8 * sh; i += blockDim.x) {
+      const int bx = i & 7, ty = i >> 3;
+      const int by = (ty * 16 + 8) / bh;
+      if (by >= 8) continue;
+      const int2 xr = bin_range(bx, bw, sw);
+      float row = 0.f;
+      for (int tx = xr.x; tx < xr.y; ++tx) row = __fadd_rn(row, c.sub_sum[ty * sw + tx]);
+      rows[by * 8 + bx][ty - bin_range(by, bh, sh).x] = row;
+    }
+  }
+  __syncthreads();
   if (threadIdx.x < 64) {
     float acc = 0.f;
     if (bw > 0 && bh > 0) {
-      const int bx = threadIdx.x & 7, by = threadIdx.x >> 3;
-      for (int ty = 0; ty < sh; ++ty) {
-        if ((ty * 16 + 8) / bh != by) continue;
-        float row = 0.f;
-        for (int tx = 0; tx < sw; ++tx)
-          if ((tx * 16 + 8) / bw == bx) row = __fadd_rn(row, c.sub_sum[ty * sw + tx]);
-        acc = __fadd_rn(acc, row);
-      }
+      const int2 yr = bin_range(threadIdx.x >> 3, bh, sh);
+      for (int k = 0; k < yr.y - yr.x; ++k) acc = __fadd_rn(acc, rows[threadIdx.x][k]);
     }
     bins[threadIdx.x] = acc;
   }
@@ -437,7 +454,7 @@ cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap
   if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
   alive_kernel<<<b.ncams, 256, 0, s>>>(b);
   tile_kernel<<<total_tiles, kTileThreads, 0, s>>>(b);
-  quota_kernel<<<b.ncams, 64, 0, s>>>(b);
+  quota_kernel<<<b.ncams, 512, 0, s>>>(b);
   bin_kernel<<<dim3(64, b.ncams), 256, sizeof(uint64_t) * bin_key_cap, s>>>(b, bin_key_cap);
   final_kernel<<<b.ncams, 1024, sizeof(uint64_t) * final_key_cap, s>>>(b, final_key_cap);
   return cudaGetLastError();
