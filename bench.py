@@ -121,6 +121,33 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def reduce_max(x, dist, device):
+    """Max over ranks of a per-rank scalar (timing); identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x, dist, device):
+    """Sum over ranks of a per-rank count; identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(round(t.item()))
+
+
+def throughput(units_all_ranks, steps, ms_max):
+    """Whole-job units/s: the units all ranks processed per step, over the slowest rank's time."""
+    return units_all_ranks * steps / (ms_max / 1e3)
+
+
 def cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads):
     """A callable running one frame step of the restated reference CPU tracker over all cameras."""
     from oracle import oracle as O
@@ -230,22 +257,18 @@ def main():
             fn()
         e.record(stream)
         torch.cuda.synchronize()
-        ms = s.elapsed_time(e)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return reduce_max(s.elapsed_time(e), dist, dev)
 
     # ---- headline: batched, device-resident inputs
     with ClockSampler(local) as clk:
         ms = timed(step_batched, args.steps, args.warmup)
     clocks = clk.summary()
-    value = world * attempted * args.steps / (ms / 1e3)
+    total_units = reduce_sum(attempted, dist, dev)
+    value = throughput(total_units, args.steps, ms)
 
     # ---- plain per-camera launch sequence (same work)
     ms_plain = timed(step_plain, max(3, args.steps // 2), 2)
-    plain_value = world * attempted * max(3, args.steps // 2) / (ms_plain / 1e3)
+    plain_value = throughput(total_units, max(3, args.steps // 2), ms_plain)
 
     # ---- end to end through the public API with host buffers
     pin_imgs = [torch.from_numpy(n).pin_memory() for n in nexts]
@@ -268,7 +291,7 @@ def main():
             oc.copy_(f.new_count, non_blocking=True)
 
     ms_e2e = timed(step_e2e, args.steps, max(args.warmup, 3))
-    e2e_value = world * attempted * args.steps / (ms_e2e / 1e3)
+    e2e_value = throughput(total_units, args.steps, ms_e2e)
 
     # ---- dominant part and its roofline (pyramid stages: HBM-bound)
     def part(p):
@@ -311,7 +334,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "tracks_per_step": attempted, "cameras": len(shapes),
+            "config": {"workload": WORKLOAD, "tracks_per_step": total_units, "cameras": len(shapes) * world,
                        "l2": "working set > L2 (~600 MB of pyramids written per step)", "sampling": "texture"},
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain / max(3, args.steps // 2)},
             "batched_over_plain": value / plain_value,
