@@ -67,6 +67,7 @@ _SIGS = {
     "fe_build_pyramid": (_I, [_P, _P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid), _P]),
     "fe_build_pyramid_f32": (_I, [_P, _P, _I64, _I, _I, ctypes.POINTER(FePyramid), _P]),
     "fe_select": (_I, [_P, ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
+    "fe_select_noalloc": (_I, [ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
     "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "fe_track": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _P]),
     "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),

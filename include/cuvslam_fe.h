@@ -144,6 +144,22 @@ FE_API int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int
               int border_right, const uint8_t* mask, int64_t mask_pitch_bytes, const float* alive_xy, int n_alive,
               int num_desired, float* out_xy, int32_t* out_count, fe_stream stream);
 
+/* fe_select without a context and without allocating: for callers that cannot call cudaMalloc
+ * while they run (a tracking loop with a per-frame deadline that reserves all memory at start-up,
+ * where cudaMalloc's device synchronisation and unbounded latency would break the deadline, or a
+ * process whose device memory all belongs to its own pool allocator).  No counterpart in the
+ * reference: it has no allocation-free selection.
+ * Scratch is a static device array of about 1.5 MB inside the library, held by every GPU that
+ * loads it until the process exits.  Limits: width, height <= 2048 and n_alive + num_desired
+ * <= 16320; larger requests return FE_ERR_CAPACITY.  The first call on a device sets up that
+ * device (looks up the array's device address, sets kernel attributes) and must come before any
+ * stream capture on it.  All calls share the one array: calls whose GPU work overlaps (other
+ * streams, other host threads) race and must be serialised by the caller.  Results equal
+ * fe_select's. */
+FE_API int fe_select_noalloc(const fe_pyramid* pyr, int border_top, int border_bottom, int border_left,
+                             int border_right, const uint8_t* mask, int64_t mask_pitch_bytes, const float* alive_xy,
+                             int n_alive, int num_desired, float* out_xy, int32_t* out_count, fe_stream stream);
+
 /* Diagnostic outputs of the last fe_select on this context (device pointers, valid until the
  * next fe_select): the response map (level-0 size, pitch = width*4) and the NMS map. */
 FE_API int fe_select_debug(fe_context* ctx, const float** response, const float** nms);
