@@ -96,7 +96,6 @@ using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
 // to two more.
 int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan) {
   const fe::Pyr pyr = to_pyr(p);
-  const int T = fe::stage_tile();
   int s = 0;
   for (int stage = 0;; ++stage) {
     const int nl = std::min(2, pyr.levels - 1 - s);
@@ -109,10 +108,12 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.src_w = pyr.lv[s].w;
     job.src_h = pyr.lv[s].h;
     for (int k = 0; k <= nl; ++k) job.out[k] = pyr.lv[s + k];
+    const bool kind_u8 = stage == 0 && u8;
+    const int T = fe::stage_tile(kind_u8, nl);
     const fe::Level& deep = pyr.lv[s + nl];
     job.tiles_x = (deep.w + T - 1) / T;
     job.tiles_y = (deep.h + T - 1) / T;
-    const bool kind_u8 = stage == 0 && u8;
+    if (kind_u8 && nl == 2) fe::encode_frame_tmap(job);
     if ((int)plan.size() <= stage) plan.resize(stage + 1);
     StageGroup* g = nullptr;
     for (auto& gg : plan[stage])

@@ -1,6 +1,7 @@
 // Host-visible job descriptors and launchers shared by the kernel files and the C ABI layer.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -9,11 +10,13 @@
 namespace fe {
 
 // ---------------------------------------------------------------- pyramid
-struct StageJob {
+struct alignas(64) StageJob {
+  CUtensorMap tmap;         // uint8 frame (levels 0-2 stage, when use_tma)
   const void* src;          // level s: uint8 (s == 0) or float
   int64_t src_pitch_bytes;
   int src_w, src_h;
   int write_level0;         // also write level s (image cast + gradients): the uint8 stage
+  int use_tma;              // frame meets TMA alignment (16-byte base and pitch)
   int tiles_x, tiles_y;
   int tile_begin;           // first CTA of this job in the launch
   Level out[3];             // out[k] = level s + k; out[0] describes level s
@@ -21,10 +24,14 @@ struct StageJob {
 
 struct StageBatch {
   int njobs;
+  int* status;              // device flags: bit 0 = a TMA wait ran out (tile skipped)
   StageJob job[kMaxCams];
 };
 
-int stage_tile();
+int stage_tile(bool u8, int nl);  // deepest-level core tile edge of a stage kind
+// Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
+// TMA alignment (the stage then stages its tile with ordinary loads).
+bool encode_frame_tmap(StageJob& job);
 cudaError_t pyramid_init();  // kernel attributes; call once per device before capture
 cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, cudaStream_t s);
 

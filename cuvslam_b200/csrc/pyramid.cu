@@ -167,6 +167,296 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
   }
 }
 
+// ---------------------------------------------------------------- levels 0-2 from the uint8 frame
+//
+// The first stage dominates the pyramid's HBM traffic (it writes ~98% of the bytes), so it has its
+// own kernel.  A CTA owns a 32x32 level-2 core tile (128x128 at level 0) and
+//   1. stages its 176x161 uint8 tile with one TMA copy (zero fill outside the frame), or with plain
+//      loads when the frame's base/pitch are not 16-byte aligned;
+//   2. computes level 1 on its 79x79 region as column strips with a sliding 5-row window of
+//      horizontal 5-tap sums, in integers;
+//   3. computes level 2 on its 38x38 region the same way from level 1, in FP32;
+//   4. writes the three core tiles (image, grad_x, grad_y) with 16-byte stores.
+// Levels 1 and 2 are exact in any summation order (all partial sums are multiples of 2^-16 below
+// 2^8), so the separable sums equal gaussian_scaling_kernel's 25-tap FMA chain bit for bit; only the
+// four image-corner pixels, where the reference skips the taps outside in both x and y, are redone
+// with the 25-tap rule.
+namespace l012 {
+
+constexpr int kT2 = 32;
+constexpr int kThreads = 512;
+constexpr int kS0W = 176, kS0H = 161;  // uint8 tile: cols [4X2-32, 4X2+144), rows [4Y2-18, 4Y2+143)
+constexpr int kS1 = 79, kS1S = 80;     // level 1: [2X2-8, 2X2+71) in x and y
+constexpr int kS2 = 38, kS2S = 40;     // level 2: rows [Y2-3, Y2+35); columns stored from X2-4
+constexpr int kB0Bytes = kS0W * kS0H;
+constexpr int kOffB1 = (kB0Bytes + 127) / 128 * 128;
+constexpr int kOffB2 = kOffB1 + kS1 * kS1S * 4;
+constexpr int kOffBar = kOffB2 + kS2 * kS2S * 4;
+constexpr int kSmem = kOffBar + 64;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait on an mbarrier phase: false when it ran out (the caller reports it and gives up).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 25-tap value with the reference's corner rule (taps outside in x and y skipped), uint8 source.
+__device__ float corner_l1(const uint8_t* B0, int a0x, int a0y, int w0, int h0, int x1, int y1) {
+  int acc = 0;
+  for (int k = 0; k < 5; ++k)
+    for (int l = 0; l < 5; ++l) {
+      const int xc = 2 * x1 - 2 + l, yc = 2 * y1 - 2 + k;
+      if ((xc < 0 || xc >= w0) && (yc < 0 || yc >= h0)) continue;
+      const int wk = k == 2 ? 6 : (k & 1 ? 4 : 1), wl = l == 2 ? 6 : (l & 1 ? 4 : 1);
+      acc += wk * wl * (int)B0[(mirror_index(yc, h0) - a0y) * kS0W + (mirror_index(xc, w0) - a0x)];
+    }
+  return (float)acc * (1.f / 256.f);
+}
+
+__global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_constant__ StageBatch batch) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  uint8_t* B0 = sm;
+  float* B1 = reinterpret_cast<float*>(sm + kOffB1);
+  float* B2 = reinterpret_cast<float*>(sm + kOffB2);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kOffBar);
+  const int tid = threadIdx.x;
+
+  int lo = 0, hi = batch.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (batch.job[mid].tile_begin <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+  }
+  const StageJob& job = batch.job[lo];
+  const int t = (int)blockIdx.x - job.tile_begin;
+  const int X2 = (t % job.tiles_x) * kT2, Y2 = (t / job.tiles_x) * kT2;
+  const Level& L0 = job.out[0];
+  const Level& L1 = job.out[1];
+  const Level& L2 = job.out[2];
+  const int w0 = L0.w, h0 = L0.h, w1 = L1.w, h1 = L1.h, w2 = L2.w, h2 = L2.h;
+  const int a0x = 4 * X2 - 32, a0y = 4 * Y2 - 18;
+  const int a1x = 2 * X2 - 8, a1y = 2 * Y2 - 8;
+  const int a2x = X2 - 4, a2y = Y2 - 3;  // level-2 storage origin (column X2-4 is never computed)
+
+  // 1. the uint8 tile
+  if (job.use_tma) {
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(kB0Bytes)
+                   : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+          "[%4];" ::"r"(smem_u32(B0)),
+          "l"(reinterpret_cast<uint64_t>(&job.tmap)), "r"(a0x), "r"(a0y), "r"(smem_u32(bar))
+          : "memory");
+    }
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0 && batch.status) atomicOr(batch.status, 1);
+      // the copy may still land: wait once more (bounded) so no write targets a retired CTA
+      mbar_wait(bar, 0);
+      return;
+    }
+  } else {
+    const uint8_t* src = static_cast<const uint8_t*>(job.src);
+    for (int i = tid; i < kS0H * kS0W; i += kThreads) {
+      const int r = i / kS0W, c = i - r * kS0W;
+      const int gx = a0x + c, gy = a0y + r;
+      B0[i] = (gx >= 0 && gy >= 0 && gx < w0 && gy < h0) ? __ldg(src + (int64_t)gy * job.src_pitch_bytes + gx) : 0;
+    }
+  }
+  __syncthreads();
+
+  // 2. level 1: column strips of 14 rows, sliding window of horizontal sums
+  if (tid < kS1 * 6) {
+    const int c = tid % kS1, band = tid / kS1;
+    const int x1 = a1x + c;
+    const int ys = max(a1y + band * 14, 0), ye = min(a1y + min(band * 14 + 14, kS1), h1);
+    if (x1 >= 0 && x1 < w1 && ys < ye) {
+      int col[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * x1 - 2 + l, w0) - a0x;
+      auto H = [&](int r) {
+        const uint8_t* p = B0 + (mirror_index(r, h0) - a0y) * kS0W;
+        return (int)p[col[0]] + (int)p[col[4]] + 4 * ((int)p[col[1]] + (int)p[col[3]]) + 6 * (int)p[col[2]];
+      };
+      int h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
+      for (int y = ys;; ) {
+        const int S = h0_ + h4_ + 4 * (h1_ + h3_) + 6 * h2_;
+        B1[(y - a1y) * kS1S + c] = (float)S * (1.f / 256.f);
+        if (++y >= ye) break;
+        h0_ = h2_;
+        h1_ = h3_;
+        h2_ = h4_;
+        h3_ = H(2 * y + 1);
+        h4_ = H(2 * y + 2);
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < 4) {
+    const int x1 = (tid & 1) ? w1 - 1 : 0, y1 = (tid & 2) ? h1 - 1 : 0;
+    if (x1 >= a1x && x1 < a1x + kS1 && y1 >= a1y && y1 < a1y + kS1)
+      B1[(y1 - a1y) * kS1S + (x1 - a1x)] = corner_l1(B0, a0x, a0y, w0, h0, x1, y1);
+  }
+  __syncthreads();
+
+  // 3. level 2 from level 1, same scheme in FP32 (exact)
+  if (tid < kS2 * 13) {
+    const int c = tid % kS2, band = tid / kS2;
+    const int x2 = X2 - 3 + c;
+    const int ys = max(a2y + band * 3, 0), ye = min(a2y + min(band * 3 + 3, kS2), h2);
+    if (x2 >= 0 && x2 < w2 && ys < ye) {
+      int col[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * x2 - 2 + l, w1) - a1x;
+      auto H = [&](int r) {
+        const float* p = B1 + (mirror_index(r, h1) - a1y) * kS1S;
+        return (p[col[0]] + p[col[4]]) + 4.f * (p[col[1]] + p[col[3]]) + 6.f * p[col[2]];
+      };
+      float h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
+      for (int y = ys;; ) {
+        const float S = (h0_ + h4_) + 4.f * (h1_ + h3_) + 6.f * h2_;
+        B2[(y - a2y) * kS2S + (x2 - a2x)] = S * (1.f / 256.f);
+        if (++y >= ye) break;
+        h0_ = h2_;
+        h1_ = h3_;
+        h2_ = h4_;
+        h3_ = H(2 * y + 1);
+        h4_ = H(2 * y + 2);
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < 4) {
+    const int x2 = (tid & 1) ? w2 - 1 : 0, y2 = (tid & 2) ? h2 - 1 : 0;
+    if (x2 >= X2 - 3 && x2 < X2 + 35 && y2 >= a2y && y2 < a2y + kS2)
+      B2[(y2 - a2y) * kS2S + (x2 - a2x)] = downscale_px(B1, kS1S, a1x, a1y, w1, h1, x2, y2);
+  }
+  __syncthreads();
+
+  // 4. core outputs, four pixels per thread and store
+  // level 0: 128x128 from the uint8 tile
+#pragma unroll 1
+  for (int q = tid; q < 128 * 32; q += kThreads) {
+    const int y = 4 * Y2 + (q >> 5), x = 4 * X2 + (q & 31) * 4;
+    if (y >= h0 || x >= w0) continue;
+    const int r = y - a0y, c = x - a0x;
+    float v[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c - 4 + 4 * k);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) v[4 * k + b] = (float)((wd >> (8 * b)) & 0xffu);
+    }
+    float col[7][4];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + (r - 3 + k) * kS0W + c);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) col[k][b] = (float)((wd >> (8 * b)) & 0xffu);
+    }
+    float img[4], gx[4], gy[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      img[i] = v[4 + i];
+      float sx = 0.f, sy = 0.f;
+      if (x + i > 2 && x + i < w0 - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) sx = __fmaf_rn(dsp_tap(j), v[4 + i - 3 + j], sx);
+      }
+      if (y > 2 && y < h0 - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) sy = __fmaf_rn(dsp_tap(j), col[j][i], sy);
+      }
+      gx[i] = sx;
+      gy[i] = sy;
+    }
+    const int64_t o = (int64_t)y * L0.pitch + x;
+    if (x + 3 < w0) {
+      *reinterpret_cast<float4*>(L0.img + o) = make_float4(img[0], img[1], img[2], img[3]);
+      *reinterpret_cast<float4*>(L0.gx + o) = make_float4(gx[0], gx[1], gx[2], gx[3]);
+      *reinterpret_cast<float4*>(L0.gy + o) = make_float4(gy[0], gy[1], gy[2], gy[3]);
+    } else {
+      for (int i = 0; i < 4 && x + i < w0; ++i) {
+        L0.img[o + i] = img[i];
+        L0.gx[o + i] = gx[i];
+        L0.gy[o + i] = gy[i];
+      }
+    }
+  }
+  // levels 1 and 2 from their shared-memory tiles
+#pragma unroll 1
+  for (int q = tid; q < 64 * 16 + 32 * 8; q += kThreads) {
+    const bool lev1 = q < 64 * 16;
+    const int qq = lev1 ? q : q - 64 * 16;
+    const Level& L = lev1 ? L1 : L2;
+    const int qpr = lev1 ? 16 : 8;
+    const int y = (lev1 ? 2 * Y2 : Y2) + qq / qpr, x = (lev1 ? 2 * X2 : X2) + (qq % qpr) * 4;
+    if (y >= L.h || x >= L.w) continue;
+    const float* T = lev1 ? B1 : B2;
+    const int stride = lev1 ? kS1S : kS2S;
+    const int r = y - (lev1 ? a1y : a2y), c = x - (lev1 ? a1x : a2x);
+    float v[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 f = *reinterpret_cast<const float4*>(T + r * stride + c - 4 + 4 * k);
+      v[4 * k] = f.x;
+      v[4 * k + 1] = f.y;
+      v[4 * k + 2] = f.z;
+      v[4 * k + 3] = f.w;
+    }
+    float gx[4], gy[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float sx = 0.f, sy = 0.f;
+      if (x + i > 2 && x + i < L.w - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) sx = __fmaf_rn(dsp_tap(j), v[4 + i - 3 + j], sx);
+      }
+      if (y > 2 && y < L.h - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) sy = __fmaf_rn(dsp_tap(j), T[(r - 3 + j) * stride + c + i], sy);
+      }
+      gx[i] = sx;
+      gy[i] = sy;
+    }
+    const int64_t o = (int64_t)y * L.pitch + x;
+    if (x + 3 < L.w) {
+      *reinterpret_cast<float4*>(L.img + o) = make_float4(v[4], v[5], v[6], v[7]);
+      *reinterpret_cast<float4*>(L.gx + o) = make_float4(gx[0], gx[1], gx[2], gx[3]);
+      *reinterpret_cast<float4*>(L.gy + o) = make_float4(gy[0], gy[1], gy[2], gy[3]);
+    } else {
+      for (int i = 0; i < 4 && x + i < L.w; ++i) {
+        L.img[o + i] = v[4 + i];
+        L.gx[o + i] = gx[i];
+        L.gy[o + i] = gy[i];
+      }
+    }
+  }
+}
+
+}  // namespace l012
+
 template <typename InT, int NL>
 cudaError_t set_stage_attr() {
   return cudaFuncSetAttribute(pyramid_stage_kernel<InT, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -181,10 +471,44 @@ cudaError_t launch_stage(const StageBatch& b, int tiles, cudaStream_t s) {
 
 }  // namespace
 
-int stage_tile() { return kT; }
+int stage_tile(bool u8, int nl) { return (u8 && nl == 2) ? l012::kT2 : kT; }
+
+bool encode_frame_tmap(StageJob& job) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<Encode>(fn);
+    looked_up = true;
+  }
+  job.use_tma = 0;
+  if (!encode) return false;
+  // TMA needs a 16-byte aligned base and pitch; frames smaller than the box use plain loads
+  if (((uintptr_t)job.src % 16) != 0 || (job.src_pitch_bytes % 16) != 0) return false;
+  if (job.src_w < l012::kS0W || job.src_h < l012::kS0H) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)job.src_w, (cuuint64_t)job.src_h};
+  const cuuint64_t strides[1] = {(cuuint64_t)job.src_pitch_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)l012::kS0W, (cuuint32_t)l012::kS0H};
+  const cuuint32_t estr[2] = {1, 1};
+  if (encode(&job.tmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(job.src), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  job.use_tma = 1;
+  return true;
+}
 
 cudaError_t pyramid_init() {
   cudaError_t e;
+  if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                l012::kSmem)) != cudaSuccess)
+    return e;
   if ((e = set_stage_attr<uint8_t, 0>()) != cudaSuccess) return e;
   if ((e = set_stage_attr<uint8_t, 1>()) != cudaSuccess) return e;
   if ((e = set_stage_attr<uint8_t, 2>()) != cudaSuccess) return e;
@@ -199,7 +523,9 @@ cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl
     switch (nl) {
       case 0: return launch_stage<uint8_t, 0>(b, tiles, s);
       case 1: return launch_stage<uint8_t, 1>(b, tiles, s);
-      default: return launch_stage<uint8_t, 2>(b, tiles, s);
+      default:
+        l012::pyramid_l012_kernel<<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
+        return cudaGetLastError();
     }
   }
   switch (nl) {
