@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["pyramid", "lk", "select"], default=None,
+                    help="run only this part of the step (warmup + steps launches) for an ncu capture")
     return ap.parse_args()
 
 
@@ -231,6 +233,17 @@ def main():
         frames.append(CameraFrame(img_dev[i], cur_pyr[i], prev_pyr[i], td, counts[i], (0, 0, 0, 0)))
     batch = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)
     attempted = sum(len(t) for t in host_tracks)
+    if args.profile:
+        part_id = {"pyramid": 0, "lk": 1, "select": 2}[args.profile]
+        batch.run_part(0, stream)
+        batch.run_part(1, stream)
+        for _ in range(args.warmup + args.steps):
+            batch.run_part(part_id, stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "launches": args.warmup + args.steps}))
+        batch.close()
+        ctx.close()
+        return
     kernels_per_step = batch.kernel_count()
 
     def restore():

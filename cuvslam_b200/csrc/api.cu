@@ -165,6 +165,7 @@ struct SelectScratch {
 struct fe_context {
   int device = 0;
   SelectScratch sel;
+  int* lk_counter = nullptr;  // persistent LK warps' track counter
   bool debug = false;
 };
 
@@ -304,6 +305,11 @@ int fe_create(int device, fe_context** out) {
   if (!c) return FE_ERR_OUT_OF_MEMORY;
   c->device = device;
   c->debug = getenv("CUVSLAM_FE_DEBUG_MAPS") != nullptr;
+  cudaError_t e = cudaMalloc((void**)&c->lk_counter, 256);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e);
+  }
   *out = c;
   return FE_OK;
 }
@@ -311,6 +317,7 @@ int fe_create(int device, fe_context** out) {
 int fe_destroy(fe_context* ctx) {
   if (!ctx) return FE_ERR_INVALID_ARGUMENT;
   if (ctx->sel.mem) cudaFree(ctx->sel.mem);
+  if (ctx->lk_counter) cudaFree(ctx->lk_counter);
   if (ctx->sel.resp) cudaFree(ctx->sel.resp);
   if (ctx->sel.nms) cudaFree(ctx->sel.nms);
   delete ctx;
@@ -439,6 +446,7 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
   fe::LkLaunch p;
   memset(&p, 0, sizeof(p));
   p.cams = nullptr;
+  p.counter = ctx->lk_counter;
   p.ncams = 1;
   p.total = n;
   p.horizontal = horizontal ? 1 : 0;
@@ -464,27 +472,44 @@ struct fe_batch {
   std::vector<char> has_prev;
   StagePlan plan;
   fe::LkCam* d_lk = nullptr;
+  int* lk_counter = nullptr;
   fe::LkLaunch lk;
   fe::SelectBatch* sel = nullptr;  // heap: large
-  int sel_tiles = 0, bin_cap = 1, final_cap = 1;
+  int sel_tiles = 0, bin_cap = 1, final_cap = 1, touched_words = 0;
   void* sel_mem = nullptr;
   size_t zero_bytes = 0;
   bool any_select = false;
   cudaStream_t cap_stream = nullptr;
+  cudaStream_t side_stream = nullptr;   // second branch of the captured step
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
 
-int enqueue_batch(fe_batch* b, cudaStream_t st) {
+// One frame step.  After the pyramids the step forks: LK on `st` and the selection's response tiles
+// (which do not depend on tracking) on `side` run concurrently; the rest of the selection (burn of
+// the LK survivors, burned cells, quotas, order) joins after both.
+int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side) {
   int rc = run_plan(b->plan, st);
   if (rc) return rc;
-  if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
-  if (b->any_select) {
-    FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
-    FE_CUDA(fe::launch_select(*b->sel, b->sel_tiles, b->bin_cap, b->final_cap, st));
+  if (b->any_select) FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
+  const bool fork = b->any_select && side;
+  if (fork) {
+    FE_CUDA(cudaEventRecord(b->fork_ev, st));
+    FE_CUDA(cudaStreamWaitEvent(side, b->fork_ev, 0));
+    FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, side));
+  } else if (b->any_select) {
+    FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   }
+  if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
+  if (fork) {
+    FE_CUDA(cudaEventRecord(b->join_ev, side));
+    FE_CUDA(cudaStreamWaitEvent(st, b->join_ev, 0));
+  }
+  if (b->any_select)
+    FE_CUDA(fe::launch_select_rest(*b->sel, b->touched_words, b->bin_cap, b->final_cap, st));
   return FE_OK;
 }
 
@@ -549,14 +574,22 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     if (e != cudaSuccess) return fail(cuda_fail(e));
     e = cudaMemcpy(b->d_lk, lk.data(), sizeof(fe::LkCam) * lk.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_fail(e));
+    e = cudaMalloc((void**)&b->lk_counter, 256);
+    if (e != cudaSuccess) return fail(cuda_fail(e));
     b->lk.cams = b->d_lk;
+    b->lk.counter = b->lk_counter;
     b->lk.ncams = (int)lk.size();
     b->lk.total = total;
     b->lk.horizontal = 0;
     b->lk.sampling = sampling;
   }
-  // selection scratch: all cameras' [stats | burn] regions first (one memset), then the rest
-  std::vector<ScratchLayout> lay(ncams);
+  // selection scratch: every camera's [stats | burn | touched] first (one memset per step), then
+  // each camera's cells, sub-tile sums, quotas, kept keys and response/NMS maps
+  struct BatchSel {
+    size_t stats, burn, touched, zero, cell_m, cell_xy, sub_sum, bin_want, q_keys, resp, nms, rest;
+    int touched_words;
+  };
+  std::vector<BatchSel> lay(ncams);
   size_t zero = 0, rest = 0;
   std::vector<int> qcaps(ncams);
   for (int i = 0; i < ncams; ++i) {
@@ -571,9 +604,32 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     b->bin_cap = std::max(b->bin_cap, bc);
     b->final_cap = std::max(b->final_cap, fc);
     qcaps[i] = qc;
-    lay[i] = scratch_layout(c.width, c.height, 0, qc);
-    zero += (size_t)align_up((int64_t)lay[i].burn_bytes, kAlign);
-    rest += lay[i].total - lay[i].cell_m;
+    const int w = c.width, h = c.height;
+    const size_t cells = std::max<size_t>((size_t)(w / 8) * (h / 8), 1);
+    const int vcells = ((w + 7) / 8) * ((h + 7) / 8);
+    BatchSel& L = lay[i];
+    L.touched_words = (vcells + 31) / 32;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+      size_t at = o;
+      o = (size_t)align_up((int64_t)(o + bytes), kAlign);
+      return at;
+    };
+    L.stats = take(16 * sizeof(int));
+    L.burn = take((size_t)((w + 31) / 32) * h * 4);
+    L.touched = take((size_t)L.touched_words * 4);
+    L.zero = o;
+    o = 0;
+    L.cell_m = take(cells * 4);
+    L.cell_xy = take(cells * 8);
+    L.sub_sum = take((size_t)((w + 15) / 16) * ((h + 15) / 16) * 4);
+    L.bin_want = take(128 * 4);
+    L.q_keys = take((size_t)std::max(qc, 1) * 8);
+    L.resp = take((size_t)w * h * 4);
+    L.nms = take((size_t)w * h * 4);
+    L.rest = o;
+    zero += L.zero;
+    rest += L.rest;
     b->any_select = true;
   }
   if (b->any_select) {
@@ -588,19 +644,25 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     for (int i = 0; i < ncams; ++i) {
       const fe_camera_frame& c = cams[i];
       if (c.num_desired <= 0) continue;
-      const ScratchLayout& L = lay[i];
+      const BatchSel& L = lay[i];
       SelectScratch s;
       s.stats = (int*)(zp + L.stats);
       s.burn = (uint32_t*)(zp + L.burn);
-      zp += align_up((int64_t)L.burn_bytes, kAlign);
-      s.cell_m = (float*)(rp + (L.cell_m - L.cell_m));
-      s.cell_xy = (float2*)(rp + (L.cell_xy - L.cell_m));
-      s.sub_sum = (float*)(rp + (L.sub_sum - L.cell_m));
-      s.bin_want = (int*)(rp + (L.bin_want - L.cell_m));
-      s.q_keys = (uint64_t*)(rp + (L.q_keys - L.cell_m));
-      rp += L.total - L.cell_m;
+      uint32_t* touched = (uint32_t*)(zp + L.touched);
+      zp += L.zero;
+      s.cell_m = (float*)(rp + L.cell_m);
+      s.cell_xy = (float2*)(rp + L.cell_xy);
+      s.sub_sum = (float*)(rp + L.sub_sum);
+      s.bin_want = (int*)(rp + L.bin_want);
+      s.q_keys = (uint64_t*)(rp + L.q_keys);
+      s.resp = (float*)(rp + L.resp);
+      s.nms = (float*)(rp + L.nms);
+      rp += L.rest;
       fe::SelectCam& sc = sb.cam[sb.ncams++];
       fill_select_cam(sc, s, b->cur[i], qcaps[i]);
+      sc.touched = touched;
+      sc.touched_begin = b->touched_words;
+      b->touched_words += L.touched_words;
       sc.alive_tracks = b->has_prev[i] ? c.tracks : nullptr;
       sc.n_alive = b->has_prev[i] ? c.n_tracks : 0;
       sc.num_desired = c.num_desired;
@@ -614,10 +676,13 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   }
   // capture the step into a graph
   cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(cuda_fail(e));
   e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return fail(cuda_fail(e));
-  int rc = enqueue_batch(b, b->cap_stream);
+  int rc = enqueue_batch(b, b->cap_stream, b->side_stream);
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(b->cap_stream, &g);
   if (rc) {
@@ -650,7 +715,8 @@ int fe_batch_run_part(fe_batch* b, int part, fe_stream stream) {
     case FE_PART_SELECT:
       if (b->any_select) {
         FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
-        FE_CUDA(fe::launch_select(*b->sel, b->sel_tiles, b->bin_cap, b->final_cap, st));
+        FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
+        FE_CUDA(fe::launch_select_rest(*b->sel, b->touched_words, b->bin_cap, b->final_cap, st));
       }
       return FE_OK;
     default:
@@ -717,7 +783,11 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->side_stream) cudaStreamDestroy(b->side_stream);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+  if (b->join_ev) cudaEventDestroy(b->join_ev);
   if (b->d_lk) cudaFree(b->d_lk);
+  if (b->lk_counter) cudaFree(b->lk_counter);
   if (b->sel_mem) cudaFree(b->sel_mem);
   delete b->sel;
   delete b;

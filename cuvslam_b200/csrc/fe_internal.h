@@ -55,9 +55,11 @@ struct SelectCam {
   float* out_xy;
   int32_t* out_count;
   // scratch (device)
-  float* resp;                  // w*h response (written when debug)
-  float* nms;                   // w*h nms map (written when debug)
+  float* resp;                  // w*h response map (batched path; single camera: debug only)
+  float* nms;                   // w*h NMS map (burned pixels zeroed as the reference's)
   uint32_t* burn;               // ceil(w/32) * h bit mask of burned pixels
+  uint32_t* touched;            // bit per 8x8 cell (ceil(w/8) x ceil(h/8)) reached by a burn window
+  int touched_begin;            // first touched-mask word of this camera in the launch
   float* cell_m;                // (w/8)*(h/8) cell strength (0 = none)
   float2* cell_xy;              // refined position
   float* sub_sum;               // ceil(w/16)*ceil(h/16) sub-tile sums
@@ -77,8 +79,14 @@ struct SelectBatch {
 constexpr int kMaxSelectKeys = 16384;  // shared-memory sort capacity of the selection kernels
 int select_tile();
 cudaError_t select_init();
+// single-camera selection (burn before the response tiles; maps only when b.debug)
 cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap, int final_key_cap,
                           cudaStream_t s);
+// batched selection in two parts: the response tiles (no dependency on tracking; writes the resp and
+// nms maps) and, after tracking, the burn, the burned cells, quotas and order
+cudaError_t launch_select_response(const SelectBatch& b, int total_tiles, cudaStream_t s);
+cudaError_t launch_select_rest(const SelectBatch& b, int touched_words, int bin_key_cap, int final_key_cap,
+                               cudaStream_t s);
 
 // ---------------------------------------------------------------- LK
 struct LkCam {
@@ -91,6 +99,7 @@ struct LkCam {
 
 struct LkLaunch {
   const LkCam* cams;            // device array (batched) or nullptr
+  int* counter;                 // device track counter (persistent warps), or nullptr: one warp per track
   int ncams;
   int total;
   int horizontal;

@@ -2,10 +2,14 @@
 //
 // Launch sequence (all on one stream, every step over all cameras of a batch):
 //   alive_kernel   : compacts alive features (explicit list, or tracks that LK kept) in order,
-//                    burns their 9x9 neighbourhoods into a bit mask and counts them per bin.
+//                    burns their 9x9 neighbourhoods into a bit mask, marks the cells they reach and
+//                    counts them per bin.
 //   tile_kernel    : one CTA per 32x32 tile: structure tensor (separable 7-tap Gaussian), the
-//                    response log(1 + lambda_min), 3x3 NMS, burn mask, one candidate per 8x8 cell
-//                    with sub-pixel refinement, and the 16x16 sub-tile strength sums.
+//                    response log(1 + lambda_min), 3x3 NMS, one candidate per 8x8 cell with
+//                    sub-pixel refinement, and the 16x16 sub-tile strength sums.  Single camera:
+//                    after alive_kernel, with the burn applied.  Batched: before the burn, so it
+//                    does not depend on tracking and runs concurrently with LK; cells_kernel then
+//                    redoes the cells that alive features burned into.
 //   quota_kernel   : per camera: 64 bin sums in a fixed order, the strength total, per-bin quotas.
 //   bin_kernel     : per (bin, camera): filter the bin's candidates (borders, mask), sort by key
 //                    and keep the best `quota` of them.
@@ -94,6 +98,16 @@ __global__ void alive_kernel(const __grid_constant__ SelectBatch b) {
       if (rank < ncell) {
         const int cx = __float2int_rn(x), cy = __float2int_rn(y);
         const int x0 = max(cx - 4, 0), x1 = min(cx + 4, c.w - 1);
+        if (c.touched) {  // batched path: mark the cells this window reaches
+          const int vcw = (c.w + 7) / 8;
+          const int y0 = max(cy - 4, 0), y1 = min(cy + 4, c.h - 1);
+          if (x0 <= x1 && y0 <= y1)
+            for (int ty = y0 / 8; ty <= y1 / 8; ++ty)
+              for (int tx = x0 / 8; tx <= x1 / 8; ++tx) {
+                const int vcell = ty * vcw + tx;
+                atomicOr(&c.touched[vcell >> 5], 1u << (vcell & 31));
+              }
+        }
         for (int yy = max(cy - 4, 0); yy <= min(cy + 4, c.h - 1); ++yy) {
           for (int xx = x0; xx <= x1;) {
             const int wd = xx >> 5;
@@ -127,6 +141,11 @@ __device__ __forceinline__ float find_min_1d(float y1, float y2, float y3) {
   return m;
 }
 
+// kSplit = false: the single-camera path; alive_kernel ran first and the burn applies here, the maps
+//   are written only for debugging.
+// kSplit = true: the batched path (response_kernel); no burn yet, the response and NMS maps are
+//   always written for cells_kernel.
+template <bool kSplit>
 __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constant__ SelectBatch b) {
   __shared__ float2 g[kGradR][kGradR];        // (gx, gy)
   __shared__ float3 hs[kGradR][kRespR];       // horizontal sums (xx, xy, yy)
@@ -186,7 +205,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
     resp[r][q] = __logf(__fadd_rn(e, 1.f));
   }
   __syncthreads();
-  // NMS on the core with clamped neighbours, then the burn mask
+  // NMS on the core with clamped neighbours, then (single-camera path) the burn mask
   const int words = (w + 31) / 32;
   for (int i = threadIdx.x; i < kTile * kTile; i += kTileThreads) {
     const int r = i / kTile, q = i - r * kTile;
@@ -206,16 +225,17 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
         is_max &= resp[yy][xx] <= v;
       }
     float m = is_max ? v : 0.f;
-    if ((__ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31)) & 1u) m = 0.f;
+    if (!kSplit && ((__ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31)) & 1u)) m = 0.f;
     nms[r][q] = m;
-    if (b.debug) {
+    if (kSplit || b.debug) {
       c.resp[(size_t)y * w + x] = v;
       c.nms[(size_t)y * w + x] = m;
     }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  // 16 cells of 8x8, two per warp, with the reference's lane order and tie rule
+  // 16 cells of 8x8, two per warp, with the reference's lane order and tie rule (in the batched
+  // path before the burn: cells_kernel redoes the cells that alive features burn into)
   const int cw = w / 8, ch = h / 8;
   for (int cc = wid; cc < 16; cc += kTileThreads / 32) {
     const int ccx = cc & 3, ccy = cc >> 2;
@@ -278,6 +298,79 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
     const int stx = X / 16 + sj, sty = Y / 16 + si;
     const int sw = (w + 15) / 16, sh = (h + 15) / 16;
     if (lane == 0 && stx < sw && sty < sh) c.sub_sum[sty * sw + stx] = v;
+  }
+}
+
+// ---------------------------------------------------------------- burned cells
+// Redoes the cells that an alive feature's 9x9 window reaches: zero the burned pixels of the NMS map
+// (filter_maximums_kernel, selection_v2.cu:251-277) and take the cell's max/argmax again with the
+// reference's lane order, then refine.  One warp per 32 cells of the touched-cell bit mask.
+__global__ void __launch_bounds__(256) cells_kernel(const __grid_constant__ SelectBatch b, int words_total) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (gw >= words_total) return;
+  int lo = 0, hi = b.ncams - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.cam[mid].touched_begin <= gw) lo = mid; else hi = mid - 1;
+  }
+  const SelectCam& c = b.cam[lo];
+  const int word = gw - c.touched_begin;
+  const int vcw = (c.w + 7) / 8, vch = (c.h + 7) / 8;  // cell grid incl. partial border cells
+  if (word * 32 >= vcw * vch) return;
+  uint32_t bits = c.touched[word];
+  const int w = c.w, h = c.h, cw = w / 8, ch = h / 8;
+  const int bwords = (w + 31) / 32;
+  while (bits) {
+    const int k = __ffs(bits) - 1;
+    bits &= bits - 1;
+    const int vcell = word * 32 + k;
+    if (vcell >= vcw * vch) break;
+    const int cellx = vcell % vcw, celly = vcell / vcw;
+    float m = 0.f;
+    unsigned idx = 0;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int f = lane + 32 * e, dy = f >> 3, dx = f & 7;
+      const int x = cellx * 8 + dx, y = celly * 8 + dy;
+      if (x < w && y < h) {
+        float v = c.nms[(size_t)y * w + x];
+        if ((c.burn[(size_t)y * bwords + (x >> 5)] >> (x & 31)) & 1u) {
+          v = 0.f;
+          c.nms[(size_t)y * w + x] = 0.f;
+        }
+        if (v > m) {
+          m = v;
+          idx = (unsigned)dx | ((unsigned)dy << 16);
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const float m2 = __shfl_down_sync(0xffffffffu, m, d);
+      const unsigned i2 = __shfl_down_sync(0xffffffffu, idx, d);
+      if (m2 > m) {
+        m = m2;
+        idx = i2;
+      }
+    }
+    if (lane == 0 && cellx < cw && celly < ch) {
+      const int cell = celly * cw + cellx;
+      const int px = cellx * 8 + (int)(idx & 0xffffu), py = celly * 8 + (int)(idx >> 16);
+      float out_m = 0.f;
+      float2 pos = make_float2((float)px, (float)py);
+      if (m > (float)1e-2) {
+        out_m = m;
+        if (!(px == 0 || px == w - 1 || py == 0 || py == h - 1)) {
+          const float* r = c.resp + (size_t)py * w + px;
+          const float gc = r[0];
+          pos.x = (float)px + find_min_1d(r[-1], gc, r[1]);
+          pos.y = (float)py + find_min_1d(r[-w], gc, r[w]);
+        }
+      }
+      c.cell_m[cell] = out_m;
+      c.cell_xy[cell] = pos;
+    }
   }
 }
 
@@ -449,15 +542,34 @@ cudaError_t select_init() {
                               (int)(sizeof(uint64_t) * kMaxSelectKeys));
 }
 
-cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap, int final_key_cap,
-                          cudaStream_t s) {
-  if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
-  alive_kernel<<<b.ncams, 256, 0, s>>>(b);
-  tile_kernel<<<total_tiles, kTileThreads, 0, s>>>(b);
+cudaError_t launch_select_response(const SelectBatch& b, int total_tiles, cudaStream_t s) {
+  tile_kernel<true><<<total_tiles, kTileThreads, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+namespace {
+cudaError_t launch_quota_bins_final(const SelectBatch& b, int bin_key_cap, int final_key_cap, cudaStream_t s) {
   quota_kernel<<<b.ncams, 512, 0, s>>>(b);
   bin_kernel<<<dim3(64, b.ncams), 256, sizeof(uint64_t) * bin_key_cap, s>>>(b, bin_key_cap);
   final_kernel<<<b.ncams, 1024, sizeof(uint64_t) * final_key_cap, s>>>(b, final_key_cap);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_select_rest(const SelectBatch& b, int touched_words, int bin_key_cap, int final_key_cap,
+                               cudaStream_t s) {
+  if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
+  alive_kernel<<<b.ncams, 256, 0, s>>>(b);
+  cells_kernel<<<(touched_words + 7) / 8, 256, 0, s>>>(b, touched_words);
+  return launch_quota_bins_final(b, bin_key_cap, final_key_cap, s);
+}
+
+cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap, int final_key_cap,
+                          cudaStream_t s) {
+  if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
+  alive_kernel<<<b.ncams, 256, 0, s>>>(b);
+  tile_kernel<false><<<total_tiles, kTileThreads, 0, s>>>(b);
+  return launch_quota_bins_final(b, bin_key_cap, final_key_cap, s);
 }
 
 }  // namespace fe
