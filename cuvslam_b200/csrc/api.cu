@@ -60,6 +60,8 @@ bool valid_pyramid(const fe_pyramid* p) {
   if (!p || p->levels <= 0 || p->levels > FE_MAX_LEVELS) return false;
   for (int l = 0; l < p->levels; ++l) {
     if (!p->image[l] || !p->grad_x[l] || p->width[l] <= 0 || p->height[l] <= 0) return false;
+    // 16-byte aligned planes (vector loads/stores)
+    if (((uintptr_t)p->image[l] | (uintptr_t)p->grad_x[l] | (uintptr_t)p->grad_y[l]) % 16 != 0) return false;
     if (p->pitch_bytes[l] % 16 != 0 || p->pitch_bytes[l] < (int64_t)p->width[l] * 4) return false;
     if (l > 0 && (p->width[l] != (p->width[l - 1] + 1) / 2 || p->height[l] != (p->height[l - 1] + 1) / 2)) return false;
   }
@@ -267,9 +269,8 @@ void fill_select_cam(fe::SelectCam& c, const SelectScratch& s, const fe_pyramid&
   c.stats = s.stats;
   c.q_keys = s.q_keys;
   c.q_cap = q_cap;
-  const int T = fe::select_tile();
-  c.tiles_x = (c.w + T - 1) / T;
-  c.tiles_y = (c.h + T - 1) / T;
+  c.tiles_x = (c.w + fe::select_tile_w() - 1) / fe::select_tile_w();
+  c.tiles_y = (c.h + fe::select_tile_h() - 1) / fe::select_tile_h();
 }
 
 }  // namespace

@@ -77,7 +77,8 @@ struct SelectBatch {
 };
 
 constexpr int kMaxSelectKeys = 16384;  // shared-memory sort capacity of the selection kernels
-int select_tile();
+int select_tile_w();  // response tile (level-0 pixels)
+int select_tile_h();
 cudaError_t select_init();
 // single-camera selection (burn before the response tiles; maps only when b.debug)
 cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap, int final_key_cap,

@@ -29,7 +29,7 @@ namespace fe {
 
 namespace {
 
-constexpr int kT = 16;        // deepest-level core tile
+constexpr int kT = 8;         // deepest-level core tile (generic stages: small levels, many CTAs)
 constexpr int kThreads = 256;
 
 __host__ __device__ constexpr int region_size(int nl, int k) {

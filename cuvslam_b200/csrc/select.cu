@@ -4,7 +4,7 @@
 //   alive_kernel   : compacts alive features (explicit list, or tracks that LK kept) in order,
 //                    burns their 9x9 neighbourhoods into a bit mask, marks the cells they reach and
 //                    counts them per bin.
-//   tile_kernel    : one CTA per 32x32 tile: structure tensor (separable 7-tap Gaussian), the
+//   tile_kernel    : one CTA per 64x32 tile: structure tensor (separable 7-tap Gaussian), the
 //                    response log(1 + lambda_min), 3x3 NMS, one candidate per 8x8 cell with
 //                    sub-pixel refinement, and the 16x16 sub-tile strength sums.  Single camera:
 //                    after alive_kernel, with the burn applied.  Batched: before the burn, so it
@@ -37,10 +37,6 @@ namespace fe {
 
 namespace {
 
-constexpr int kTile = 32;            // response tile
-constexpr int kTileThreads = 256;
-constexpr int kRespR = kTile + 2;    // response region (NMS halo 1)
-constexpr int kGradR = kTile + 8;    // gradient region (tensor halo 3 + NMS halo 1)
 
 __device__ __forceinline__ uint64_t make_key(float m, int cell) {
   // strength descending, then cell ascending; m > 0 so its bits order like the value
@@ -141,17 +137,40 @@ __device__ __forceinline__ float find_min_1d(float y1, float y2, float y3) {
   return m;
 }
 
+// One CTA per 64x32 tile of level 0 (256 threads).  Shared memory holds (gx, gy) on the tile plus
+// a 4-pixel halo (tensor taps 3 + NMS 1), the horizontal 7-tap sums as three planes, and later the
+// response (aliasing the gradients) and the NMS values (aliasing the sums).
 // kSplit = false: the single-camera path; alive_kernel ran first and the burn applies here, the maps
 //   are written only for debugging.
-// kSplit = true: the batched path (response_kernel); no burn yet, the response and NMS maps are
-//   always written for cells_kernel.
+// kSplit = true: the batched path; no burn yet, the response and NMS maps are always written for
+//   cells_kernel.
+namespace tile {
+constexpr int TW = 64, TH = 32;              // core
+constexpr int RW = TW + 2;                   // response region width (height TH + 2)
+constexpr int GW = TW + 10, GH = TH + 8;     // gradients loaded (two spare columns for 4-wide quads)
+constexpr int GS = 76;                       // row stride of the gradient planes (16-byte rows)
+constexpr int HS = 68;                       // row stride of the horizontal sums (>= RW, 4-aligned)
+constexpr int RS = 68;                       // row stride of the response
+constexpr int kThreads = 256;
+constexpr int kOffH = 0;                                     // 3 planes [GH][HS]
+constexpr int kOffG = kOffH + 3 * GH * HS * 4;               // 2 planes [GH][GS]
+constexpr int kSmem = kOffG + 2 * GH * GS * 4;
+}  // namespace tile
+
+__device__ __forceinline__ float2 dup(float c) { return make_float2(c, c); }
+
 template <bool kSplit>
-__global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constant__ SelectBatch b) {
-  __shared__ float2 g[kGradR][kGradR];        // (gx, gy)
-  __shared__ float3 hs[kGradR][kRespR];       // horizontal sums (xx, xy, yy)
-  __shared__ float resp[kRespR][kRespR + 1];
-  __shared__ float nms[kTile][kTile + 1];
-  __shared__ float part[4][8];
+__global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_constant__ SelectBatch b) {
+  using namespace tile;
+  extern __shared__ __align__(16) unsigned char tsm[];
+  float* hxx = reinterpret_cast<float*>(tsm + kOffH);
+  float* hxy = hxx + GH * HS;
+  float* hyy = hxy + GH * HS;
+  float* gxs = reinterpret_cast<float*>(tsm + kOffG);
+  float* gys = gxs + GH * GS;
+  float* resp = reinterpret_cast<float*>(tsm + kOffG);  // after the horizontal pass
+  float* nms = hxx;                                      // after the vertical pass
+  __shared__ float part[8][8];
 
   int lo = 0, hi = b.ncams - 1;
   while (lo < hi) {
@@ -160,85 +179,132 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
   }
   const SelectCam& c = b.cam[lo];
   const int t = (int)blockIdx.x - c.tile_begin;
-  const int X = (t % c.tiles_x) * kTile, Y = (t / c.tiles_x) * kTile;
+  const int X = (t % c.tiles_x) * TW, Y = (t / c.tiles_x) * TH;
   const int w = c.w, h = c.h;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
-  // gradients on [X-4, X+36) x [Y-4, Y+36), mirrored like the reference's tile loader
-  for (int i = threadIdx.x; i < kGradR * kGradR; i += kTileThreads) {
-    const int r = i / kGradR, q = i - r * kGradR;
-    const int yy = mirror_index(Y - 4 + r, h), xx = mirror_index(X - 4 + q, w);
-    // mirror once more for tiny images (the reference's texture clamps there)
-    const int ys = min(max(yy, 0), h - 1), xs = min(max(xx, 0), w - 1);
-    g[r][q] = make_float2(__ldg(c.gx + (size_t)ys * c.pitch + xs), __ldg(c.gy + (size_t)ys * c.pitch + xs));
+  // A. gradients on [X-4, X+70) x [Y-4, Y+36), mirrored like the reference's tile loader (and
+  //    clamped, as its texture does, for images smaller than the mirror span)
+  if (X >= 4 && Y >= 4 && X - 4 + GW <= w && Y - 4 + GH <= h) {
+    // interior tile: 16-byte loads (X - 4 is a multiple of 4 and rows are 16-byte aligned)
+    for (int i = tid; i < GH * 19 * 2; i += kThreads) {
+      const int plane = i / (GH * 19), k = i - plane * (GH * 19);
+      const int r = k / 19, v = k - r * 19;
+      const float* src = (plane ? c.gy : c.gx) + (size_t)(Y - 4 + r) * c.pitch + (X - 4);
+      float* dst = (plane ? gys : gxs) + r * GS;
+      if (v < 18) {
+        *reinterpret_cast<float4*>(dst + 4 * v) = __ldg(reinterpret_cast<const float4*>(src) + v);
+      } else {
+        *reinterpret_cast<float2*>(dst + 72) = __ldg(reinterpret_cast<const float2*>(src + 72));
+      }
+    }
+  } else {
+    for (int i = tid; i < GH * GW; i += kThreads) {
+      const int r = i / GW, q = i - r * GW;
+      const int yy = min(max(mirror_index(Y - 4 + r, h), 0), h - 1);
+      const int xx = min(max(mirror_index(X - 4 + q, w), 0), w - 1);
+      const size_t o = (size_t)yy * c.pitch + xx;
+      gxs[r * GS + q] = __ldg(c.gx + o);
+      gys[r * GS + q] = __ldg(c.gy + o);
+    }
   }
   __syncthreads();
-  // horizontal 7-tap: xx += (c*gx)*gx as in gftt.cu:131-137
-  for (int i = threadIdx.x; i < kGradR * kRespR; i += kTileThreads) {
-    const int r = i / kRespR, q = i - r * kRespR;
-    float xx = 0.f, xy = 0.f, yy = 0.f;
+
+  // B. horizontal 7-tap sums for 40 rows x 68 columns, two column pairs per thread with packed
+  //    FP32x2 arithmetic: xx += (c_j gx) gx, xy += (c_j gx) gy, yy += (c_j gy) gy (gftt.cu:131-137)
+  for (int qd = tid; qd < GH * (HS / 4); qd += kThreads) {
+    const int r = qd / (HS / 4), q0 = (qd - r * (HS / 4)) * 4;
+    float2 ax[5], ay[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      ax[m] = *reinterpret_cast<const float2*>(gxs + r * GS + q0 + 2 * m);
+      ay[m] = *reinterpret_cast<const float2*>(gys + r * GS + q0 + 2 * m);
+    }
+    // pairs (v[k], v[k+1]) of columns q0 + k, k = 0..8
+    auto px = [&](int k) { return (k & 1) ? make_float2(ax[k >> 1].y, ax[(k >> 1) + 1].x) : ax[k >> 1]; };
+    auto py = [&](int k) { return (k & 1) ? make_float2(ay[k >> 1].y, ay[(k >> 1) + 1].x) : ay[k >> 1]; };
+    float2 xx0 = dup(0.f), xy0 = dup(0.f), yy0 = dup(0.f), xx1 = dup(0.f), xy1 = dup(0.f), yy1 = dup(0.f);
 #pragma unroll
     for (int j = 0; j < 7; ++j) {
-      const float2 v = g[r][q + j];
-      const float cx = gauss7(j) * v.x, cy = gauss7(j) * v.y;
-      xx = __fmaf_rn(cx, v.x, xx);
-      xy = __fmaf_rn(cx, v.y, xy);
-      yy = __fmaf_rn(cy, v.y, yy);
+      const float2 cj = dup(gauss7(j));
+      const float2 gx0 = px(j), gy0 = py(j), gx1 = px(j + 2), gy1 = py(j + 2);
+      const float2 cx0 = __fmul2_rn(cj, gx0), cy0 = __fmul2_rn(cj, gy0);
+      const float2 cx1 = __fmul2_rn(cj, gx1), cy1 = __fmul2_rn(cj, gy1);
+      xx0 = __ffma2_rn(cx0, gx0, xx0);
+      xy0 = __ffma2_rn(cx0, gy0, xy0);
+      yy0 = __ffma2_rn(cy0, gy0, yy0);
+      xx1 = __ffma2_rn(cx1, gx1, xx1);
+      xy1 = __ffma2_rn(cx1, gy1, xy1);
+      yy1 = __ffma2_rn(cy1, gy1, yy1);
     }
-    hs[r][q] = make_float3(xx, xy, yy);
+    *reinterpret_cast<float4*>(hxx + r * HS + q0) = make_float4(xx0.x, xx0.y, xx1.x, xx1.y);
+    *reinterpret_cast<float4*>(hxy + r * HS + q0) = make_float4(xy0.x, xy0.y, xy1.x, xy1.y);
+    *reinterpret_cast<float4*>(hyy + r * HS + q0) = make_float4(yy0.x, yy0.y, yy1.x, yy1.y);
   }
   __syncthreads();
-  // vertical 7-tap and the measure (gftt.cu:61-66, 148-160)
-  for (int i = threadIdx.x; i < kRespR * kRespR; i += kTileThreads) {
-    const int r = i / kRespR, q = i - r * kRespR;
-    float xx = 0.f, xy = 0.f, yy = 0.f;
+
+  // C. vertical 7-tap and the measure (gftt.cu:61-66, 148-160) for 34 rows x 66 columns, one
+  //    column pair per work item, packed FP32x2 arithmetic
+  for (int it = tid; it < (TH + 2) * (RW / 2); it += kThreads) {
+    const int r = it / (RW / 2), q = (it - r * (RW / 2)) * 2;
+    float2 xx = dup(0.f), xy = dup(0.f), yy = dup(0.f);
 #pragma unroll
     for (int j = 0; j < 7; ++j) {
-      const float3 v = hs[r + j][q];
-      xx = __fmaf_rn(gauss7(j), v.x, xx);
-      xy = __fmaf_rn(gauss7(j), v.y, xy);
-      yy = __fmaf_rn(gauss7(j), v.z, yy);
+      const float2 cj = dup(gauss7(j));
+      xx = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hxx + (r + j) * HS + q), xx);
+      xy = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hxy + (r + j) * HS + q), xy);
+      yy = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hyy + (r + j) * HS + q), yy);
     }
-    const float d = __fsub_rn(xx, yy);
-    const float D = __fsqrt_rn(__fmaf_rn(__fmul_rn(4.f, xy), xy, __fmul_rn(d, d)));
-    const float T = __fadd_rn(xx, yy);
-    const float e = __fmul_rn(__fsub_rn(T, D), 0.5f);
-    resp[r][q] = __logf(__fadd_rn(e, 1.f));
+    const float2 d = __fadd2_rn(xx, make_float2(-yy.x, -yy.y));
+    const float2 D2 = __ffma2_rn(__fmul2_rn(dup(4.f), xy), xy, __fmul2_rn(d, d));
+    const float2 T = __fadd2_rn(xx, yy);
+    const float2 D = make_float2(__fsqrt_rn(D2.x), __fsqrt_rn(D2.y));
+    const float2 e1 = __fadd2_rn(__fmul2_rn(__fadd2_rn(T, make_float2(-D.x, -D.y)), dup(0.5f)), dup(1.f));
+    *reinterpret_cast<float2*>(resp + r * RS + q) = make_float2(__logf(e1.x), __logf(e1.y));
   }
   __syncthreads();
-  // NMS on the core with clamped neighbours, then (single-camera path) the burn mask
+
+  // D. NMS on the core with clamped neighbours, then (single-camera path) the burn mask
   const int words = (w + 31) / 32;
-  for (int i = threadIdx.x; i < kTile * kTile; i += kTileThreads) {
-    const int r = i / kTile, q = i - r * kTile;
+  for (int i = tid; i < TW * TH; i += kThreads) {
+    const int r = i / TW, q = i - r * TW;
     const int x = X + q, y = Y + r;
     if (x >= w || y >= h) {
-      nms[r][q] = 0.f;
+      nms[r * TW + q] = 0.f;
       continue;
     }
-    const float v = resp[r + 1][q + 1];
-    bool is_max = true;
+    const float* rp = resp + (r + 1) * RS + (q + 1);
+    const float v = rp[0];
+    bool is_max;
+    if (x > 0 && y > 0 && x < w - 1 && y < h - 1) {
+      is_max = rp[-RS - 1] <= v && rp[-RS] <= v && rp[-RS + 1] <= v && rp[-1] <= v && rp[1] <= v &&
+               rp[RS - 1] <= v && rp[RS] <= v && rp[RS + 1] <= v;
+    } else {
+      is_max = true;
 #pragma unroll
-    for (int dy = -1; dy <= 1; ++dy)
+      for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (!dx && !dy) continue;
-        const int yy = min(max(y + dy, 0), h - 1) - Y + 1, xx = min(max(x + dx, 0), w - 1) - X + 1;
-        is_max &= resp[yy][xx] <= v;
-      }
+        for (int dx = -1; dx <= 1; ++dx) {
+          if (!dx && !dy) continue;
+          const int yy = min(max(y + dy, 0), h - 1) - Y + 1, xx = min(max(x + dx, 0), w - 1) - X + 1;
+          is_max &= resp[yy * RS + xx] <= v;
+        }
+    }
     float m = is_max ? v : 0.f;
     if (!kSplit && ((__ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31)) & 1u)) m = 0.f;
-    nms[r][q] = m;
+    nms[r * TW + q] = m;
     if (kSplit || b.debug) {
       c.resp[(size_t)y * w + x] = v;
       c.nms[(size_t)y * w + x] = m;
     }
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  // 16 cells of 8x8, two per warp, with the reference's lane order and tie rule (in the batched
-  // path before the burn: cells_kernel redoes the cells that alive features burn into)
+
+  // E. 32 cells of 8x8, four per warp, with the reference's lane order and tie rule (in the
+  //    batched path before the burn: cells_kernel redoes the cells that alive features reach)
   const int cw = w / 8, ch = h / 8;
-  for (int cc = wid; cc < 16; cc += kTileThreads / 32) {
-    const int ccx = cc & 3, ccy = cc >> 2;
+  for (int cc = wid; cc < 32; cc += kThreads / 32) {
+    const int ccx = cc & 7, ccy = cc >> 3;
     const int cellx = X / 8 + ccx, celly = Y / 8 + ccy;
     if (cellx >= cw || celly >= ch) continue;  // warp-uniform
     float m = 0.f;
@@ -246,7 +312,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int f = lane + 32 * e, dy = f >> 3, dx = f & 7;
-      const float v = nms[ccy * 8 + dy][ccx * 8 + dx];
+      const float v = nms[(ccy * 8 + dy) * TW + ccx * 8 + dx];
       if (v > m) {
         m = v;
         idx = (unsigned)dx | ((unsigned)dy << 16);
@@ -269,32 +335,34 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(const __grid_constan
       if (m > (float)1e-2) {
         out_m = m;
         if (!(px == 0 || px == w - 1 || py == 0 || py == h - 1)) {
-          const int lr = py - Y + 1, lc = px - X + 1;
-          const float gc = resp[lr][lc];
-          pos.x = (float)px + find_min_1d(resp[lr][lc - 1], gc, resp[lr][lc + 1]);
-          pos.y = (float)py + find_min_1d(resp[lr - 1][lc], gc, resp[lr + 1][lc]);
+          const float* rp = resp + (py - Y + 1) * RS + (px - X + 1);
+          const float gc = rp[0];
+          pos.x = (float)px + find_min_1d(rp[-1], gc, rp[1]);
+          pos.y = (float)py + find_min_1d(rp[-RS], gc, rp[RS]);
         }
       }
       c.cell_m[cell] = out_m;
       c.cell_xy[cell] = pos;
     }
   }
-  // 16x16 sub-tile sums of the response (accumulateGFTT_kernel's reduction order)
+
+  // F. 16x16 sub-tile sums of the response (accumulateGFTT_kernel's reduction order): warp w sums
+  //    rows 2w, 2w+1 of each of the 8 sub-tiles, then a 3-level butterfly over the 8 warp sums
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    const int si = s >> 1, sj = s & 1;
+  for (int s8 = 0; s8 < 8; ++s8) {
+    const int si = s8 >> 2, sj = s8 & 3;
     const int ty = 2 * wid + (lane >> 4), tx = lane & 15;
     const int x = X + sj * 16 + tx, y = Y + si * 16 + ty;
-    const float v = (x < w && y < h) ? resp[si * 16 + ty + 1][sj * 16 + tx + 1] : 0.f;
+    const float v = (x < w && y < h) ? resp[(si * 16 + ty + 1) * RS + sj * 16 + tx + 1] : 0.f;
     const float ws = warp_sum(v);
-    if (lane == 0) part[s][wid] = ws;
+    if (lane == 0) part[s8][wid] = ws;
   }
   __syncthreads();
-  if (wid < 4) {
+  {
     float v = lane < 8 ? part[wid][lane] : 0.f;
 #pragma unroll
     for (int m = 1; m < 8; m <<= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
-    const int si = wid >> 1, sj = wid & 1;
+    const int si = wid >> 2, sj = wid & 3;
     const int stx = X / 16 + sj, sty = Y / 16 + si;
     const int sw = (w + 15) / 16, sh = (h + 15) / 16;
     if (lane == 0 && stx < sw && sty < sh) c.sub_sum[sty * sw + stx] = v;
@@ -532,10 +600,15 @@ __global__ void final_kernel(const __grid_constant__ SelectBatch b, int key_cap)
 
 }  // namespace
 
-int select_tile() { return kTile; }
+int select_tile_w() { return tile::TW; }
+int select_tile_h() { return tile::TH; }
 
 cudaError_t select_init() {
-  cudaError_t e = cudaFuncSetAttribute(bin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::kSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::kSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(bin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(uint64_t) * kMaxSelectKeys));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -543,7 +616,7 @@ cudaError_t select_init() {
 }
 
 cudaError_t launch_select_response(const SelectBatch& b, int total_tiles, cudaStream_t s) {
-  tile_kernel<true><<<total_tiles, kTileThreads, 0, s>>>(b);
+  tile_kernel<true><<<total_tiles, tile::kThreads, tile::kSmem, s>>>(b);
   return cudaGetLastError();
 }
 
@@ -568,7 +641,7 @@ cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap
                           cudaStream_t s) {
   if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
   alive_kernel<<<b.ncams, 256, 0, s>>>(b);
-  tile_kernel<false><<<total_tiles, kTileThreads, 0, s>>>(b);
+  tile_kernel<false><<<total_tiles, tile::kThreads, tile::kSmem, s>>>(b);
   return launch_quota_bins_final(b, bin_key_cap, final_key_cap, s);
 }
 

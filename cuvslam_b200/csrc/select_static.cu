@@ -157,9 +157,8 @@ extern "C" FE_API int fe_select_noalloc(const fe_pyramid* pyr, int border_top, i
   c.bin_want = (int*)(s + L.bin_want);
   c.q_keys = (uint64_t*)(s + L.q_keys);
   c.q_cap = q_cap;
-  const int T = fe::select_tile();
-  c.tiles_x = (w + T - 1) / T;
-  c.tiles_y = (h + T - 1) / T;
+  c.tiles_x = (w + fe::select_tile_w() - 1) / fe::select_tile_w();
+  c.tiles_y = (h + fe::select_tile_h() - 1) / fe::select_tile_h();
   c.tile_begin = 0;
   if (fe::launch_select(b, c.tiles_x * c.tiles_y, bin_cap, final_cap, st) != cudaSuccess) return FE_ERR_CUDA;
   return FE_OK;
