@@ -587,7 +587,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   // selection scratch: every camera's [stats | burn | touched] first (one memset per step), then
   // each camera's cells, sub-tile sums, quotas, kept keys and response/NMS maps
   struct BatchSel {
-    size_t stats, burn, touched, zero, cell_m, cell_xy, sub_sum, bin_want, q_keys, resp, nms, rest;
+    size_t stats, burn, touched, zero, cell_m, cell_xy, sub_sum, bin_want, q_keys, resp, rest;
     int touched_words;
   };
   std::vector<BatchSel> lay(ncams);
@@ -626,8 +626,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     L.sub_sum = take((size_t)((w + 15) / 16) * ((h + 15) / 16) * 4);
     L.bin_want = take(128 * 4);
     L.q_keys = take((size_t)std::max(qc, 1) * 8);
-    L.resp = take((size_t)w * h * 4);
-    L.nms = take((size_t)w * h * 4);
+    L.resp = take((size_t)w * h * 4);  // the response map that cells_kernel reads
     L.rest = o;
     zero += L.zero;
     rest += L.rest;
@@ -657,7 +656,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
       s.bin_want = (int*)(rp + L.bin_want);
       s.q_keys = (uint64_t*)(rp + L.q_keys);
       s.resp = (float*)(rp + L.resp);
-      s.nms = (float*)(rp + L.nms);
+      s.nms = nullptr;
       rp += L.rest;
       fe::SelectCam& sc = sb.cam[sb.ncams++];
       fill_select_cam(sc, s, b->cur[i], qcaps[i]);

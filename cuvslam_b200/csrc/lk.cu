@@ -128,14 +128,16 @@ __device__ __forceinline__ float sample(const float* win, int stride, const Tap&
   return __fmaf_rn(t.w10, __fsub_rn(bot, top), top);
 }
 
-// Stage the n x n texels starting at (bx, by), clamped to the image (the texture's clamp mode).
+// Stage the n x n texels starting at (bx, by), clamped to the image (the texture's clamp mode), as
+// asynchronous copies; the caller waits (cp_async_wait_all) and then __syncwarp()s.
 template <int N, int S>
 __device__ __forceinline__ void stage(float* win, const float* img, int pitch, int w, int h, int bx, int by,
                                       int lane) {
+#pragma unroll
   for (int i = lane; i < N * N; i += 32) {
     const int r = i / N, c = i - r * N;
     const int y = min(max(by + r, 0), h - 1), x = min(max(bx + c, 0), w - 1);
-    win[r * S + c] = __ldg(img + (size_t)y * pitch + x);
+    cp_async4(win + r * S + c, img + (size_t)y * pitch + x);
   }
 }
 
@@ -204,6 +206,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
       stage<kPW, kPS>(sm.img, PL.img, PL.pitch, PL.w, PL.h, bx, by, lane);
       stage<kPW, kPS>(sm.gx, PL.gx, PL.pitch, PL.w, PL.h, bx, by, lane);
       if (!HORIZ) stage<kPW, kPS>(sm.gy, PL.gy, PL.pitch, PL.w, PL.h, bx, by, lane);
+      cp_async_wait_all();
       __syncwarp();
       const TapSet ts = make_taps<SAMPLING>(xmin, ymin, bx, by, kPS, lane);
       float gxp[kNE], gyp[kNE], p1[kNE];
@@ -276,6 +279,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           wby = nby - 2;
           __syncwarp();
           stage<kCW, kCS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+          cp_async_wait_all();
           __syncwarp();
         }
         const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCS, lane);

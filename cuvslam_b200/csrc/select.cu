@@ -37,7 +37,6 @@ namespace fe {
 
 namespace {
 
-
 __device__ __forceinline__ uint64_t make_key(float m, int cell) {
   // strength descending, then cell ascending; m > 0 so its bits order like the value
   return ((uint64_t)(~__float_as_uint(m)) << 32) | (uint32_t)cell;
@@ -142,7 +141,7 @@ __device__ __forceinline__ float find_min_1d(float y1, float y2, float y3) {
 // response (aliasing the gradients) and the NMS values (aliasing the sums).
 // kSplit = false: the single-camera path; alive_kernel ran first and the burn applies here, the maps
 //   are written only for debugging.
-// kSplit = true: the batched path; no burn yet, the response and NMS maps are always written for
+// kSplit = true: the batched path; no burn yet, the response map is always written for
 //   cells_kernel.
 namespace tile {
 constexpr int TW = 64, TH = 32;              // core
@@ -158,6 +157,7 @@ constexpr int kSmem = kOffG + 2 * GH * GS * 4;
 }  // namespace tile
 
 __device__ __forceinline__ float2 dup(float c) { return make_float2(c, c); }
+
 
 template <bool kSplit>
 __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_constant__ SelectBatch b) {
@@ -184,19 +184,18 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
   // A. gradients on [X-4, X+70) x [Y-4, Y+36), mirrored like the reference's tile loader (and
-  //    clamped, as its texture does, for images smaller than the mirror span)
+  //    clamped, as its texture does, for images smaller than the mirror span).  Every copy is an
+  //    asynchronous global->shared copy issued before the one wait, so a thread has all of its
+  //    loads in flight at once.
   if (X >= 4 && Y >= 4 && X - 4 + GW <= w && Y - 4 + GH <= h) {
-    // interior tile: 16-byte loads (X - 4 is a multiple of 4 and rows are 16-byte aligned)
+    // interior tile: 16-byte copies (X - 4 is a multiple of 4 and rows are 16-byte aligned)
     for (int i = tid; i < GH * 19 * 2; i += kThreads) {
       const int plane = i / (GH * 19), k = i - plane * (GH * 19);
       const int r = k / 19, v = k - r * 19;
       const float* src = (plane ? c.gy : c.gx) + (size_t)(Y - 4 + r) * c.pitch + (X - 4);
       float* dst = (plane ? gys : gxs) + r * GS;
-      if (v < 18) {
-        *reinterpret_cast<float4*>(dst + 4 * v) = __ldg(reinterpret_cast<const float4*>(src) + v);
-      } else {
-        *reinterpret_cast<float2*>(dst + 72) = __ldg(reinterpret_cast<const float2*>(src + 72));
-      }
+      if (v < 18) cp_async16(dst + 4 * v, src + 4 * v);
+      else cp_async8(dst + 72, src + 72);
     }
   } else {
     for (int i = tid; i < GH * GW; i += kThreads) {
@@ -204,10 +203,11 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
       const int yy = min(max(mirror_index(Y - 4 + r, h), 0), h - 1);
       const int xx = min(max(mirror_index(X - 4 + q, w), 0), w - 1);
       const size_t o = (size_t)yy * c.pitch + xx;
-      gxs[r * GS + q] = __ldg(c.gx + o);
-      gys[r * GS + q] = __ldg(c.gy + o);
+      cp_async4(gxs + r * GS + q, c.gx + o);
+      cp_async4(gys + r * GS + q, c.gy + o);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
 
   // B. horizontal 7-tap sums for 40 rows x 68 columns, two column pairs per thread with packed
@@ -293,10 +293,8 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
     float m = is_max ? v : 0.f;
     if (!kSplit && ((__ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31)) & 1u)) m = 0.f;
     nms[r * TW + q] = m;
-    if (kSplit || b.debug) {
-      c.resp[(size_t)y * w + x] = v;
-      c.nms[(size_t)y * w + x] = m;
-    }
+    if (kSplit || b.debug) c.resp[(size_t)y * w + x] = v;
+    if (!kSplit && b.debug) c.nms[(size_t)y * w + x] = m;
   }
   __syncthreads();
 
@@ -370,9 +368,10 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
 }
 
 // ---------------------------------------------------------------- burned cells
-// Redoes the cells that an alive feature's 9x9 window reaches: zero the burned pixels of the NMS map
-// (filter_maximums_kernel, selection_v2.cu:251-277) and take the cell's max/argmax again with the
-// reference's lane order, then refine.  One warp per 32 cells of the touched-cell bit mask.
+// Redoes the cells that an alive feature's 9x9 window reaches: NMS again from the response map,
+// burned pixels zeroed (filter_maximums_kernel, selection_v2.cu:251-277), the cell's max/argmax
+// again with the reference's lane order, then the refinement.  One warp per 32 cells of the
+// touched-cell bit mask.
 __global__ void __launch_bounds__(256) cells_kernel(const __grid_constant__ SelectBatch b, int words_total) {
   const int lane = threadIdx.x & 31;
   const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -401,13 +400,18 @@ __global__ void __launch_bounds__(256) cells_kernel(const __grid_constant__ Sele
     for (int e = 0; e < 2; ++e) {
       const int f = lane + 32 * e, dy = f >> 3, dx = f & 7;
       const int x = cellx * 8 + dx, y = celly * 8 + dy;
-      if (x < w && y < h) {
-        float v = c.nms[(size_t)y * w + x];
-        if ((c.burn[(size_t)y * bwords + (x >> 5)] >> (x & 31)) & 1u) {
-          v = 0.f;
-          c.nms[(size_t)y * w + x] = 0.f;
-        }
-        if (v > m) {
+      if (x < w && y < h && !((c.burn[(size_t)y * bwords + (x >> 5)] >> (x & 31)) & 1u)) {
+        const float v = c.resp[(size_t)y * w + x];
+        bool is_max = true;
+#pragma unroll
+        for (int ny = -1; ny <= 1; ++ny)
+#pragma unroll
+          for (int nx = -1; nx <= 1; ++nx) {
+            if (!nx && !ny) continue;
+            const int yy = min(max(y + ny, 0), h - 1), xx = min(max(x + nx, 0), w - 1);
+            is_max &= c.resp[(size_t)yy * w + xx] <= v;
+          }
+        if (is_max && v > m) {
           m = v;
           idx = (unsigned)dx | ((unsigned)dy << 16);
         }
