@@ -45,6 +45,31 @@ class FeCameraFrame(ctypes.Structure):
     ]
 
 
+class FeAdjointJob(ctypes.Structure):
+    _fields_ = [
+        ("prev", ctypes.POINTER(FePyramid)),
+        ("cur", ctypes.POINTER(FePyramid)),
+        ("tracks_in", ctypes.c_void_p),
+        ("tracks_out", ctypes.c_void_p),
+        ("n_tracks", ctypes.c_int32),
+        ("grad_xy", ctypes.c_void_p),
+        ("grad_prev", ctypes.c_void_p),
+        ("grad_prev_pitch_bytes", ctypes.c_int64),
+        ("grad_cur", ctypes.c_void_p),
+        ("grad_cur_pitch_bytes", ctypes.c_int64),
+        ("grad_track", ctypes.c_void_p),
+        ("grad_offset", ctypes.c_void_p),
+        ("prev_image", ctypes.c_void_p),
+        ("cur_image", ctypes.c_void_p),
+        ("image_pitch_bytes", ctypes.c_int64),
+        ("image_scale", ctypes.c_float),
+    ]
+
+
+FE_ADJOINT_IMPLICIT = 0
+FE_ADJOINT_UNROLLED = 1
+
+
 class FeError(RuntimeError):
     pass
 
@@ -76,6 +101,17 @@ _SIGS = {
     "fe_batch_run_part": (_I, [_P, _I, _P]),
     "fe_batch_kernel_count": (_I, [_P]),
     "fe_batch_destroy": (_I, [_P]),
+    "fe_adjoint_create": (_I, [_P, ctypes.POINTER(FeAdjointJob), _I, _I, _I, ctypes.c_float, ctypes.POINTER(_P)]),
+    "fe_adjoint_build_pyramids": (_I, [_P, _P]),
+    "fe_adjoint_forward": (_I, [_P, _P]),
+    "fe_adjoint_backward": (_I, [_P, _P]),
+    "fe_adjoint_kernel_count": (_I, [_P, _I]),
+    "fe_adjoint_dropped": (_I, [_P, _P, _P]),
+    "fe_adjoint_destroy": (_I, [_P]),
+    "fe_track_diff": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _P, _I, _I, _I,
+                           ctypes.c_float, _P]),
+    "fe_track_backward": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _P, _I, _I, _I,
+                               ctypes.c_float, _P, _P, _I64, _P, _I64, _P, _P, _P]),
 }
 
 EXPORTED = tuple(_SIGS)

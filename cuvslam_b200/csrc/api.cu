@@ -96,7 +96,8 @@ using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
 // Appends the stages of one camera's pyramid build: stage 0 reads the frame (uint8 or FP32) and
 // writes levels 0..2; each later stage reads the deepest level of the previous one and writes up
 // to two more.
-int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan) {
+int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan,
+                 float scale = 1.f) {
   const fe::Pyr pyr = to_pyr(p);
   int s = 0;
   for (int stage = 0;; ++stage) {
@@ -107,6 +108,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.src = stage == 0 ? src : (const void*)pyr.lv[s].img;
     job.src_pitch_bytes = stage == 0 ? src_pitch : (int64_t)pyr.lv[s].pitch * 4;
     job.write_level0 = stage == 0 ? 1 : 0;
+    job.scale = stage == 0 && !u8 ? scale : 1.f;
     job.src_w = pyr.lv[s].w;
     job.src_h = pyr.lv[s].h;
     for (int k = 0; k <= nl; ++k) job.out[k] = pyr.lv[s + k];
@@ -302,6 +304,7 @@ int fe_create(int device, fe_context** out) {
   FE_CUDA(cudaSetDevice(device));
   FE_CUDA(fe::pyramid_init());
   FE_CUDA(fe::select_init());
+  FE_CUDA(fe::adjoint_init());
   fe_context* c = new (std::nothrow) fe_context;
   if (!c) return FE_ERR_OUT_OF_MEMORY;
   c->device = device;
@@ -792,6 +795,373 @@ int fe_batch_destroy(fe_batch* b) {
   delete b->sel;
   delete b;
   return FE_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ differentiable LK + adjoint
+struct fe_adjoint {
+  fe_context* ctx = nullptr;
+  int mode = FE_ADJOINT_IMPLICIT, iters = 0;
+  int L = 1, total = 0, nplanes = 0, total_tiles = 0;
+  fe::LkLaunch lk;
+  fe::AdjLaunch adj;
+  fe::AdjGather gat;
+  std::vector<fe::AdjPyrLevel> pyr;  // [level]
+  StagePlan build;                   // pyramid builds of the jobs that name their frames
+  bool forward_ran = false;          // the unrolled backward can use the forward's records
+  fe::lk::LkRecord* recs = nullptr;
+  void* mem = nullptr;               // every device buffer of the plan
+  int* counters = nullptr;           // [0] forward track counter, [1] adjoint counter, [2] dropped
+};
+
+namespace {
+
+constexpr int kAdjMaxTracks = 16384;  // per camera: the gather's shared-memory sort capacity
+
+}  // namespace
+
+extern "C" {
+
+int fe_adjoint_destroy(fe_adjoint* a) {
+  if (!a) return FE_ERR_INVALID_ARGUMENT;
+  if (a->mem) cudaFree(a->mem);
+  delete a;
+  return FE_OK;
+}
+
+int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, int mode, int iterations,
+                      float tolerance, fe_adjoint** out) {
+  if (!out) return FE_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!ctx || !jobs || njobs <= 0 || njobs > fe::kMaxCams) return FE_ERR_INVALID_ARGUMENT;
+  if (mode != FE_ADJOINT_IMPLICIT && mode != FE_ADJOINT_UNROLLED) return FE_ERR_INVALID_ARGUMENT;
+  if (mode == FE_ADJOINT_UNROLLED && (iterations < 1 || iterations > fe::lk_max_unrolled())) return FE_ERR_INVALID_ARGUMENT;
+  if (mode == FE_ADJOINT_IMPLICIT && (iterations < 0 || !(tolerance >= 0.f))) return FE_ERR_INVALID_ARGUMENT;
+  int L = 1, total = 0;
+  for (int j = 0; j < njobs; ++j) {
+    const fe_adjoint_job& J = jobs[j];
+    if (!valid_pyramid(J.prev) || !valid_pyramid(J.cur) || J.prev->levels != J.cur->levels) return FE_ERR_INVALID_ARGUMENT;
+    for (int l = 0; l < J.prev->levels; ++l)
+      if (!J.prev->grad_y[l] || J.prev->width[l] != J.cur->width[l] || J.prev->height[l] != J.cur->height[l])
+        return FE_ERR_INVALID_ARGUMENT;
+    if (J.n_tracks < 0) return FE_ERR_INVALID_ARGUMENT;
+    if (J.n_tracks > kAdjMaxTracks) return FE_ERR_CAPACITY;
+    if (J.n_tracks > 0 && (!J.tracks_in || !J.tracks_out || !J.grad_xy)) return FE_ERR_INVALID_ARGUMENT;
+    if ((uintptr_t)J.tracks_in % 16 || (uintptr_t)J.tracks_out % 16 || (uintptr_t)J.grad_xy % 8) return FE_ERR_INVALID_ARGUMENT;
+    if ((uintptr_t)J.grad_track % 8 || (uintptr_t)J.grad_offset % 8) return FE_ERR_INVALID_ARGUMENT;
+    const int w = J.prev->width[0], h = J.prev->height[0];
+    if (!J.grad_prev || !J.grad_cur || J.grad_prev_pitch_bytes < (int64_t)w * 4 || J.grad_cur_pitch_bytes < (int64_t)w * 4 ||
+        J.grad_prev_pitch_bytes % 4 || J.grad_cur_pitch_bytes % 4 || (uintptr_t)J.grad_prev % 4 || (uintptr_t)J.grad_cur % 4)
+      return FE_ERR_INVALID_ARGUMENT;
+    (void)h;
+    if ((J.prev_image || J.cur_image) &&
+        (!J.prev_image || !J.cur_image || J.image_pitch_bytes < (int64_t)w * 4 || J.image_pitch_bytes % 4 ||
+         !(J.image_scale > 0.f)))
+      return FE_ERR_INVALID_ARGUMENT;
+    if (mode == FE_ADJOINT_UNROLLED) L = std::max(L, J.prev->levels);
+    total += J.n_tracks;
+  }
+  fe_adjoint* a = new (std::nothrow) fe_adjoint;
+  if (!a) return FE_ERR_OUT_OF_MEMORY;
+  auto fail = [&](int rc) {
+    fe_adjoint_destroy(a);
+    return rc;
+  };
+  a->ctx = ctx;
+  a->mode = mode;
+  a->iters = iterations;
+  a->L = L;
+  a->total = total;
+  const int cur_s = mode == FE_ADJOINT_UNROLLED ? 32 : 12;
+
+  // planes: (camera, q, level); level-0 image planes are the caller's gradient buffers
+  struct PlaneSpec {
+    int w, h, pitch;
+    float* user;        // caller's buffer, or null: scratch at `off`
+    size_t off;
+  };
+  std::vector<PlaneSpec> spec((size_t)njobs * 4 * L);
+  std::vector<fe::AdjPlane> planes(spec.size());
+  size_t scratch = 0;
+  int tiles = 0;
+  for (int j = 0; j < njobs; ++j)
+    for (int q = 0; q < 4; ++q)
+      for (int l = 0; l < L; ++l) {
+        const size_t k = ((size_t)j * 4 + q) * L + l;
+        PlaneSpec& s = spec[k];
+        fe::AdjPlane& P = planes[k];
+        memset(&P, 0, sizeof(P));
+        s = PlaneSpec{0, 0, 0, nullptr, 0};
+        P.tile_begin = tiles;
+        if (l >= jobs[j].prev->levels) continue;
+        s.w = jobs[j].prev->width[l];
+        s.h = jobs[j].prev->height[l];
+        if (l == 0 && q == 0) {
+          s.user = jobs[j].grad_prev;
+          s.pitch = (int)(jobs[j].grad_prev_pitch_bytes / 4);
+        } else if (l == 0 && q == 3) {
+          s.user = jobs[j].grad_cur;
+          s.pitch = (int)(jobs[j].grad_cur_pitch_bytes / 4);
+        } else {
+          s.pitch = (int)(align_up((int64_t)s.w * 4, kAlign) / 4);
+          s.off = scratch;
+          scratch += (size_t)s.pitch * s.h * 4;
+        }
+        P.w = s.w;
+        P.h = s.h;
+        P.pitch = s.pitch;
+        P.tiles_x = (s.w + 31) / 32;
+        P.ntiles = P.tiles_x * ((s.h + 31) / 32);
+        tiles += P.ntiles;
+      }
+  a->nplanes = (int)planes.size();
+  a->total_tiles = tiles;
+
+  // one allocation: scratch planes, records, tile lists, descriptors, counters
+  const size_t nslots = (size_t)4 * L * total;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = (size_t)align_up((int64_t)(o + bytes), kAlign);
+    return at;
+  };
+  const size_t o_planes = take(scratch);
+  const size_t o_hdr = take(std::max<size_t>(nslots, 1) * sizeof(int4));
+  const size_t o_dprev = take(std::max<size_t>((size_t)3 * L * total * 144 * 4, 4));
+  const size_t o_dcur = take(std::max<size_t>((size_t)L * total * cur_s * cur_s * 4, 4));
+  const size_t o_count = take(((size_t)tiles + 1) * 4);
+  const size_t o_off = take(((size_t)tiles + 1) * 4);
+  const size_t o_cursor = take(((size_t)tiles + 1) * 4);
+  const size_t o_list = take(std::max<size_t>(nslots * 4, 1) * 4);  // a record covers <= 4 tiles
+  const size_t o_pl = take(planes.size() * sizeof(fe::AdjPlane));
+  const size_t o_cams = take((size_t)njobs * sizeof(fe::AdjCam));
+  const size_t o_lk = take((size_t)njobs * sizeof(fe::LkCam));
+  const size_t o_recs = take(mode == FE_ADJOINT_UNROLLED ? std::max(total, 1) * fe::lk_record_bytes() : 0);
+  const size_t o_ctr = take(256);
+  cudaError_t e = cudaMalloc(&a->mem, o);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  char* base = (char*)a->mem;
+  a->counters = (int*)(base + o_ctr);
+  for (size_t k = 0; k < planes.size(); ++k)
+    if (planes[k].ntiles > 0) planes[k].dst = spec[k].user ? spec[k].user : (float*)(base + o_planes + spec[k].off);
+
+  std::vector<fe::AdjCam> cams(njobs);
+  std::vector<fe::LkCam> lks(njobs);
+  int begin = 0, max_n = 1;
+  for (int j = 0; j < njobs; ++j) {
+    const fe_adjoint_job& J = jobs[j];
+    fe::LkCam& lc = lks[j];
+    memset(&lc, 0, sizeof(lc));
+    lc.prev = to_pyr(*J.prev);
+    lc.cur = to_pyr(*J.cur);
+    lc.tracks = J.tracks_out;
+    lc.tracks_in = J.tracks_in;
+    lc.n = J.n_tracks;
+    lc.begin = begin;
+    fe::AdjCam& ac = cams[j];
+    memset(&ac, 0, sizeof(ac));
+    ac.lk = lc;
+    ac.tracks_out = J.tracks_out;
+    ac.grad_xy = J.grad_xy;
+    ac.grad_track = J.grad_track;
+    ac.grad_offset = J.grad_offset;
+    begin += J.n_tracks;
+    max_n = std::max(max_n, J.n_tracks);
+  }
+  e = cudaMemcpy(base + o_pl, planes.data(), planes.size() * sizeof(fe::AdjPlane), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(base + o_cams, cams.data(), cams.size() * sizeof(fe::AdjCam), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(base + o_lk, lks.data(), lks.size() * sizeof(fe::LkCam), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+
+  memset(&a->lk, 0, sizeof(a->lk));
+  a->lk.cams = (const fe::LkCam*)(base + o_lk);
+  a->lk.counter = a->counters;
+  a->lk.ncams = njobs;
+  a->lk.total = total;
+  a->lk.sampling = FE_SAMPLE_EXACT;
+  a->lk.mode = mode == FE_ADJOINT_UNROLLED ? fe::kLkUnrolled : fe::kLkImplicit;
+  a->lk.iters = iterations;
+  a->lk.tol2 = tolerance * tolerance;
+  if (mode == FE_ADJOINT_UNROLLED) {
+    a->recs = (fe::lk::LkRecord*)(base + o_recs);
+    a->lk.recs = a->recs;
+  }
+  for (int j = 0; j < njobs; ++j) {
+    const fe_adjoint_job& J = jobs[j];
+    if (!J.prev_image) continue;
+    int rc = plan_pyramid(J.prev_image, J.image_pitch_bytes, false, *J.prev, a->build, J.image_scale);
+    if (!rc) rc = plan_pyramid(J.cur_image, J.image_pitch_bytes, false, *J.cur, a->build, J.image_scale);
+    if (rc) return fail(rc);
+  }
+
+  memset(&a->adj, 0, sizeof(a->adj));
+  a->adj.cams = (const fe::AdjCam*)(base + o_cams);
+  a->adj.ncams = njobs;
+  a->adj.total = total;
+  a->adj.counter = a->counters + 1;
+  a->adj.mode = a->lk.mode;
+  a->adj.iters = iterations;
+  a->adj.L = L;
+  a->adj.cur_s = cur_s;
+  a->adj.hdr = (int4*)(base + o_hdr);
+  a->adj.data_prev = (float*)(base + o_dprev);
+  a->adj.data_cur = (float*)(base + o_dcur);
+  a->adj.overflow = a->counters + 2;
+
+  memset(&a->gat, 0, sizeof(a->gat));
+  a->gat.planes = (const fe::AdjPlane*)(base + o_pl);
+  a->gat.cams = a->adj.cams;
+  a->gat.nplanes = a->nplanes;
+  a->gat.ncams = njobs;
+  a->gat.total_tiles = tiles;
+  a->gat.nslots = (int)nslots;
+  a->gat.L = L;
+  a->gat.total = total;
+  a->gat.cur_s = cur_s;
+  a->gat.hdr = a->adj.hdr;
+  a->gat.data_prev = a->adj.data_prev;
+  a->gat.data_cur = a->adj.data_cur;
+  a->gat.count = (int*)(base + o_count);
+  a->gat.off = (int*)(base + o_off);
+  a->gat.cursor = (int*)(base + o_cursor);
+  a->gat.list = (int*)(base + o_list);
+  a->gat.list_cap = next_pow2(max_n);
+
+  // pyramid adjoint, one launch per level (top level first)
+  a->pyr.resize(L);
+  for (int l = 0; l < L; ++l) {
+    fe::AdjPyrLevel& lv = a->pyr[l];
+    memset(&lv, 0, sizeof(lv));
+    int px = 0;
+    for (int j = 0; j < njobs; ++j) {
+      if (l >= jobs[j].prev->levels) continue;
+      for (int side = 0; side < 2; ++side) {
+        const int q = side ? 3 : 0;
+        const fe::AdjPlane& P = planes[((size_t)j * 4 + q) * L + l];
+        fe::AdjPyrJob& J = lv.job[lv.njobs++];
+        memset(&J, 0, sizeof(J));
+        J.img = P.dst;
+        J.pitch = P.pitch;
+        J.w = P.w;
+        J.h = P.h;
+        if (!side) {
+          J.gx = planes[((size_t)j * 4 + 1) * L + l].dst;
+          J.gy = planes[((size_t)j * 4 + 2) * L + l].dst;
+          J.gpitch = planes[((size_t)j * 4 + 1) * L + l].pitch;
+        }
+        if (l + 1 < L && l + 1 < jobs[j].prev->levels) {
+          const fe::AdjPlane& U = planes[((size_t)j * 4 + q) * L + l + 1];
+          J.up = U.dst;
+          J.up_pitch = U.pitch;
+          J.up_w = U.w;
+          J.up_h = U.h;
+        }
+        J.px_begin = px;
+        px += P.w * P.h;
+      }
+    }
+    lv.total_px = px;
+  }
+  *out = a;
+  return FE_OK;
+}
+
+int fe_adjoint_build_pyramids(fe_adjoint* a, fe_stream stream) {
+  if (!a) return FE_ERR_INVALID_ARGUMENT;
+  return run_plan(a->build, (cudaStream_t)stream);
+}
+
+int fe_adjoint_forward(fe_adjoint* a, fe_stream stream) {
+  if (!a) return FE_ERR_INVALID_ARGUMENT;
+  FE_CUDA(fe::launch_lk(a->lk, (cudaStream_t)stream));
+  a->forward_ran = true;
+  return FE_OK;
+}
+
+int fe_adjoint_backward(fe_adjoint* a, fe_stream stream) {
+  if (!a) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  a->adj.recs = a->forward_ran ? a->recs : nullptr;
+  FE_CUDA(cudaMemsetAsync(a->adj.overflow, 0, sizeof(int), st));
+  FE_CUDA(fe::launch_lk_adjoint(a->adj, st));
+  FE_CUDA(fe::launch_adjoint_gather(a->gat, st));
+  for (int l = a->L - 1; l >= 0; --l) FE_CUDA(fe::launch_pyramid_adjoint(a->pyr[l], st));
+  return FE_OK;
+}
+
+int fe_adjoint_kernel_count(const fe_adjoint* a, int backward) {
+  if (!a) return 0;
+  if (backward == 2) {  // pyramid builds
+    int n = 0;
+    for (const auto& stage : a->build) n += (int)stage.size();
+    return n;
+  }
+  if (!backward) return a->total > 0 ? 1 : 0;
+  int n = a->total > 0 ? 1 : 0;              // adjoint
+  if (a->total_tiles > 0) n += a->gat.nslots > 0 ? 4 : 2;  // count, scan, fill, gather
+  for (int l = 0; l < a->L; ++l) n += a->pyr[l].total_px > 0 ? 1 : 0;
+  return n;
+}
+
+int fe_adjoint_dropped(const fe_adjoint* a, int32_t* device_out, fe_stream stream) {
+  if (!a || !device_out) return FE_ERR_INVALID_ARGUMENT;
+  FE_CUDA(cudaMemcpyAsync(device_out, a->adj.overflow, sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                          (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_track_diff(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, const fe_track_data* tracks_in,
+                  fe_track_data* tracks_out, int n, int mode, int iterations, float tolerance, fe_stream stream) {
+  if (!prev) return FE_ERR_INVALID_ARGUMENT;
+  // the plan wants gradient outputs; the forward never touches them
+  fe_adjoint_job J;
+  memset(&J, 0, sizeof(J));
+  J.prev = prev;
+  J.cur = cur;
+  J.tracks_in = tracks_in;
+  J.tracks_out = tracks_out;
+  J.n_tracks = n;
+  J.grad_xy = reinterpret_cast<const float*>(tracks_out);
+  J.grad_prev = J.grad_cur = reinterpret_cast<float*>(tracks_out);
+  J.grad_prev_pitch_bytes = J.grad_cur_pitch_bytes = (int64_t)prev->width[0] * 4;
+  if (n == 0) return FE_OK;
+  fe_adjoint* a = nullptr;
+  int rc = fe_adjoint_create(ctx, &J, 1, mode, iterations, tolerance, &a);
+  if (rc) return rc;
+  rc = fe_adjoint_forward(a, stream);
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  fe_adjoint_destroy(a);
+  if (rc) return rc;
+  return e == cudaSuccess ? FE_OK : cuda_fail(e);
+}
+
+int fe_track_backward(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, const fe_track_data* tracks_in,
+                      const fe_track_data* tracks_out, int n, int mode, int iterations, float tolerance,
+                      const float* grad_xy, float* grad_prev, int64_t grad_prev_pitch_bytes, float* grad_cur,
+                      int64_t grad_cur_pitch_bytes, float* grad_track, float* grad_offset, fe_stream stream) {
+  fe_adjoint_job J;
+  memset(&J, 0, sizeof(J));
+  J.prev = prev;
+  J.cur = cur;
+  J.tracks_in = tracks_in;
+  J.tracks_out = const_cast<fe_track_data*>(tracks_out);
+  J.n_tracks = n;
+  J.grad_xy = grad_xy;
+  J.grad_prev = grad_prev;
+  J.grad_prev_pitch_bytes = grad_prev_pitch_bytes;
+  J.grad_cur = grad_cur;
+  J.grad_cur_pitch_bytes = grad_cur_pitch_bytes;
+  J.grad_track = grad_track;
+  J.grad_offset = grad_offset;
+  fe_adjoint* a = nullptr;
+  int rc = fe_adjoint_create(ctx, &J, 1, mode, iterations, tolerance, &a);
+  if (rc) return rc;
+  rc = fe_adjoint_backward(a, stream);
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  fe_adjoint_destroy(a);
+  if (rc) return rc;
+  return e == cudaSuccess ? FE_OK : cuda_fail(e);
 }
 
 }  // extern "C"

@@ -17,6 +17,7 @@ struct alignas(64) StageJob {
   int src_w, src_h;
   int write_level0;         // also write level s (image cast + gradients): the uint8 stage
   int use_tma;              // frame meets TMA alignment (16-byte base and pitch)
+  float scale;              // factor on the staged source (FP32 first stage; 1 otherwise)
   int tiles_x, tiles_y;
   int tile_begin;           // first CTA of this job in the launch
   Level out[3];             // out[k] = level s + k; out[0] describes level s
@@ -94,9 +95,18 @@ struct LkCam {
   Pyr prev;                     // image + gradients
   Pyr cur;                      // image
   fe_track_data* tracks;
+  const fe_track_data* tracks_in;  // out-of-place input records, or nullptr (tracks in place)
   int n;
   int begin;                    // first track of this camera in the flattened list
 };
+
+// Iteration rule of a launch: the reference tracker, or the differentiable tracker (exact
+// sampling) in one of its two adjoint modes.
+constexpr int kLkReference = 0, kLkImplicit = 1, kLkUnrolled = 2;
+
+namespace lk {
+struct LkRecord;
+}
 
 struct LkLaunch {
   const LkCam* cams;            // device array (batched) or nullptr
@@ -105,9 +115,82 @@ struct LkLaunch {
   int total;
   int horizontal;
   int sampling;
+  int mode;                     // kLk*
+  int iters;                    // implicit: refinement steps at level 0; unrolled: steps per level
+  float tol2;                   // implicit: squared step below which the refinement stops
+  lk::LkRecord* recs;           // unrolled: per-track records for the adjoint (may be null)
   LkCam single;                 // used when cams == nullptr
 };
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
+
+// ---------------------------------------------------------------- LK adjoint
+// Per-track gradient contributions are written as window records (slot = (plane q, level l, track g),
+// q: 0 previous image, 1 previous grad_x, 2 previous grad_y, 3 current image), then summed per
+// 32x32 tile of each plane in track order (a deterministic segmented reduction), then pushed through
+// the gradient filters and the decimation, from the top level down.
+struct AdjCam {
+  LkCam lk;                          // pyramids, tracks_in (forward inputs), n, begin
+  const fe_track_data* tracks_out;   // forward results (implicit mode reads position and status)
+  const float* grad_xy;              // n x 2: dL/d(output position)
+  float* grad_track;                 // n x 2 or null: dL/d(track position)
+  float* grad_offset;                // n x 2 or null: dL/d(offset)
+};
+
+struct AdjLaunch {
+  const AdjCam* cams;
+  int ncams, total;
+  int* counter;                      // persistent-warp track counter
+  int mode, iters;                   // kLkImplicit / kLkUnrolled
+  int L;                             // record levels (1 implicit; deepest pyramid unrolled)
+  int cur_s;                         // current-image record edge: 12 implicit, 32 unrolled
+  const lk::LkRecord* recs;          // unrolled: the forward's records, or null (replay the forward)
+  int4* hdr;                         // [4][L][total] {x0, y0, w, h}; w == 0: empty
+  float* data_prev;                  // [3][L][total][12 * 12]
+  float* data_cur;                   // [L][total][cur_s * cur_s]
+  int* overflow;                     // tracks dropped because a level's iterates spread too far
+};
+
+struct AdjPlane {
+  float* dst;                        // dense gradient plane (written whole)
+  int pitch, w, h;                   // pitch in floats
+  int tiles_x, tile_begin, ntiles;
+};
+
+struct AdjGather {
+  const AdjPlane* planes;            // [(cam * 4 + q) * L + l]
+  const AdjCam* cams;
+  int nplanes, ncams, total_tiles, nslots, L, total, cur_s;
+  const int4* hdr;
+  const float* data_prev;
+  const float* data_cur;
+  int* count;                        // [total_tiles]
+  int* off;                          // [total_tiles + 1]
+  int* cursor;                       // [total_tiles]
+  int* list;
+  int list_cap;                      // power of two >= the longest list (tracks of one camera)
+};
+
+struct AdjPyrJob {
+  float* img;                        // in: summed records of the level; out: complete gradient
+  const float* gx;                   // previous frame: gradient planes' adjoints (null: current frame)
+  const float* gy;
+  const float* up;                   // complete gradient of the next level (null at the top)
+  int pitch, gpitch, up_pitch;
+  int w, h, up_w, up_h;
+  int px_begin;
+};
+
+struct AdjPyrLevel {
+  int njobs, total_px;
+  AdjPyrJob job[2 * kMaxCams];
+};
+
+cudaError_t adjoint_init();        // kernel attributes; call once per device before capture
+int lk_max_unrolled();             // most steps per level the unrolled mode records
+size_t lk_record_bytes();          // bytes of one track's unrolled-mode record
+cudaError_t launch_lk_adjoint(const AdjLaunch& a, cudaStream_t s);
+cudaError_t launch_adjoint_gather(const AdjGather& g, cudaStream_t s);
+cudaError_t launch_pyramid_adjoint(const AdjPyrLevel& lv, cudaStream_t s);
 
 }  // namespace fe

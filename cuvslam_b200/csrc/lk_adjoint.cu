@@ -1,0 +1,854 @@
+// Adjoint of the differentiable LK tracker: one warp per track computes the track's gradient
+// contributions to the pyramids' planes as small window records; a tile-segmented reduction sums
+// the records of every 32x32 tile of every plane in track order; the pyramid adjoint then applies
+// the transposed gradient filters and the transposed 5x5 decimation from the top level down to the
+// level-0 images.  Everything is deterministic: no floating-point atomics.
+//
+// Forward model (lk_track.cuh, exact bilinear sampling): per level l a template at s_l
+// (P1, Gx, Gy on the 9x9 taps; a = Gx - mean, b = Gy - mean; H = I + sum w g g^T) and steps
+// c += v, v = H^-1 e(c), e = sum w r g, r = P2(c) - P1 - (mean P2 - mean P1).
+//
+// Implicit mode (implicit-function theorem at the converged level-0 displacement c*, where
+// e(c*) = 0): J = de/dc = sum w g (dP2/dc - mean dP2/dc)^T, J^T lambda = dL/dc*, and
+// dL/dtheta = -lambda^T de/dtheta, i.e. per tap
+//   dL/dP2 = u - mean u, dL/dP1 = -(u - mean u), u = -w (lambda . g),
+//   dL/dGx = ab - mean ab, ab = -w r lambda_x  (Gy likewise).
+// Unrolled mode: the replayed forward (lk_track.cuh records the iterates) is differentiated step by
+// step backwards, patches re-sampled from the pyramids rather than stored:
+//   mu = H^-1 cbar, Hbar -= mu v^T, dL/dP2 = u - mean u with u = w (mu . g), cbar += sum dL/dP2 dP2/dc,
+//   dL/dP1 -= dL/dP2, abar += w r mu_x, bbar += w r mu_y; after the level
+//   abar += w (2 Hbar_xx a + (Hbar_xy + Hbar_yx) b), bbar likewise, dL/dGx = abar - mean abar.
+// Template positions receive sum dL/dP1 dP1/ds + dL/dGx dGx/ds + dL/dGy dGy/ds; positions map
+// between levels as s_l = 2 s_{l+1} - 1/2.
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "fe_common.cuh"
+#include "fe_internal.h"
+#include "lk_common.cuh"
+#include "lk_track.cuh"
+
+namespace fe {
+
+namespace {
+
+using namespace lk;
+
+constexpr int kAdjWarps = 4;
+constexpr int kRP = 12;  // previous-image record edge (the template's 12x12 window)
+constexpr int kTile = 32;
+constexpr int kGatherThreads = 256;
+constexpr int kGatherWarps = kGatherThreads / 32;
+
+struct AdjSmem {
+  WarpSmem win;               // staging windows, as the forward
+  LkRecord rec;               // the replayed forward (unrolled)
+  fe_track_data td;           // the replayed record (unrolled)
+  float acc[32 * 32];         // current-image record
+  float prec[3][kRP * kRP];   // previous-image records
+  float coef[3][81];          // tap coefficients (serial scatter)
+  int cb[9], rb[9];           // column / row texel index (serial scatter)
+  float cf[9], rf[9];         // column / row fraction
+};
+
+// Adds the transposed bilinear taps of NP coefficient sets (tap f = lane + 32 e) into shared-memory
+// records dst[p] (row stride rs, origin (rx0, ry0) in level texels).  Texel indices are clamped to
+// the W x H level as the forward's staged windows clamp them.  When all taps share their fractions
+// and none clamps, four conflict-free passes (one per bilinear corner) add the taps; otherwise lane 0
+// adds every tap in order.  Both are deterministic.
+template <int NP>
+__device__ void scatter_taps(float* const (&dst)[NP], int rs, int rx0, int ry0, const TapSet& ts,
+                             const float (&c)[NP][kNE], const bool (&valid)[kNE], const int (&ix)[kNE],
+                             const int (&iy)[kNE], int W, int H, AdjSmem& sm, int lane) {
+  const int b0x = __shfl_sync(kFull, ts.base, 0), b0y = __shfl_sync(kFull, ts.base, 16);
+  __syncwarp();
+  if (ts.uniform && b0x >= 0 && b0y >= 0 && b0x + 9 <= W - 1 && b0y + 9 <= H - 1) {
+    const float fx = ts.u.w00, fy = ts.u.w10;
+    const float gx = __fsub_rn(1.f, fx), gy = __fsub_rn(1.f, fy);
+    const float wc[4] = {__fmul_rn(gx, gy), __fmul_rn(fx, gy), __fmul_rn(gx, fy), __fmul_rn(fx, fy)};
+#pragma unroll
+    for (int corner = 0; corner < 4; ++corner) {
+      const int cx = corner & 1, cy = corner >> 1;
+#pragma unroll
+      for (int e = 0; e < kNE; ++e) {
+        if (valid[e]) {
+          const int o = (b0y + iy[e] + cy - ry0) * rs + (b0x + ix[e] + cx - rx0);
+#pragma unroll
+          for (int q = 0; q < NP; ++q) dst[q][o] = __fmaf_rn(wc[corner], c[q][e], dst[q][o]);
+        }
+      }
+      __syncwarp();
+    }
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < kNE; ++e)
+    if (valid[e])
+#pragma unroll
+      for (int q = 0; q < NP; ++q) sm.coef[q][lane + 32 * e] = c[q][e];
+  if (lane < 9) {
+    sm.cb[lane] = ts.base;
+    sm.cf[lane] = ts.fr;
+  }
+  if (lane >= 16 && lane < 25) {
+    sm.rb[lane - 16] = ts.base;
+    sm.rf[lane - 16] = ts.fr;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int f = 0; f < 81; ++f) {
+      const int i = f % 9, j = f / 9;
+      const float fx = sm.cf[i], fy = sm.rf[j];
+      const float gx = __fsub_rn(1.f, fx), gy = __fsub_rn(1.f, fy);
+      const int x0 = min(max(sm.cb[i], 0), W - 1) - rx0, x1 = min(max(sm.cb[i] + 1, 0), W - 1) - rx0;
+      const int y0 = min(max(sm.rb[j], 0), H - 1) - ry0, y1 = min(max(sm.rb[j] + 1, 0), H - 1) - ry0;
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        const float v = sm.coef[q][f];
+        dst[q][y0 * rs + x0] = __fmaf_rn(__fmul_rn(gx, gy), v, dst[q][y0 * rs + x0]);
+        dst[q][y0 * rs + x1] = __fmaf_rn(__fmul_rn(fx, gy), v, dst[q][y0 * rs + x1]);
+        dst[q][y1 * rs + x0] = __fmaf_rn(__fmul_rn(gx, fy), v, dst[q][y1 * rs + x0]);
+        dst[q][y1 * rs + x1] = __fmaf_rn(__fmul_rn(fx, fy), v, dst[q][y1 * rs + x1]);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void zero_smem(float* p, int n, int lane) {
+  for (int i = lane; i < n; i += 32) p[i] = 0.f;
+  __syncwarp();
+}
+
+// Copies a w x h shared-memory record (row stride rs) to its global slot (row stride gs).
+__device__ __forceinline__ void store_record(float* dst, int gs, const float* src, int rs, int w, int h, int lane) {
+  for (int i = lane; i < w * h; i += 32) {
+    const int r = i / w, c = i - r * w;
+    dst[r * gs + c] = src[r * rs + c];
+  }
+}
+
+// The template of one level: the previous-frame windows staged at the patch under s, the taps'
+// samples, the mean-subtracted gradients and (unrolled) H, all as lk_track.cuh computes them.
+struct Templ {
+  float p1[kNE], a[kNE], b[kNE];
+  float sp, gxx, gxy, gyy, det_rcp;
+  int bx, by;
+  TapSet ts;
+};
+
+__device__ void make_template(const Level& PL, float sx, float sy, const bool (&valid)[kNE], const int (&ix)[kNE],
+                              const int (&iy)[kNE], const float (&wt)[kNE], AdjSmem& sm, int lane, Templ& T) {
+  const float rcp81 = 1.f / 81.f;
+  const float xmin = __fadd_rn(sx, -4.f), ymin = __fadd_rn(sy, -4.f);
+  T.bx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1;
+  T.by = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
+  __syncwarp();
+  stage<kPW, kPS>(sm.win.img, PL.img, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
+  stage<kPW, kPS>(sm.win.gx, PL.gx, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
+  stage<kPW, kPS>(sm.win.gy, PL.gy, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
+  cp_async_wait_all();
+  __syncwarp();
+  T.ts = make_taps<FE_SAMPLE_EXACT>(xmin, ymin, T.bx, T.by, kPS, lane);
+  float gxp[kNE], gyp[kNE];
+  float sgx = 0.f, sgy = 0.f, sp = 0.f;
+#pragma unroll
+  for (int e = 0; e < kNE; ++e) {
+    gxp[e] = gyp[e] = T.p1[e] = 0.f;
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.bx, T.by, kPS);
+    if (valid[e]) {
+      gxp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gx, kPS, t);
+      gyp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gy, kPS, t);
+      T.p1[e] = sample<FE_SAMPLE_EXACT>(sm.win.img, kPS, t);
+      sgx = __fadd_rn(sgx, gxp[e]);
+      sgy = __fadd_rn(sgy, gyp[e]);
+      sp = __fadd_rn(sp, T.p1[e]);
+    }
+  }
+  sgx = warp_sum(sgx);
+  sgy = warp_sum(sgy);
+  T.sp = warp_sum(sp);
+  float lxx = 1.f / 32.f, lxy = 0.f, lyy = 1.f / 32.f;
+#pragma unroll
+  for (int e = 0; e < kNE; ++e) {
+    T.a[e] = T.b[e] = 0.f;
+    if (valid[e]) {
+      T.a[e] = __fmaf_rn(-sgx, rcp81, gxp[e]);
+      T.b[e] = __fmaf_rn(-sgy, rcp81, gyp[e]);
+      lxx = __fmaf_rn(__fmul_rn(T.a[e], T.a[e]), wt[e], lxx);
+      lxy = __fmaf_rn(__fmul_rn(T.a[e], T.b[e]), wt[e], lxy);
+      lyy = __fmaf_rn(__fmul_rn(T.b[e], T.b[e]), wt[e], lyy);
+    }
+  }
+  T.gxx = warp_sum(lxx);
+  T.gxy = warp_sum(lxy);
+  T.gyy = warp_sum(lyy);
+  T.det_rcp = __fdiv_rn(1.f, __fmaf_rn(T.gxx, T.gyy, -__fmul_rn(T.gxy, T.gxy)));
+}
+
+// Writes the three previous-image records of (level, track) from the template adjoint and returns
+// dL/ds (the template position) through (dsx, dsy).  The staged windows of make_template are read.
+__device__ void finish_template(const AdjLaunch& p, int g, int level, int W, int H, const Templ& T,
+                                const float (&p1b)[kNE], const float (&gxb)[kNE], const float (&gyb)[kNE],
+                                const bool (&valid)[kNE], const int (&ix)[kNE], const int (&iy)[kNE], AdjSmem& sm,
+                                int lane, float& dsx, float& dsy) {
+  // dL/ds from the staged windows
+  float sx = 0.f, sy = 0.f;
+#pragma unroll
+  for (int e = 0; e < kNE; ++e) {
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.bx, T.by, kPS);
+    if (valid[e]) {
+      float v, dx, dy;
+      sample_vg(sm.win.img, kPS, t, v, dx, dy);
+      sx = __fmaf_rn(p1b[e], dx, sx);
+      sy = __fmaf_rn(p1b[e], dy, sy);
+      sample_vg(sm.win.gx, kPS, t, v, dx, dy);
+      sx = __fmaf_rn(gxb[e], dx, sx);
+      sy = __fmaf_rn(gxb[e], dy, sy);
+      sample_vg(sm.win.gy, kPS, t, v, dx, dy);
+      sx = __fmaf_rn(gyb[e], dx, sx);
+      sy = __fmaf_rn(gyb[e], dy, sy);
+    }
+  }
+  dsx = warp_sum(sx);
+  dsy = warp_sum(sy);
+  // records
+  const int rx0 = max(T.bx, 0), ry0 = max(T.by, 0);
+  zero_smem(&sm.prec[0][0], 3 * kRP * kRP, lane);
+  float* const dst[3] = {sm.prec[0], sm.prec[1], sm.prec[2]};
+  const float c[3][kNE] = {{p1b[0], p1b[1], p1b[2]}, {gxb[0], gxb[1], gxb[2]}, {gyb[0], gyb[1], gyb[2]}};
+  scatter_taps<3>(dst, kRP, rx0, ry0, T.ts, c, valid, ix, iy, W, H, sm, lane);
+  const int rw = min(kRP, W - rx0), rh = min(kRP, H - ry0);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const size_t slot = ((size_t)q * p.L + level) * p.total + g;
+    store_record(p.data_prev + slot * (kRP * kRP), kRP, sm.prec[q], kRP, rw, rh, lane);
+    if (lane == 0) p.hdr[slot] = make_int4(rx0, ry0, rw, rh);
+  }
+}
+
+__device__ __forceinline__ void empty_level(const AdjLaunch& p, int g, int level, int lane) {
+  if (lane < 4) p.hdr[((size_t)lane * p.L + level) * p.total + g] = make_int4(0, 0, 0, 0);
+}
+
+__device__ __forceinline__ void finish_track(const AdjCam& cam, int i, float gtx, float gty, float gox, float goy,
+                                             int lane) {
+  if (lane == 0) {
+    if (cam.grad_track) reinterpret_cast<float2*>(cam.grad_track)[i] = make_float2(gtx, gty);
+    if (cam.grad_offset) reinterpret_cast<float2*>(cam.grad_offset)[i] = make_float2(gox, goy);
+  }
+}
+
+// Stages the current-image 16x16 window for a patch at c when the window (wbx, wby) does not cover
+// it (as the forward does) and returns the patch's tap set.
+__device__ __forceinline__ TapSet cur_taps(const Level& CL, float cx, float cy, int& wbx, int& wby, AdjSmem& sm,
+                                           int lane) {
+  const float xmin = __fadd_rn(cx, -4.f), ymin = __fadd_rn(cy, -4.f);
+  const int nbx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, nby = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
+  if (nbx < wbx || nbx + kPW > wbx + kCW || nby < wby || nby + kPW > wby + kCW) {
+    wbx = nbx - 2;
+    wby = nby - 2;
+    __syncwarp();
+    stage<kCW, kCS>(sm.win.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+    cp_async_wait_all();
+    __syncwarp();
+  }
+  return make_taps<FE_SAMPLE_EXACT>(xmin, ymin, wbx, wby, kCS, lane);
+}
+
+__device__ __forceinline__ int patch_base(float c) {
+  return (int)floorf(__fsub_rn(__fadd_rn(c, -4.f), 0.5f));
+}
+
+template <int MODE>
+__device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSmem& sm, int lane) {
+  const int i = g - cam.lk.begin;
+  const fe_track_data& tin = cam.lk.tracks_in[i];
+  const float2 gout = reinterpret_cast<const float2*>(cam.grad_xy)[i];
+  const int levels = cam.lk.prev.levels, top = levels - 1;
+  const float rcp81 = 1.f / 81.f;
+
+  int ix[kNE], iy[kNE];
+  float wt[kNE];
+  bool valid[kNE];
+#pragma unroll
+  for (int e = 0; e < kNE; ++e) {
+    const int f = lane + 32 * e;
+    valid[e] = f < 81;
+    iy[e] = valid[e] ? f / 9 : 0;
+    ix[e] = valid[e] ? f - (f / 9) * 9 : 0;
+    wt[e] = valid[e] ? gauss9(iy[e]) * gauss9(ix[e]) : 0.f;
+  }
+  auto drop = [&](float value) {
+    for (int l = 0; l < p.L; ++l) empty_level(p, g, l, lane);
+    finish_track(cam, i, value, value, value, value, lane);
+  };
+  const bool gfinite = isfinite(gout.x) && isfinite(gout.y);
+
+  if (MODE == kLkImplicit) {
+    const fe_track_data& tout = cam.tracks_out[i];
+    if (!tout.track_status || !gfinite) return drop(0.f);
+    // level-0 template position, through the forward's chain of level scalings
+    const float scale = 1.f / (float)(1 << top);
+    float sx = __fmaf_rn(__fsub_rn(tin.track[0], 0.5f), scale, 0.5f);
+    float sy = __fmaf_rn(__fsub_rn(tin.track[1], 0.5f), scale, 0.5f);
+    for (int l = top; l > 0; --l) {
+      sx = __fmaf_rn(sx, 2.f, -0.5f);
+      sy = __fmaf_rn(sy, 2.f, -0.5f);
+    }
+    const float cx = tout.track[0], cy = tout.track[1];
+    const Level& PL = cam.lk.prev.lv[0];
+    const Level& CL = cam.lk.cur.lv[0];
+    const int W = CL.w, H = CL.h;
+    Templ T;
+    make_template(PL, sx, sy, valid, ix, iy, wt, sm, lane, T);
+    int wbx = INT_MIN / 2, wby = INT_MIN / 2;
+    const TapSet tc = cur_taps(CL, cx, cy, wbx, wby, sm, lane);
+    float p2[kNE], dx[kNE], dy[kNE];
+    float sc = 0.f, sdx = 0.f, sdy = 0.f;
+#pragma unroll
+    for (int e = 0; e < kNE; ++e) {
+      p2[e] = dx[e] = dy[e] = 0.f;
+      const Tap t = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCS);
+      if (valid[e]) {
+        sample_vg(sm.win.cur, kCS, t, p2[e], dx[e], dy[e]);
+        sc = __fadd_rn(sc, p2[e]);
+        sdx = __fadd_rn(sdx, dx[e]);
+        sdy = __fadd_rn(sdy, dy[e]);
+      }
+    }
+    sc = warp_sum(sc);
+    const float mdx = __fmul_rn(warp_sum(sdx), rcp81), mdy = __fmul_rn(warp_sum(sdy), rcp81);
+    const float delta = __fmul_rn(__fsub_rn(sc, T.sp), rcp81);
+    float r[kNE], j00 = 0.f, j01 = 0.f, j10 = 0.f, j11 = 0.f;
+#pragma unroll
+    for (int e = 0; e < kNE; ++e) {
+      r[e] = 0.f;
+      if (valid[e]) {
+        r[e] = __fsub_rn(__fsub_rn(p2[e], T.p1[e]), delta);
+        const float wa = __fmul_rn(wt[e], T.a[e]), wb = __fmul_rn(wt[e], T.b[e]);
+        const float ddx = __fsub_rn(dx[e], mdx), ddy = __fsub_rn(dy[e], mdy);
+        j00 = __fmaf_rn(wa, ddx, j00);
+        j01 = __fmaf_rn(wa, ddy, j01);
+        j10 = __fmaf_rn(wb, ddx, j10);
+        j11 = __fmaf_rn(wb, ddy, j11);
+      }
+    }
+    j00 = warp_sum(j00);
+    j01 = warp_sum(j01);
+    j10 = warp_sum(j10);
+    j11 = warp_sum(j11);
+    const float detj = __fmaf_rn(j00, j11, -__fmul_rn(j01, j10));
+    if (!(fabsf(detj) > 0.f) || !isfinite(detj)) return drop(0.f);
+    // J^T lambda = dL/dc*
+    const float lx = __fdiv_rn(__fmaf_rn(j11, gout.x, -__fmul_rn(j10, gout.y)), detj);
+    const float ly = __fdiv_rn(__fmaf_rn(j00, gout.y, -__fmul_rn(j01, gout.x)), detj);
+    float u[kNE], ab[kNE], bb[kNE];
+    float su = 0.f, sa = 0.f, sb = 0.f;
+#pragma unroll
+    for (int e = 0; e < kNE; ++e) {
+      u[e] = ab[e] = bb[e] = 0.f;
+      if (valid[e]) {
+        u[e] = -__fmul_rn(wt[e], __fmaf_rn(lx, T.a[e], __fmul_rn(ly, T.b[e])));
+        const float wr = __fmul_rn(wt[e], r[e]);
+        ab[e] = -__fmul_rn(wr, lx);
+        bb[e] = -__fmul_rn(wr, ly);
+        su = __fadd_rn(su, u[e]);
+        sa = __fadd_rn(sa, ab[e]);
+        sb = __fadd_rn(sb, bb[e]);
+      }
+    }
+    const float mu = __fmul_rn(warp_sum(su), rcp81);
+    const float ma = __fmul_rn(warp_sum(sa), rcp81), mb = __fmul_rn(warp_sum(sb), rcp81);
+    float p2b[kNE], p1b[kNE], gxb[kNE], gyb[kNE];
+#pragma unroll
+    for (int e = 0; e < kNE; ++e) {
+      p2b[e] = valid[e] ? __fsub_rn(u[e], mu) : 0.f;
+      p1b[e] = -p2b[e];
+      gxb[e] = valid[e] ? __fsub_rn(ab[e], ma) : 0.f;
+      gyb[e] = valid[e] ? __fsub_rn(bb[e], mb) : 0.f;
+    }
+    // current-image record at c*
+    {
+      const int rx0 = max(patch_base(cx) - 1, 0), ry0 = max(patch_base(cy) - 1, 0);
+      const int rs = p.cur_s;
+      zero_smem(sm.acc, rs * rs, lane);
+      float* const dst[1] = {sm.acc};
+      const float c1[1][kNE] = {{p2b[0], p2b[1], p2b[2]}};
+      scatter_taps<1>(dst, rs, rx0, ry0, tc, c1, valid, ix, iy, W, H, sm, lane);
+      const int rw = min(rs, W - rx0), rh = min(rs, H - ry0);
+      const size_t slot = (size_t)g;  // level 0
+      store_record(p.data_cur + slot * (rs * rs), rs, sm.acc, rs, rw, rh, lane);
+      if (lane == 0) p.hdr[(size_t)3 * p.L * p.total + slot] = make_int4(rx0, ry0, rw, rh);
+    }
+    float dsx, dsy;
+    finish_template(p, g, 0, W, H, T, p1b, gxb, gyb, valid, ix, iy, sm, lane, dsx, dsy);
+    for (int l = 1; l < p.L; ++l) empty_level(p, g, l, lane);
+    finish_track(cam, i, dsx, dsy, 0.f, 0.f, lane);
+    return;
+  }
+
+  // ---- unrolled: the forward's record of every level's iterates (or a replay of the forward)
+  __syncwarp();
+  if (p.recs) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(p.recs + g);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.rec);
+    for (int k = lane; k < (int)(sizeof(LkRecord) / 4); k += 32) dst[k] = src[k];
+    __syncwarp();
+    // level 0 accepted <=> the track is tracked
+    if (sm.rec.flags[0] != 3 || !gfinite) return drop(0.f);
+  } else {
+    if (lane < 20) reinterpret_cast<uint32_t*>(&sm.td)[lane] = reinterpret_cast<const uint32_t*>(&tin)[lane];
+    __syncwarp();
+    track_one<FE_SAMPLE_EXACT, false, kModeUnrolled>(cam.lk, sm.td, sm.win, lane, p.iters, 0.f, &sm.rec);
+    __syncwarp();
+    if (!sm.td.track_status || !gfinite) return drop(0.f);
+  }
+  // current-image record boxes of the accepted levels must fit cur_s x cur_s
+  for (int level = 0; level <= top; ++level) {
+    if (sm.rec.flags[level] != 3) continue;
+    const int K = sm.rec.K[level];
+    int lox = INT_MAX, hix = INT_MIN, loy = INT_MAX, hiy = INT_MIN;
+    for (int t = 0; t < K; ++t) {
+      const float2 c = sm.rec.it[level][t];
+      lox = min(lox, patch_base(c.x));
+      hix = max(hix, patch_base(c.x));
+      loy = min(loy, patch_base(c.y));
+      hiy = max(hiy, patch_base(c.y));
+    }
+    // taps of a patch reach texels [base, base + 10]; the record starts one texel left of the
+    // smallest base
+    if (hix - lox + 12 > p.cur_s || hiy - loy + 12 > p.cur_s) {
+      if (lane == 0) atomicAdd(p.overflow, 1);
+      return drop(__int_as_float(0x7fc00000));  // NaN: no gradient for this track
+    }
+  }
+  float cbx = gout.x, cby = gout.y;  // dL/d(end position of the level)
+  float gtx = 0.f, gty = 0.f;
+  for (int level = 0; level <= top; ++level) {
+    if (sm.rec.flags[level] == 3) {
+      const Level& PL = cam.lk.prev.lv[level];
+      const Level& CL = cam.lk.cur.lv[level];
+      const int W = CL.w, H = CL.h;
+      const float2 s = sm.rec.s[level];
+      Templ T;
+      make_template(PL, s.x, s.y, valid, ix, iy, wt, sm, lane, T);
+      const int K = sm.rec.K[level];
+      int lox = INT_MAX, loy = INT_MAX, hix = INT_MIN, hiy = INT_MIN;
+      for (int t = 0; t < K; ++t) {
+        const int bx = patch_base(sm.rec.it[level][t].x), by = patch_base(sm.rec.it[level][t].y);
+        lox = min(lox, bx);
+        loy = min(loy, by);
+        hix = max(hix, bx);
+        hiy = max(hiy, by);
+      }
+      // the record spans the iterates' taps: texels [lo - 1, hi + 10] clipped to the level
+      const int rs = p.cur_s;
+      const int rx0 = max(lox - 1, 0), ry0 = max(loy - 1, 0);
+      const int rw = min(hix + 10, W - 1) - rx0 + 1, rh = min(hiy + 10, H - 1) - ry0 + 1;
+      for (int k = lane; k < rw * rh; k += 32) sm.acc[(k / rw) * rs + k % rw] = 0.f;
+      __syncwarp();
+      float p1b[kNE], ab[kNE], bb[kNE];
+#pragma unroll
+      for (int e = 0; e < kNE; ++e) p1b[e] = ab[e] = bb[e] = 0.f;
+      float hxx = 0.f, hxy = 0.f, hyx = 0.f, hyy = 0.f;
+      int wbx = INT_MIN / 2, wby = INT_MIN / 2;
+      for (int t = K - 1; t >= 0; --t) {
+        const float2 c = sm.rec.it[level][t];
+        const TapSet tc = cur_taps(CL, c.x, c.y, wbx, wby, sm, lane);
+        float p2[kNE], dx[kNE], dy[kNE];
+        float sc = 0.f;
+#pragma unroll
+        for (int e = 0; e < kNE; ++e) {
+          p2[e] = dx[e] = dy[e] = 0.f;
+          const Tap tp = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCS);
+          if (valid[e]) {
+            sample_vg(sm.win.cur, kCS, tp, p2[e], dx[e], dy[e]);
+            sc = __fadd_rn(sc, p2[e]);
+          }
+        }
+        sc = warp_sum(sc);
+        const float delta = __fmul_rn(__fsub_rn(sc, T.sp), rcp81);
+        float r[kNE], ex = 0.f, ey = 0.f;
+#pragma unroll
+        for (int e = 0; e < kNE; ++e) {
+          r[e] = 0.f;
+          if (valid[e]) {
+            r[e] = __fsub_rn(__fsub_rn(p2[e], T.p1[e]), delta);
+            const float wd = __fmul_rn(wt[e], r[e]);
+            ex = __fmaf_rn(wd, T.a[e], ex);
+            ey = __fmaf_rn(wd, T.b[e], ey);
+          }
+        }
+        ex = warp_sum(ex);
+        ey = warp_sum(ey);
+        const float vx = __fmul_rn(__fmaf_rn(T.gyy, ex, -__fmul_rn(T.gxy, ey)), T.det_rcp);
+        const float vy = __fmul_rn(__fmaf_rn(T.gxx, ey, -__fmul_rn(T.gxy, ex)), T.det_rcp);
+        const float mux = __fmul_rn(__fmaf_rn(T.gyy, cbx, -__fmul_rn(T.gxy, cby)), T.det_rcp);
+        const float muy = __fmul_rn(__fmaf_rn(T.gxx, cby, -__fmul_rn(T.gxy, cbx)), T.det_rcp);
+        hxx = __fmaf_rn(-mux, vx, hxx);
+        hxy = __fmaf_rn(-mux, vy, hxy);
+        hyx = __fmaf_rn(-muy, vx, hyx);
+        hyy = __fmaf_rn(-muy, vy, hyy);
+        float u[kNE], su = 0.f;
+#pragma unroll
+        for (int e = 0; e < kNE; ++e) {
+          u[e] = 0.f;
+          if (valid[e]) {
+            u[e] = __fmul_rn(wt[e], __fmaf_rn(mux, T.a[e], __fmul_rn(muy, T.b[e])));
+            su = __fadd_rn(su, u[e]);
+          }
+        }
+        const float mu = __fmul_rn(warp_sum(su), rcp81);
+        float p2b[kNE], gx = 0.f, gy = 0.f;
+#pragma unroll
+        for (int e = 0; e < kNE; ++e) {
+          p2b[e] = 0.f;
+          if (valid[e]) {
+            p2b[e] = __fsub_rn(u[e], mu);
+            gx = __fmaf_rn(p2b[e], dx[e], gx);
+            gy = __fmaf_rn(p2b[e], dy[e], gy);
+            p1b[e] = __fsub_rn(p1b[e], p2b[e]);
+            const float wr = __fmul_rn(wt[e], r[e]);
+            ab[e] = __fmaf_rn(wr, mux, ab[e]);
+            bb[e] = __fmaf_rn(wr, muy, bb[e]);
+          }
+        }
+        float* const dst[1] = {sm.acc};
+        const float c1[1][kNE] = {{p2b[0], p2b[1], p2b[2]}};
+        scatter_taps<1>(dst, rs, rx0, ry0, tc, c1, valid, ix, iy, W, H, sm, lane);
+        cbx = __fadd_rn(cbx, warp_sum(gx));
+        cby = __fadd_rn(cby, warp_sum(gy));
+      }
+      const float hs = __fadd_rn(hxy, hyx);
+      float sa = 0.f, sb = 0.f;
+#pragma unroll
+      for (int e = 0; e < kNE; ++e) {
+        if (valid[e]) {
+          ab[e] = __fmaf_rn(wt[e], __fmaf_rn(2.f * hxx, T.a[e], __fmul_rn(hs, T.b[e])), ab[e]);
+          bb[e] = __fmaf_rn(wt[e], __fmaf_rn(hs, T.a[e], __fmul_rn(2.f * hyy, T.b[e])), bb[e]);
+          sa = __fadd_rn(sa, ab[e]);
+          sb = __fadd_rn(sb, bb[e]);
+        }
+      }
+      const float ma = __fmul_rn(warp_sum(sa), rcp81), mb = __fmul_rn(warp_sum(sb), rcp81);
+      float gxb[kNE], gyb[kNE];
+#pragma unroll
+      for (int e = 0; e < kNE; ++e) {
+        gxb[e] = valid[e] ? __fsub_rn(ab[e], ma) : 0.f;
+        gyb[e] = valid[e] ? __fsub_rn(bb[e], mb) : 0.f;
+      }
+      // current-image record of the level
+      {
+        const size_t slot = (size_t)level * p.total + g;
+        store_record(p.data_cur + slot * (rs * rs), rs, sm.acc, rs, rw, rh, lane);
+        if (lane == 0) p.hdr[(size_t)3 * p.L * p.total + slot] = make_int4(rx0, ry0, rw, rh);
+      }
+      float dsx, dsy;
+      finish_template(p, g, level, W, H, T, p1b, gxb, gyb, valid, ix, iy, sm, lane, dsx, dsy);
+      const float sl = 1.f / (float)(1 << level);
+      gtx = __fmaf_rn(dsx, sl, gtx);
+      gty = __fmaf_rn(dsy, sl, gty);
+    } else {
+      empty_level(p, g, level, lane);
+    }
+    if (level < top) {
+      cbx = __fmul_rn(cbx, 2.f);
+      cby = __fmul_rn(cby, 2.f);
+    }
+  }
+  for (int l = levels; l < p.L; ++l) empty_level(p, g, l, lane);
+  const float st = 1.f / (float)(1 << top);
+  finish_track(cam, i, __fmaf_rn(cbx, st, gtx), __fmaf_rn(cby, st, gty), __fmul_rn(cbx, st), __fmul_rn(cby, st),
+               lane);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kAdjWarps * 32, 4) adjoint_kernel(const __grid_constant__ AdjLaunch p) {
+  __shared__ AdjSmem smem[kAdjWarps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (;;) {
+    int v = 0;
+    if (lane == 0) v = atomicAdd(p.counter, 1);
+    const int g = __shfl_sync(kFull, v, 0);
+    if (g >= p.total) return;  // warp-uniform
+    int lo = 0, hi = p.ncams - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.cams[mid].lk.begin <= g) lo = mid; else hi = mid - 1;
+    }
+    adjoint_one<MODE>(p, p.cams[lo], g, smem[wid], lane);
+  }
+}
+
+template <int MODE>
+int adjoint_blocks() {
+  static int blocks = 0;
+  if (!blocks) {
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<MODE>, kAdjWarps * 32, 0);
+    blocks = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  return blocks;
+}
+
+// ---------------------------------------------------------------- tile-segmented reduction
+__device__ __forceinline__ int slot_camera(const AdjGather& G, int g) {
+  int lo = 0, hi = G.ncams - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G.cams[mid].lk.begin <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Visits the tiles a record covers: count (FILL = false) or list fill (FILL = true).
+template <bool FILL>
+__global__ void bin_kernel(const __grid_constant__ AdjGather G) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= G.nslots) return;
+  const int4 h = G.hdr[s];
+  if (h.z <= 0 || h.w <= 0) return;
+  const int per_q = G.L * G.total;
+  const int q = s / per_q, rem = s - q * per_q;
+  const int l = rem / G.total, g = rem - l * G.total;
+  const AdjPlane& P = G.planes[(slot_camera(G, g) * 4 + q) * G.L + l];
+  if (P.ntiles <= 0) return;
+  const int tiles_y = P.ntiles / P.tiles_x;
+  const int tx0 = h.x / kTile, tx1 = min((h.x + h.z - 1) / kTile, P.tiles_x - 1);
+  const int ty0 = h.y / kTile, ty1 = min((h.y + h.w - 1) / kTile, tiles_y - 1);
+  for (int ty = ty0; ty <= ty1; ++ty)
+    for (int tx = tx0; tx <= tx1; ++tx) {
+      const int t = P.tile_begin + ty * P.tiles_x + tx;
+      if (FILL) G.list[G.off[t] + atomicAdd(&G.cursor[t], 1)] = s;
+      else atomicAdd(&G.count[t], 1);
+    }
+}
+
+// Exclusive prefix sum of the per-tile counts (one CTA); clears the fill cursors.
+__global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjGather G) {
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < G.total_tiles; base += 1024) {
+    const int t = base + tid;
+    const int v = t < G.total_tiles ? G.count[t] : 0;
+    int x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = warp_tot[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, d);
+        if (lane >= d) w += y;
+      }
+      warp_tot[lane] = w;  // inclusive
+    }
+    __syncthreads();
+    const int before = carry + (wid > 0 ? warp_tot[wid - 1] : 0) + x - v;
+    if (t < G.total_tiles) {
+      G.off[t] = before;
+      G.cursor[t] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) carry += warp_tot[31];
+    __syncthreads();
+  }
+  if (tid == 0) G.off[G.total_tiles] = carry;
+}
+
+// One CTA per tile: sorts the tile's records by slot (track order), sums them - warp k over the k-th
+// contiguous part of the sorted list into its own partial tile, then the partials in warp order -
+// and writes every texel of the tile.
+__global__ void __launch_bounds__(kGatherThreads) gather_kernel(const __grid_constant__ AdjGather G) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  float* part = reinterpret_cast<float*>(gsm);                         // [kGatherWarps][1024]
+  int* keys = reinterpret_cast<int*>(gsm + kGatherWarps * kTile * kTile * 4);  // [list_cap]
+  const int t = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // the last plane that begins at or before t (an empty plane shares its begin with the next one)
+  int lo = 0, hi = G.nplanes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G.planes[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+  }
+  const AdjPlane& P = G.planes[lo];
+  const int lt = t - P.tile_begin;
+  const int X0 = (lt % P.tiles_x) * kTile, Y0 = (lt / P.tiles_x) * kTile;
+  const int begin = G.off[t], n = min(G.off[t + 1] - begin, G.list_cap);
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int k = tid; k < np2; k += kGatherThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
+  const int nw = min(kGatherWarps, max(1, n / 16));
+  for (int k = tid; k < nw * kTile * kTile; k += kGatherThreads) part[k] = 0.f;
+  __syncthreads();
+  // bitonic sort, ascending
+  for (int size = 2; size <= np2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = tid; k < np2; k += kGatherThreads) {
+        const int o = k ^ stride;
+        if (o > k) {
+          const int a = keys[k], b = keys[o];
+          const bool up = (k & size) == 0;
+          if ((a > b) == up) {
+            keys[k] = b;
+            keys[o] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (wid < nw) {
+    float* mine = part + wid * kTile * kTile;
+    const int r0 = (int)((long long)n * wid / nw), r1 = (int)((long long)n * (wid + 1) / nw);
+    const int per_q = G.L * G.total;
+    for (int k = r0; k < r1; ++k) {
+      const int s = keys[k];
+      const int4 h = G.hdr[s];
+      const int q = s / per_q;
+      const int S = q < 3 ? kRP : G.cur_s;
+      const float* d = q < 3 ? G.data_prev + (size_t)s * (kRP * kRP)
+                             : G.data_cur + (size_t)(s - 3 * per_q) * (G.cur_s * G.cur_s);
+      const int xa = max(h.x, X0), xb = min(h.x + h.z, X0 + kTile);
+      const int ya = max(h.y, Y0), yb = min(h.y + h.w, Y0 + kTile);
+      const int iw = xb - xa, ih = yb - ya;
+      if (iw > 0 && ih > 0) {
+        for (int idx = lane; idx < iw * ih; idx += 32) {
+          const int yy = idx / iw, xx = idx - yy * iw;
+          const int X = xa + xx, Y = ya + yy;
+          mine[(Y - Y0) * kTile + (X - X0)] += d[(Y - h.y) * S + (X - h.x)];
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < kTile * kTile; k += kGatherThreads) {
+    const int X = X0 + (k & (kTile - 1)), Y = Y0 + k / kTile;
+    if (X < P.w && Y < P.h) {
+      float v = part[k];
+      for (int w = 1; w < nw; ++w) v += part[w * kTile * kTile + k];
+      P.dst[(size_t)Y * P.pitch + X] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pyramid adjoint
+__device__ __forceinline__ float binom5(int k) {
+  return k == 2 ? 6.f / 16.f : (k == 1 || k == 3) ? 4.f / 16.f : 1.f / 16.f;
+}
+
+__global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_constant__ AdjPyrLevel L) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= L.total_px) return;
+  int lo = 0, hi = L.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.job[mid].px_begin <= idx) lo = mid; else hi = mid - 1;
+  }
+  const AdjPyrJob& J = L.job[lo];
+  const int k = idx - J.px_begin;
+  const int y = k / J.w, x = k - y * J.w;
+  float v = J.img[(size_t)y * J.pitch + x];
+  if (J.gx) {
+    // transposed 7-tap derivatives: gx(x') = sum_j D_j img(x' - 3 + j) for 2 < x' < w - 3
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      const int xp = x - j + 3;
+      if (xp > 2 && xp < J.w - 3) v = __fmaf_rn(dsp_tap(j), J.gx[(size_t)y * J.gpitch + xp], v);
+    }
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      const int yp = y - j + 3;
+      if (yp > 2 && yp < J.h - 3) v = __fmaf_rn(dsp_tap(j), J.gy[(size_t)yp * J.gpitch + x], v);
+    }
+  }
+  if (J.up) {
+    // transposed decimation: the outputs (X, Y) of the next level whose 5x5 taps read (x, y), either
+    // directly (unmirrored source coordinate 2X - 2 + k == x) or through the mirror (-x-1 below 0,
+    // 2n-x-1 above n-1); taps outside in both directions are skipped as the forward skips them
+    for (int a = 0; a < 3; ++a) {
+      const int yc = a == 0 ? y : a == 1 ? (y <= 1 ? -y - 1 : INT_MIN) : (y >= J.h - 2 ? 2 * J.h - y - 1 : INT_MIN);
+      if (yc == INT_MIN) continue;
+      const bool yo = yc < 0 || yc >= J.h;
+      for (int ky = 0; ky < 5; ++ky) {
+        const int vy = yc + 2 - ky;
+        if (vy & 1) continue;
+        const int Y = vy / 2;
+        if (Y < 0 || Y >= J.up_h) continue;
+        const float* row = J.up + (size_t)Y * J.up_pitch;
+        for (int b = 0; b < 3; ++b) {
+          const int xc = b == 0 ? x : b == 1 ? (x <= 1 ? -x - 1 : INT_MIN) : (x >= J.w - 2 ? 2 * J.w - x - 1 : INT_MIN);
+          if (xc == INT_MIN) continue;
+          const bool xo = xc < 0 || xc >= J.w;
+          if (xo && yo) continue;
+          for (int kx = 0; kx < 5; ++kx) {
+            const int vx = xc + 2 - kx;
+            if (vx & 1) continue;
+            const int X = vx / 2;
+            if (X < 0 || X >= J.up_w) continue;
+            v = __fmaf_rn(__fmul_rn(binom5(ky), binom5(kx)), row[X], v);
+          }
+        }
+      }
+    }
+  }
+  J.img[(size_t)y * J.pitch + x] = v;
+}
+
+}  // namespace
+
+int lk_max_unrolled() { return kMaxRecIt; }
+size_t lk_record_bytes() { return sizeof(LkRecord); }
+
+cudaError_t adjoint_init() {
+  cudaError_t e = cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kGatherWarps * kTile * kTile * 4 + kMaxSelectKeys * 4);
+  return e;
+}
+
+cudaError_t launch_lk_adjoint(const AdjLaunch& a, cudaStream_t s) {
+  if (a.total <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  const int want = (a.total + kAdjWarps - 1) / kAdjWarps;
+  if (a.mode == kLkUnrolled) {
+    adjoint_kernel<kLkUnrolled><<<min(want, adjoint_blocks<kLkUnrolled>()), kAdjWarps * 32, 0, s>>>(a);
+  } else {
+    adjoint_kernel<kLkImplicit><<<min(want, adjoint_blocks<kLkImplicit>()), kAdjWarps * 32, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_gather(const AdjGather& g, cudaStream_t s) {
+  if (g.total_tiles <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(g.count, 0, sizeof(int) * g.total_tiles, s);
+  if (e != cudaSuccess) return e;
+  const int nb = (g.nslots + 255) / 256;
+  if (nb > 0) bin_kernel<false><<<nb, 256, 0, s>>>(g);
+  scan_kernel<<<1, 1024, 0, s>>>(g);
+  if (nb > 0) bin_kernel<true><<<nb, 256, 0, s>>>(g);
+  const size_t smem = kGatherWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4;
+  gather_kernel<<<g.total_tiles, kGatherThreads, smem, s>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pyramid_adjoint(const AdjPyrLevel& lv, cudaStream_t s) {
+  if (lv.total_px <= 0) return cudaSuccess;
+  pyramid_adjoint_kernel<<<(lv.total_px + 255) / 256, 256, 0, s>>>(lv);
+  return cudaGetLastError();
+}
+
+}  // namespace fe

@@ -107,7 +107,8 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
     o += S[k] * S[k];
   }
 
-  // 1. stage the input region
+  // 1. stage the input region (FP32 sources as asynchronous copies, all in flight at once), scaled
+  //    by job.scale (the first stage of a scaled build; 1 otherwise)
   {
     const int w = job.src_w, h = job.src_h;
     const InT* src = static_cast<const InT*>(job.src);
@@ -115,10 +116,25 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
     for (int i = threadIdx.x; i < S[0] * S[0]; i += kThreads) {
       const int r = i / S[0], c = i - r * S[0];
       const int gx = a[0] + c, gy = ay[0] + r;
-      dst[i] = (gx >= 0 && gy >= 0 && gx < w && gy < h) ? load_px(src, job.src_pitch_bytes, gx, gy) : 0.f;
+      const bool in = gx >= 0 && gy >= 0 && gx < w && gy < h;
+      if constexpr (sizeof(InT) == 4) {
+        if (in) {
+          cp_async4(dst + i, reinterpret_cast<const float*>(reinterpret_cast<const char*>(src) +
+                                                            (int64_t)gy * job.src_pitch_bytes) + gx);
+        } else {
+          dst[i] = 0.f;
+        }
+      } else {
+        dst[i] = in ? load_px(src, job.src_pitch_bytes, gx, gy) : 0.f;
+      }
+    }
+    if constexpr (sizeof(InT) == 4) cp_async_wait_all();
+    __syncthreads();
+    if (job.scale != 1.f) {
+      for (int i = threadIdx.x; i < S[0] * S[0]; i += kThreads) dst[i] = __fmul_rn(dst[i], job.scale);
+      __syncthreads();
     }
   }
-  __syncthreads();
 
   // 2. deeper levels inside shared memory
 #pragma unroll

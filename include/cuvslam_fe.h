@@ -221,6 +221,79 @@ FE_API int fe_batch_kernel_count(fe_batch* batch);
 FE_API int fe_batch_run_plain(fe_batch* batch, fe_stream stream);
 FE_API int fe_batch_destroy(fe_batch* batch);
 
+/* ---------------------------------------------------------------------------------------- */
+/* Differentiable LK and its adjoint (no counterpart in the reference, which has no backward)  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* The differentiable tracker is fe_track with FE_SAMPLE_EXACT and one of two iteration rules:
+ *   FE_ADJOINT_IMPLICIT: the reference rule on every level (<= 11 steps, stop at |v| < 0.12 px,
+ *     radius and NCC gates), then at level 0 up to `iterations` further steps c += v, stopping
+ *     after the first with |v| < tolerance: the result is the fixed point e(c*) = 0 whose
+ *     implicit-function-theorem derivative the adjoint takes.
+ *   FE_ADJOINT_UNROLLED: exactly `iterations` (1..16) steps on every level, no early stop; a level
+ *     is accepted when its last |v| < 0.12 px and the gates pass.  The adjoint differentiates every
+ *     step, re-sampling the patches from the pyramids instead of storing them.
+ * Pixel values are those of the pyramid (the reference tracker works at uint8 intensity scale:
+ * its H carries +1 on the diagonal). */
+typedef enum { FE_ADJOINT_IMPLICIT = 0, FE_ADJOINT_UNROLLED = 1 } fe_adjoint_mode;
+
+/* One camera of a differentiable tracking step.  Pointers are device memory except prev/cur. */
+typedef struct {
+  const fe_pyramid* prev;          /* previous frame (image + gradients, e.g. fe_build_pyramid_f32) */
+  const fe_pyramid* cur;           /* current frame, same level sizes */
+  const fe_track_data* tracks_in;  /* forward input records (not modified) */
+  fe_track_data* tracks_out;       /* forward output records; the implicit adjoint reads them */
+  int32_t n_tracks;                /* <= 16384 */
+  const float* grad_xy;            /* backward input, n x 2: dL/d(output track position) */
+  float* grad_prev;                /* backward output: dL/d(level-0 previous image), written */
+  int64_t grad_prev_pitch_bytes;
+  float* grad_cur;                 /* backward output: dL/d(level-0 current image), written */
+  int64_t grad_cur_pitch_bytes;
+  float* grad_track;               /* n x 2 or NULL: dL/d(tracks_in position) */
+  float* grad_offset;              /* n x 2 or NULL: dL/d(tracks_in offset); 0 in implicit mode */
+  const float* prev_image;         /* optional level-0 FP32 frames that fe_adjoint_build_pyramids */
+  const float* cur_image;          /*   turns into prev / cur, multiplied by image_scale on load */
+  int64_t image_pitch_bytes;
+  float image_scale;
+} fe_adjoint_job;
+
+typedef struct fe_adjoint fe_adjoint;
+
+/* Plans the differentiable step over njobs cameras (<= 64): allocates all scratch and copies the
+ * descriptors once, so that forward and backward allocate nothing and can be captured into a CUDA
+ * graph.  Failed tracks get zero gradients.  Deterministic: the per-pixel gradient sums run in a
+ * fixed order (tracks in index order per 32x32 tile), no floating-point atomics. */
+FE_API int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, int mode, int iterations,
+                             float tolerance, fe_adjoint** out);
+/* Builds prev and cur of every job that names its frames (prev_image, cur_image) as
+ * fe_build_pyramid_f32 would from image_scale * frame, all jobs in the same few launches. */
+FE_API int fe_adjoint_build_pyramids(fe_adjoint* adj, fe_stream stream);
+/* The differentiable tracker over all jobs: tracks_in -> tracks_out (one launch).  In unrolled
+ * mode it also records every level's iterates for the backward. */
+FE_API int fe_adjoint_forward(fe_adjoint* adj, fe_stream stream);
+/* The vector-Jacobian product over all jobs: grad_xy -> grad_prev, grad_cur, grad_track,
+ * grad_offset.  Reads the pyramids, so they must hold the forward's frames (rebuilt or kept).
+ * Unrolled mode uses the iterates the plan's last forward recorded; before any forward it replays
+ * the forward itself. */
+FE_API int fe_adjoint_backward(fe_adjoint* adj, fe_stream stream);
+/* Kernel launches of one forward (backward = 0), backward (1) or build_pyramids (2) call. */
+FE_API int fe_adjoint_kernel_count(const fe_adjoint* adj, int backward);
+/* Enqueues a copy, into the device int32 at `device_out`, of the number of tracks of the last
+ * backward whose unrolled iterates on one level spread over more than 20 texels: those get NaN
+ * position gradients and contribute nothing to the image gradients. */
+FE_API int fe_adjoint_dropped(const fe_adjoint* adj, int32_t* device_out, fe_stream stream);
+FE_API int fe_adjoint_destroy(fe_adjoint* adj);
+
+/* One-camera conveniences (plan, run, synchronise the stream, free). */
+FE_API int fe_track_diff(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur,
+                         const fe_track_data* tracks_in, fe_track_data* tracks_out, int n, int mode, int iterations,
+                         float tolerance, fe_stream stream);
+FE_API int fe_track_backward(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur,
+                             const fe_track_data* tracks_in, const fe_track_data* tracks_out, int n, int mode,
+                             int iterations, float tolerance, const float* grad_xy, float* grad_prev,
+                             int64_t grad_prev_pitch_bytes, float* grad_cur, int64_t grad_cur_pitch_bytes,
+                             float* grad_track, float* grad_offset, fe_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,7 +11,8 @@
  *              __fdividef, whose implementations are not ours to restate, are replaced by logf
  *              and IEEE division.
  *   cpu_*    : the reference CPU path (libs/sof, use_gpu=false), the timed CPU baseline.
- * plus an FP64 LK (or_lk_track_f64) used only to state per-track error.
+ * plus an FP64 LK (or_lk_track_f64) used only to state per-track error, and an FP64
+ * differentiable LK with its adjoint (or64_*) that pins the CUDA adjoint.
  */
 #ifndef FE_ORACLE_H
 #define FE_ORACLE_H
@@ -62,6 +63,25 @@ void or_lk_track_horizontal(int levels, const int* ws, const int* hs, const floa
 void or_lk_track_f64(int levels, const int* ws, const int* hs, const float* const* prev_gx,
                      const float* const* prev_gy, const float* const* prev_img, const float* const* cur_img,
                      or_track_data* td, int n);
+
+/* FP64 differentiable LK tracker and its adjoint (lk_adjoint64.c). */
+enum { OR64_IMPLICIT = 0, OR64_UNROLLED = 1 };
+typedef struct or64_cam or64_cam;
+or64_cam* or64_cam_create(int w, int h, int max_levels);
+void or64_cam_destroy(or64_cam* c);
+int or64_cam_levels(const or64_cam* c);
+void or64_cam_set(or64_cam* c, const double* prev0, const double* cur0);
+void or64_cam_plane(const or64_cam* c, int level, int plane, double* out);
+void or64_track(const or64_cam* c, const or_track_data* in, int n, int mode, int iters, double tol, double* out_xy,
+                uint8_t* status);
+void or64_backward(or64_cam* c, const or_track_data* in, int n, int mode, int iters, double tol,
+                   const double* grad_xy, double* grad_prev0, double* grad_cur0, double* grad_track,
+                   double* grad_offset);
+void or64_debug_skip_pyramid_adjoint(int on);
+void or64_cam_adjoint_plane(const or64_cam* c, int level, int plane, double* out);
+void or64_fd(or64_cam* c, const double* prev0, const double* cur0, const or_track_data* in, int n, int mode,
+             int iters, double tol, const double* gt, const uint8_t* mask, int nq, const int* which,
+             const int64_t* index, double h, double* out);
 
 #ifdef __cplusplus
 }

@@ -255,3 +255,88 @@ def cpu_frame_step(prev_cams, cur_cams, images, xy, pred, num_desired, nthreads)
                          PA(*[a.ctypes.data for a in outs]), PA(*[a.ctypes.data for a in sts]),
                          PA(*[a.ctypes.data for a in news]), _p(counts), n, nthreads)
     return outs, sts, [a[:c] for a, c in zip(news, counts)]
+
+
+# ---------------------------------------------------------------- FP64 differentiable LK (lk_adjoint64.c)
+IMPLICIT = 0
+UNROLLED = 1
+
+_L64_SIGS = [
+    ("or64_cam_create", [I, I, I], P),
+    ("or64_cam_destroy", [P], None),
+    ("or64_cam_levels", [P], I),
+    ("or64_cam_set", [P, P, P], None),
+    ("or64_cam_plane", [P, I, I, P], None),
+    ("or64_track", [P, P, I, I, I, ctypes.c_double, P, P], None),
+    ("or64_backward", [P, P, I, I, I, ctypes.c_double, P, P, P, P, P], None),
+    ("or64_fd", [P, P, P, P, I, I, I, ctypes.c_double, P, P, I, P, P, ctypes.c_double, P], None),
+]
+
+
+def _l64():
+    L = lib()
+    if not getattr(L, "_l64_ready", False):
+        for name, args, res in _L64_SIGS:
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        L._l64_ready = True
+    return L
+
+
+class Diff64:
+    """FP64 differentiable LK on one camera: pyramids of a previous and a current level-0 image
+    (float64), the forward tracker in both adjoint modes, its vector-Jacobian product, and
+    central finite differences of the mean squared distance to ground truth."""
+
+    def __init__(self, prev0, cur0, max_levels=10):
+        self.prev = np.ascontiguousarray(prev0, np.float64)
+        self.cur = np.ascontiguousarray(cur0, np.float64)
+        self.h, self.w = self.prev.shape
+        L = _l64()
+        self.h_ = L.or64_cam_create(self.w, self.h, max_levels)
+        L.or64_cam_set(self.h_, _p(self.prev), _p(self.cur))
+        self.levels = L.or64_cam_levels(self.h_)
+
+    def plane(self, level, plane):
+        lw, lh = level_sizes(self.w, self.h)[level]
+        out = np.zeros((lh, lw), np.float64)
+        _l64().or64_cam_plane(self.h_, level, plane, _p(out))
+        return out
+
+    def track(self, tracks, mode, iters, tol=1e-13):
+        tracks = np.ascontiguousarray(tracks)
+        n = len(tracks)
+        xy = np.zeros((n, 2), np.float64)
+        st = np.zeros(n, np.uint8)
+        _l64().or64_track(self.h_, _p(tracks), n, mode, iters, tol, _p(xy), _p(st))
+        return xy, st
+
+    def backward(self, tracks, mode, iters, grad_xy, tol=1e-13):
+        tracks = np.ascontiguousarray(tracks)
+        n = len(tracks)
+        g = np.ascontiguousarray(grad_xy, np.float64).reshape(n, 2)
+        gp = np.zeros((self.h, self.w), np.float64)
+        gc = np.zeros((self.h, self.w), np.float64)
+        gt = np.zeros((n, 2), np.float64)
+        go = np.zeros((n, 2), np.float64)
+        _l64().or64_backward(self.h_, _p(tracks), n, mode, iters, tol, _p(g), _p(gp), _p(gc), _p(gt), _p(go))
+        return gp, gc, gt, go
+
+    def fd(self, tracks, mode, iters, gt_xy, mask, which, index, h=1e-3, tol=1e-13):
+        tracks = np.ascontiguousarray(tracks)
+        n = len(tracks)
+        gt = np.ascontiguousarray(gt_xy, np.float64).reshape(n, 2)
+        m = np.ascontiguousarray(mask, np.uint8)
+        wh = np.ascontiguousarray(which, np.int32)
+        ix = np.ascontiguousarray(index, np.int64)
+        out = np.zeros(len(wh), np.float64)
+        _l64().or64_fd(self.h_, _p(self.prev), _p(self.cur), _p(tracks), n, mode, iters, tol, _p(gt), _p(m), len(wh),
+                       _p(wh), _p(ix), h, _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            _l64().or64_cam_destroy(self.h_)
+        except Exception:
+            pass
