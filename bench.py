@@ -46,8 +46,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", choices=["pyramid", "lk", "select"], default=None,
-                    help="run only this part of the step (warmup + steps launches) for an ncu capture")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
+    ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step"], default=None,
+                    help="for an ncu capture: run only this part of the step (inside NVTX ranges named "
+                         "'part'), or whole batched steps (ranges named 'step'), warmup + steps times")
     return ap.parse_args()
 
 
@@ -188,6 +190,61 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+ADJ_CAMS, ADJ_W, ADJ_H, ADJ_TRACKS = 8, 1280, 720, 4096
+
+
+def adjoint_bench(ctx, dev, stream, timed, reps=20):
+    """LK adjoint workload: 8 cameras at 1280x720, FP32 frames in [0, 1], 4096 Shi-Tomasi tracks each,
+    loss = mean squared distance to the warp's ground truth.  Per mode: forward (both pyramids of
+    every camera + the differentiable tracker) and backward (the adjoint) times, their ratio, and
+    the kernel launches of each."""
+    import torch
+
+    from cuvslam_b200 import synthetic as S
+    from cuvslam_b200.diff import DiffTracker
+    from cuvslam_b200.frontend import ImagePyramid, Selection
+
+    sel = Selection(ctx)
+    prev, cur, xy, gt = [], [], [], []
+    for b in range(ADJ_CAMS):
+        p8, c8, warp = S.frame_pair(100 + b, ADJ_W, ADJ_H)
+        pp = ImagePyramid(ADJ_W, ADJ_H, device=dev).build(ctx, torch.from_numpy(p8).to(dev))
+        f = sel.compute_gftt_and_select_features(pp, 0, 0, 0, 0, None, None, ADJ_TRACKS).reshape(-1, 2).cpu()
+        f = torch.cat([f] * (ADJ_TRACKS // max(len(f), 1) + 1))[:ADJ_TRACKS]
+        gx, gy = warp.apply(f[:, 0].double().numpy(), f[:, 1].double().numpy())
+        prev.append(torch.from_numpy(p8.astype(np.float32) / 255.0))
+        cur.append(torch.from_numpy(c8.astype(np.float32) / 255.0))
+        xy.append(f)
+        gt.append(torch.from_numpy(np.stack([gx, gy], 1).astype(np.float32)))
+    prev, cur = torch.stack(prev).to(dev), torch.stack(cur).to(dev)
+    xy, gt = torch.stack(xy).to(dev), torch.stack(gt).to(dev)
+    out = {"workload": f"{ADJ_CAMS} cameras {ADJ_W}x{ADJ_H}, {ADJ_TRACKS} tracks each, FP32 frames in [0, 1]"}
+    for mode in ("implicit", "unrolled"):
+        t = DiffTracker(ctx, ADJ_CAMS, ADJ_H, ADJ_W, ADJ_TRACKS, mode=mode)
+        t.set_inputs(prev, cur, xy)
+        t.build_pyramids(stream)
+        t.forward_step(stream)
+        pos, st = t.outputs()
+        n = ADJ_CAMS * ADJ_TRACKS
+        t.grad_xy.copy_(torch.where(st[..., None], 2.0 * (pos - gt) / n, torch.zeros_like(pos)))
+
+        def fwd():
+            t.build_pyramids(stream)
+            t.forward_step(stream)
+
+        def bwd():
+            t.backward_step(stream)
+
+        fwd_ms = timed(fwd, reps, 3) / reps
+        bwd_ms = timed(bwd, reps, 3) / reps
+        out[mode] = {"fwd_ms": fwd_ms, "bwd_ms": bwd_ms, "bwd_over_fwd": bwd_ms / fwd_ms,
+                     "tracks_kept": int(st.sum().item()), "dropped": t.dropped(),
+                     "fwd_launches": t.kernel_count(2) + t.kernel_count(0), "bwd_launches": t.kernel_count(1),
+                     "iterations": t.iterations}
+        t.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -233,12 +290,24 @@ def main():
         frames.append(CameraFrame(img_dev[i], cur_pyr[i], prev_pyr[i], td, counts[i], (0, 0, 0, 0)))
     batch = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)
     attempted = sum(len(t) for t in host_tracks)
+    if args.profile == "step":
+        for _ in range(args.warmup + args.steps):
+            torch.cuda.nvtx.range_push("step")
+            batch.run(stream)
+            torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "step", "steps": args.warmup + args.steps, "kernels_per_step": batch.kernel_count()}))
+        batch.close()
+        ctx.close()
+        return
     if args.profile:
         part_id = {"pyramid": 0, "lk": 1, "select": 2}[args.profile]
         batch.run_part(0, stream)
         batch.run_part(1, stream)
         for _ in range(args.warmup + args.steps):
+            torch.cuda.nvtx.range_push("part")
             batch.run_part(part_id, stream)
+            torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.profile, "launches": args.warmup + args.steps}))
         batch.close()
@@ -342,6 +411,10 @@ def main():
         cpu = {"value": att * nrep / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"full 32-camera frame step x {nrep}, restated reference CPU tracker, one camera per thread"}
 
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        adjoint = adjoint_bench(ctx, dev, stream, timed)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -359,6 +432,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": kernels_per_step * args.steps,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     batch.close()
