@@ -47,9 +47,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
-    ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step"], default=None,
+    ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled"], default=None,
                     help="for an ncu capture: run only this part of the step (inside NVTX ranges named "
-                         "'part'), or whole batched steps (ranges named 'step'), warmup + steps times")
+                         "'part'), whole batched steps (ranges named 'step'), or the LK adjoint workload's "
+                         "forward and backward in one mode (ranges 'fwd', 'bwd'), warmup + steps times")
     return ap.parse_args()
 
 
@@ -193,15 +194,12 @@ def run_reference(args, rank):
 ADJ_CAMS, ADJ_W, ADJ_H, ADJ_TRACKS = 8, 1280, 720, 4096
 
 
-def adjoint_bench(ctx, dev, stream, timed, reps=20):
-    """LK adjoint workload: 8 cameras at 1280x720, FP32 frames in [0, 1], 4096 Shi-Tomasi tracks each,
-    loss = mean squared distance to the warp's ground truth.  Per mode: forward (both pyramids of
-    every camera + the differentiable tracker) and backward (the adjoint) times, their ratio, and
-    the kernel launches of each."""
+def adjoint_inputs(ctx, dev):
+    """LK adjoint workload: 8 cameras at 1280x720, FP32 frames in [0, 1], 4096 Shi-Tomasi tracks each
+    (selected on the previous frame; repeated when a frame has fewer), and the warp's ground truth."""
     import torch
 
     from cuvslam_b200 import synthetic as S
-    from cuvslam_b200.diff import DiffTracker
     from cuvslam_b200.frontend import ImagePyramid, Selection
 
     sel = Selection(ctx)
@@ -216,17 +214,34 @@ def adjoint_bench(ctx, dev, stream, timed, reps=20):
         cur.append(torch.from_numpy(c8.astype(np.float32) / 255.0))
         xy.append(f)
         gt.append(torch.from_numpy(np.stack([gx, gy], 1).astype(np.float32)))
-    prev, cur = torch.stack(prev).to(dev), torch.stack(cur).to(dev)
-    xy, gt = torch.stack(xy).to(dev), torch.stack(gt).to(dev)
+    return torch.stack(prev).to(dev), torch.stack(cur).to(dev), torch.stack(xy).to(dev), torch.stack(gt).to(dev)
+
+
+def adjoint_tracker(ctx, mode, inputs, stream):
+    """A DiffTracker over the adjoint workload after one forward, with dL/dpos of the mean squared
+    distance to ground truth loaded as its backward input."""
+    import torch
+
+    from cuvslam_b200.diff import DiffTracker
+
+    prev, cur, xy, gt = inputs
+    t = DiffTracker(ctx, ADJ_CAMS, ADJ_H, ADJ_W, ADJ_TRACKS, mode=mode)
+    t.set_inputs(prev, cur, xy)
+    t.build_pyramids(stream)
+    t.forward_step(stream)
+    pos, st = t.outputs()
+    n = ADJ_CAMS * ADJ_TRACKS
+    t.grad_xy.copy_(torch.where(st[..., None], 2.0 * (pos - gt) / n, torch.zeros_like(pos)))
+    return t, st
+
+
+def adjoint_bench(ctx, dev, stream, timed, reps=20):
+    """Per mode: forward (both pyramids of every camera + the differentiable tracker) and backward
+    (the adjoint) times, their ratio, and the kernel launches of each."""
+    inputs = adjoint_inputs(ctx, dev)
     out = {"workload": f"{ADJ_CAMS} cameras {ADJ_W}x{ADJ_H}, {ADJ_TRACKS} tracks each, FP32 frames in [0, 1]"}
     for mode in ("implicit", "unrolled"):
-        t = DiffTracker(ctx, ADJ_CAMS, ADJ_H, ADJ_W, ADJ_TRACKS, mode=mode)
-        t.set_inputs(prev, cur, xy)
-        t.build_pyramids(stream)
-        t.forward_step(stream)
-        pos, st = t.outputs()
-        n = ADJ_CAMS * ADJ_TRACKS
-        t.grad_xy.copy_(torch.where(st[..., None], 2.0 * (pos - gt) / n, torch.zeros_like(pos)))
+        t, st = adjoint_tracker(ctx, mode, inputs, stream)
 
         def fwd():
             t.build_pyramids(stream)
@@ -245,6 +260,30 @@ def adjoint_bench(ctx, dev, stream, timed, reps=20):
     return out
 
 
+def profile_adjoint(args, local):
+    import torch
+
+    from cuvslam_b200.frontend import Context
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.current_stream()
+    t, _ = adjoint_tracker(ctx, args.profile, adjoint_inputs(ctx, torch.device("cuda", local)), stream)
+    for _ in range(args.warmup + args.steps):
+        torch.cuda.nvtx.range_push("fwd")
+        t.build_pyramids(stream)
+        t.forward_step(stream)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.nvtx.range_push("bwd")
+        t.backward_step(stream)
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile, "fwd_launches": t.kernel_count(2) + t.kernel_count(0),
+                      "bwd_launches": t.kernel_count(1)}))
+    t.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -253,6 +292,8 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank)
 
+    if args.profile in ("implicit", "unrolled"):
+        return profile_adjoint(args, local)
     shapes, counts, prevs, nexts = workload(seed_offset=rank)
     import torch
 

@@ -805,6 +805,7 @@ struct fe_adjoint {
   int mode = FE_ADJOINT_IMPLICIT, iters = 0;
   int L = 1, total = 0, nplanes = 0, total_tiles = 0;
   fe::LkLaunch lk;
+  fe::LkLaunch lk_replay;            // unrolled backward before any forward: records into scratch tracks
   fe::AdjLaunch adj;
   fe::AdjGather gat;
   std::vector<fe::AdjPyrLevel> pyr;  // [level]
@@ -933,10 +934,13 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   const size_t o_count = take(((size_t)tiles + 1) * 4);
   const size_t o_off = take(((size_t)tiles + 1) * 4);
   const size_t o_cursor = take(((size_t)tiles + 1) * 4);
+  const size_t o_long = take(((size_t)tiles + 2) * 4);
   const size_t o_list = take(std::max<size_t>(nslots * 4, 1) * 4);  // a record covers <= 4 tiles
   const size_t o_pl = take(planes.size() * sizeof(fe::AdjPlane));
   const size_t o_cams = take((size_t)njobs * sizeof(fe::AdjCam));
   const size_t o_lk = take((size_t)njobs * sizeof(fe::LkCam));
+  const size_t o_lk2 = take(mode == FE_ADJOINT_UNROLLED ? (size_t)njobs * sizeof(fe::LkCam) : 0);
+  const size_t o_rtr = take(mode == FE_ADJOINT_UNROLLED ? (size_t)std::max(total, 1) * sizeof(fe_track_data) : 0);
   const size_t o_recs = take(mode == FE_ADJOINT_UNROLLED ? std::max(total, 1) * fe::lk_record_bytes() : 0);
   const size_t o_ctr = take(256);
   cudaError_t e = cudaMalloc(&a->mem, o);
@@ -972,6 +976,11 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   e = cudaMemcpy(base + o_pl, planes.data(), planes.size() * sizeof(fe::AdjPlane), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(base + o_cams, cams.data(), cams.size() * sizeof(fe::AdjCam), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(base + o_lk, lks.data(), lks.size() * sizeof(fe::LkCam), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && mode == FE_ADJOINT_UNROLLED) {
+    std::vector<fe::LkCam> rl = lks;
+    for (auto& c : rl) c.tracks = (fe_track_data*)(base + o_rtr) + c.begin;
+    e = cudaMemcpy(base + o_lk2, rl.data(), rl.size() * sizeof(fe::LkCam), cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) return fail(cuda_fail(e));
 
   memset(&a->lk, 0, sizeof(a->lk));
@@ -983,9 +992,12 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   a->lk.mode = mode == FE_ADJOINT_UNROLLED ? fe::kLkUnrolled : fe::kLkImplicit;
   a->lk.iters = iterations;
   a->lk.tol2 = tolerance * tolerance;
+  a->lk_replay = a->lk;
   if (mode == FE_ADJOINT_UNROLLED) {
     a->recs = (fe::lk::LkRecord*)(base + o_recs);
     a->lk.recs = a->recs;
+    a->lk_replay.cams = (const fe::LkCam*)(base + o_lk2);
+    a->lk_replay.recs = a->recs;
   }
   for (int j = 0; j < njobs; ++j) {
     const fe_adjoint_job& J = jobs[j];
@@ -1025,6 +1037,8 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   a->gat.count = (int*)(base + o_count);
   a->gat.off = (int*)(base + o_off);
   a->gat.cursor = (int*)(base + o_cursor);
+  a->gat.long_count = (int*)(base + o_long);
+  a->gat.long_tiles = (int*)(base + o_long) + 1;
   a->gat.list = (int*)(base + o_list);
   a->gat.list_cap = next_pow2(max_n);
 
@@ -1059,6 +1073,7 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
         }
         J.px_begin = px;
         px += P.w * P.h;
+        lv.max_blocks = std::max(lv.max_blocks, ((P.w + 31) / 32) * ((P.h + 7) / 8));
       }
     }
     lv.total_px = px;
@@ -1082,7 +1097,10 @@ int fe_adjoint_forward(fe_adjoint* a, fe_stream stream) {
 int fe_adjoint_backward(fe_adjoint* a, fe_stream stream) {
   if (!a) return FE_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
-  a->adj.recs = a->forward_ran ? a->recs : nullptr;
+  a->adj.recs = a->recs;
+  // the unrolled adjoint replays the recorded steps: without a forward of this plan, record them now
+  // (the tracks of this replay go to scratch)
+  if (a->mode == FE_ADJOINT_UNROLLED && !a->forward_ran) FE_CUDA(fe::launch_lk(a->lk_replay, st));
   FE_CUDA(cudaMemsetAsync(a->adj.overflow, 0, sizeof(int), st));
   FE_CUDA(fe::launch_lk_adjoint(a->adj, st));
   FE_CUDA(fe::launch_adjoint_gather(a->gat, st));
@@ -1099,7 +1117,8 @@ int fe_adjoint_kernel_count(const fe_adjoint* a, int backward) {
   }
   if (!backward) return a->total > 0 ? 1 : 0;
   int n = a->total > 0 ? 1 : 0;              // adjoint
-  if (a->total_tiles > 0) n += a->gat.nslots > 0 ? 4 : 2;  // count, scan, fill, gather
+  if (a->total > 0 && a->mode == FE_ADJOINT_UNROLLED && !a->forward_ran) ++n;  // the replayed forward
+  if (a->total_tiles > 0) n += a->gat.nslots > 0 ? 5 : 3;  // count, scan, fill, short and long gathers
   for (int l = 0; l < a->L; ++l) n += a->pyr[l].total_px > 0 ? 1 : 0;
   return n;
 }

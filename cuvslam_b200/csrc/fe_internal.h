@@ -144,7 +144,7 @@ struct AdjLaunch {
   int mode, iters;                   // kLkImplicit / kLkUnrolled
   int L;                             // record levels (1 implicit; deepest pyramid unrolled)
   int cur_s;                         // current-image record edge: 12 implicit, 32 unrolled
-  const lk::LkRecord* recs;          // unrolled: the forward's records, or null (replay the forward)
+  const lk::LkRecord* recs;          // unrolled: the forward's per-track records
   int4* hdr;                         // [4][L][total] {x0, y0, w, h}; w == 0: empty
   float* data_prev;                  // [3][L][total][12 * 12]
   float* data_cur;                   // [L][total][cur_s * cur_s]
@@ -167,6 +167,8 @@ struct AdjGather {
   int* count;                        // [total_tiles]
   int* off;                          // [total_tiles + 1]
   int* cursor;                       // [total_tiles]
+  int* long_tiles;                   // tiles with more than 32 records ([total_tiles]), and their
+  int* long_count;                   //   number
   int* list;
   int list_cap;                      // power of two >= the longest list (tracks of one camera)
 };
@@ -183,6 +185,7 @@ struct AdjPyrJob {
 
 struct AdjPyrLevel {
   int njobs, total_px;
+  int max_blocks;                    // 32x8-pixel blocks of the largest job
   AdjPyrJob job[2 * kMaxCams];
 };
 

@@ -13,8 +13,9 @@
 // dL/dtheta = -lambda^T de/dtheta, i.e. per tap
 //   dL/dP2 = u - mean u, dL/dP1 = -(u - mean u), u = -w (lambda . g),
 //   dL/dGx = ab - mean ab, ab = -w r lambda_x  (Gy likewise).
-// Unrolled mode: the replayed forward (lk_track.cuh records the iterates) is differentiated step by
-// step backwards, patches re-sampled from the pyramids rather than stored:
+// Unrolled mode: the forward's record of every step (iterate, update v, brightness offset; written by
+// lk_track.cuh) is differentiated step by step backwards, patches re-sampled from the pyramids
+// rather than stored:
 //   mu = H^-1 cbar, Hbar -= mu v^T, dL/dP2 = u - mean u with u = w (mu . g), cbar += sum dL/dP2 dP2/dc,
 //   dL/dP1 -= dL/dP2, abar += w r mu_x, bbar += w r mu_y; after the level
 //   abar += w (2 Hbar_xx a + (Hbar_xy + Hbar_yx) b), bbar likewise, dL/dGx = abar - mean abar.
@@ -40,11 +41,11 @@ constexpr int kRP = 12;  // previous-image record edge (the template's 12x12 win
 constexpr int kTile = 32;
 constexpr int kGatherThreads = 256;
 constexpr int kGatherWarps = kGatherThreads / 32;
+constexpr int kWarpList = 32;  // most records per tile that one warp sums (gather_warp_kernel)
+constexpr int kLongBlocks = 296;  // CTAs of gather_long_kernel (two per SM), looping over the long tiles
 
 struct AdjSmem {
   WarpSmem win;               // staging windows, as the forward
-  LkRecord rec;               // the replayed forward (unrolled)
-  fe_track_data td;           // the replayed record (unrolled)
   float acc[32 * 32];         // current-image record
   float prec[3][kRP * kRP];   // previous-image records
   float coef[3][81];          // tap coefficients (serial scatter)
@@ -389,36 +390,22 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
     return;
   }
 
-  // ---- unrolled: the forward's record of every level's iterates (or a replay of the forward)
-  __syncwarp();
-  if (p.recs) {
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(p.recs + g);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.rec);
-    for (int k = lane; k < (int)(sizeof(LkRecord) / 4); k += 32) dst[k] = src[k];
-    __syncwarp();
-    // level 0 accepted <=> the track is tracked
-    if (sm.rec.flags[0] != 3 || !gfinite) return drop(0.f);
-  } else {
-    if (lane < 20) reinterpret_cast<uint32_t*>(&sm.td)[lane] = reinterpret_cast<const uint32_t*>(&tin)[lane];
-    __syncwarp();
-    track_one<FE_SAMPLE_EXACT, false, kModeUnrolled>(cam.lk, sm.td, sm.win, lane, p.iters, 0.f, &sm.rec);
-    __syncwarp();
-    if (!sm.td.track_status || !gfinite) return drop(0.f);
-  }
-  // current-image record boxes of the accepted levels must fit cur_s x cur_s
+  // ---- unrolled: the forward's record of every level (p.recs, global memory; uniform loads)
+  const LkRecord& R = p.recs[g];
+  if (R.flags[0] != 3 || !gfinite) return drop(0.f);  // level 0 accepted <=> the track is tracked
+  // current-image record boxes of the accepted levels must fit cur_s x cur_s: taps of a patch reach
+  // texels [base, base + 10]; the record starts one texel left of the smallest base
   for (int level = 0; level <= top; ++level) {
-    if (sm.rec.flags[level] != 3) continue;
-    const int K = sm.rec.K[level];
+    if (R.flags[level] != 3) continue;
+    const int K = R.K[level];
     int lox = INT_MAX, hix = INT_MIN, loy = INT_MAX, hiy = INT_MIN;
     for (int t = 0; t < K; ++t) {
-      const float2 c = sm.rec.it[level][t];
+      const float2 c = R.it[level][t];
       lox = min(lox, patch_base(c.x));
       hix = max(hix, patch_base(c.x));
       loy = min(loy, patch_base(c.y));
       hiy = max(hiy, patch_base(c.y));
     }
-    // taps of a patch reach texels [base, base + 10]; the record starts one texel left of the
-    // smallest base
     if (hix - lox + 12 > p.cur_s || hiy - loy + 12 > p.cur_s) {
       if (lane == 0) atomicAdd(p.overflow, 1);
       return drop(__int_as_float(0x7fc00000));  // NaN: no gradient for this track
@@ -427,17 +414,17 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
   float cbx = gout.x, cby = gout.y;  // dL/d(end position of the level)
   float gtx = 0.f, gty = 0.f;
   for (int level = 0; level <= top; ++level) {
-    if (sm.rec.flags[level] == 3) {
+    if (R.flags[level] == 3) {
       const Level& PL = cam.lk.prev.lv[level];
       const Level& CL = cam.lk.cur.lv[level];
       const int W = CL.w, H = CL.h;
-      const float2 s = sm.rec.s[level];
+      const float2 s = R.s[level];
       Templ T;
       make_template(PL, s.x, s.y, valid, ix, iy, wt, sm, lane, T);
-      const int K = sm.rec.K[level];
+      const int K = R.K[level];
       int lox = INT_MAX, loy = INT_MAX, hix = INT_MIN, hiy = INT_MIN;
       for (int t = 0; t < K; ++t) {
-        const int bx = patch_base(sm.rec.it[level][t].x), by = patch_base(sm.rec.it[level][t].y);
+        const int bx = patch_base(R.it[level][t].x), by = patch_base(R.it[level][t].y);
         lox = min(lox, bx);
         loy = min(loy, by);
         hix = max(hix, bx);
@@ -450,47 +437,54 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
       for (int k = lane; k < rw * rh; k += 32) sm.acc[(k / rw) * rs + k % rw] = 0.f;
       __syncwarp();
       float p1b[kNE], ab[kNE], bb[kNE];
+      // per tap and bilinear corner, dL/dP2 weighted by the corner's weight, summed over the steps
+      // that share one uniform, unclamped tap base (pbx, pby); added to the record when the base
+      // changes and at the end of the level
+      float cs[kNE][4];
 #pragma unroll
-      for (int e = 0; e < kNE; ++e) p1b[e] = ab[e] = bb[e] = 0.f;
+      for (int e = 0; e < kNE; ++e) {
+        p1b[e] = ab[e] = bb[e] = 0.f;
+        cs[e][0] = cs[e][1] = cs[e][2] = cs[e][3] = 0.f;
+      }
+      int pbx = INT_MIN, pby = INT_MIN;
+      bool pending = false;
+      auto flush = [&]() {
+#pragma unroll
+        for (int corner = 0; corner < 4; ++corner) {
+          const int ox = corner & 1, oy = corner >> 1;
+#pragma unroll
+          for (int e = 0; e < kNE; ++e) {
+            if (valid[e]) {
+              const int o = (pby + iy[e] + oy - ry0) * rs + (pbx + ix[e] + ox - rx0);
+              sm.acc[o] = __fadd_rn(sm.acc[o], cs[e][corner]);
+            }
+            cs[e][corner] = 0.f;
+          }
+          __syncwarp();
+        }
+        pending = false;
+      };
       float hxx = 0.f, hxy = 0.f, hyx = 0.f, hyy = 0.f;
       int wbx = INT_MIN / 2, wby = INT_MIN / 2;
       for (int t = K - 1; t >= 0; --t) {
-        const float2 c = sm.rec.it[level][t];
+        const float2 c = R.it[level][t];
+        const float2 v = R.v[level][t];
+        const float delta = R.delta[level][t];
         const TapSet tc = cur_taps(CL, c.x, c.y, wbx, wby, sm, lane);
         float p2[kNE], dx[kNE], dy[kNE];
-        float sc = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
           p2[e] = dx[e] = dy[e] = 0.f;
           const Tap tp = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCS);
-          if (valid[e]) {
-            sample_vg(sm.win.cur, kCS, tp, p2[e], dx[e], dy[e]);
-            sc = __fadd_rn(sc, p2[e]);
-          }
+          if (valid[e]) sample_vg(sm.win.cur, kCS, tp, p2[e], dx[e], dy[e]);
         }
-        sc = warp_sum(sc);
-        const float delta = __fmul_rn(__fsub_rn(sc, T.sp), rcp81);
-        float r[kNE], ex = 0.f, ey = 0.f;
-#pragma unroll
-        for (int e = 0; e < kNE; ++e) {
-          r[e] = 0.f;
-          if (valid[e]) {
-            r[e] = __fsub_rn(__fsub_rn(p2[e], T.p1[e]), delta);
-            const float wd = __fmul_rn(wt[e], r[e]);
-            ex = __fmaf_rn(wd, T.a[e], ex);
-            ey = __fmaf_rn(wd, T.b[e], ey);
-          }
-        }
-        ex = warp_sum(ex);
-        ey = warp_sum(ey);
-        const float vx = __fmul_rn(__fmaf_rn(T.gyy, ex, -__fmul_rn(T.gxy, ey)), T.det_rcp);
-        const float vy = __fmul_rn(__fmaf_rn(T.gxx, ey, -__fmul_rn(T.gxy, ex)), T.det_rcp);
+        // v = H^-1 e is recorded; mu = H^-1 cbar, Hbar -= mu v^T
         const float mux = __fmul_rn(__fmaf_rn(T.gyy, cbx, -__fmul_rn(T.gxy, cby)), T.det_rcp);
         const float muy = __fmul_rn(__fmaf_rn(T.gxx, cby, -__fmul_rn(T.gxy, cbx)), T.det_rcp);
-        hxx = __fmaf_rn(-mux, vx, hxx);
-        hxy = __fmaf_rn(-mux, vy, hxy);
-        hyx = __fmaf_rn(-muy, vx, hyx);
-        hyy = __fmaf_rn(-muy, vy, hyy);
+        hxx = __fmaf_rn(-mux, v.x, hxx);
+        hxy = __fmaf_rn(-mux, v.y, hxy);
+        hyx = __fmaf_rn(-muy, v.x, hyx);
+        hyy = __fmaf_rn(-muy, v.y, hyy);
         float u[kNE], su = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
@@ -510,17 +504,34 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
             gx = __fmaf_rn(p2b[e], dx[e], gx);
             gy = __fmaf_rn(p2b[e], dy[e], gy);
             p1b[e] = __fsub_rn(p1b[e], p2b[e]);
-            const float wr = __fmul_rn(wt[e], r[e]);
+            const float wr = __fmul_rn(wt[e], __fsub_rn(__fsub_rn(p2[e], T.p1[e]), delta));
             ab[e] = __fmaf_rn(wr, mux, ab[e]);
             bb[e] = __fmaf_rn(wr, muy, bb[e]);
           }
         }
-        float* const dst[1] = {sm.acc};
-        const float c1[1][kNE] = {{p2b[0], p2b[1], p2b[2]}};
-        scatter_taps<1>(dst, rs, rx0, ry0, tc, c1, valid, ix, iy, W, H, sm, lane);
+        const int b0x = __shfl_sync(kFull, tc.base, 0), b0y = __shfl_sync(kFull, tc.base, 16);
+        const bool fast = tc.uniform && b0x >= 0 && b0y >= 0 && b0x + 9 <= W - 1 && b0y + 9 <= H - 1;
+        if (pending && !(fast && b0x == pbx && b0y == pby)) flush();
+        if (fast) {
+          const float fx = tc.u.w00, fy = tc.u.w10;
+          const float qx = __fsub_rn(1.f, fx), qy = __fsub_rn(1.f, fy);
+          const float wc[4] = {__fmul_rn(qx, qy), __fmul_rn(fx, qy), __fmul_rn(qx, fy), __fmul_rn(fx, fy)};
+#pragma unroll
+          for (int e = 0; e < kNE; ++e)
+#pragma unroll
+            for (int corner = 0; corner < 4; ++corner) cs[e][corner] = __fmaf_rn(wc[corner], p2b[e], cs[e][corner]);
+          pbx = b0x;
+          pby = b0y;
+          pending = true;
+        } else {
+          float* const dst[1] = {sm.acc};
+          const float c1[1][kNE] = {{p2b[0], p2b[1], p2b[2]}};
+          scatter_taps<1>(dst, rs, rx0, ry0, tc, c1, valid, ix, iy, W, H, sm, lane);
+        }
         cbx = __fadd_rn(cbx, warp_sum(gx));
         cby = __fadd_rn(cby, warp_sum(gy));
       }
+      if (pending) flush();
       const float hs = __fadd_rn(hxy, hyx);
       float sa = 0.f, sb = 0.f;
 #pragma unroll
@@ -628,16 +639,21 @@ __global__ void bin_kernel(const __grid_constant__ AdjGather G) {
     }
 }
 
-// Exclusive prefix sum of the per-tile counts (one CTA); clears the fill cursors.
+// Exclusive prefix sum of the per-tile counts (one CTA); clears the fill cursors and lists the tiles
+// with more than kWarpList records.
 __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjGather G) {
   __shared__ int warp_tot[32];
   __shared__ int carry;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) carry = 0;
+  if (tid == 0) {
+    carry = 0;
+    *G.long_count = 0;
+  }
   __syncthreads();
   for (int base = 0; base < G.total_tiles; base += 1024) {
     const int t = base + tid;
     const int v = t < G.total_tiles ? G.count[t] : 0;
+    if (v > kWarpList) G.long_tiles[atomicAdd(G.long_count, 1)] = t;  // processing order is free
     int x = v;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -668,79 +684,139 @@ __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjG
   if (tid == 0) G.off[G.total_tiles] = carry;
 }
 
-// One CTA per tile: sorts the tile's records by slot (track order), sums them - warp k over the k-th
-// contiguous part of the sorted list into its own partial tile, then the partials in warp order -
-// and writes every texel of the tile.
-__global__ void __launch_bounds__(kGatherThreads) gather_kernel(const __grid_constant__ AdjGather G) {
-  extern __shared__ __align__(16) unsigned char gsm[];
-  float* part = reinterpret_cast<float*>(gsm);                         // [kGatherWarps][1024]
-  int* keys = reinterpret_cast<int*>(gsm + kGatherWarps * kTile * kTile * 4);  // [list_cap]
-  const int t = blockIdx.x;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+__device__ __forceinline__ const float* record_data(const AdjGather& G, int s, int& S) {
+  const int per_q = G.L * G.total;
+  if (s < 3 * per_q) {
+    S = kRP;
+    return G.data_prev + (size_t)s * (kRP * kRP);
+  }
+  S = G.cur_s;
+  return G.data_cur + (size_t)(s - 3 * per_q) * (G.cur_s * G.cur_s);
+}
+
+__device__ __forceinline__ const AdjPlane& tile_plane(const AdjGather& G, int t) {
   // the last plane that begins at or before t (an empty plane shares its begin with the next one)
   int lo = 0, hi = G.nplanes - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (G.planes[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
   }
-  const AdjPlane& P = G.planes[lo];
+  return G.planes[lo];
+}
+
+// One warp adds records to its 32x32 tile at (X0, Y0): lane = column X0 + lane, acc[r] = row Y0 + r.
+// `key` is this lane's record slot (lanes 0..m-1 hold m records, in the order they are added).
+__device__ __forceinline__ void warp_add_records(const AdjGather& G, int key, int m, int X0, int Y0, float (&acc)[kTile],
+                                                 int lane) {
+  const int4 mine = lane < m ? G.hdr[key] : make_int4(0, 0, 0, 0);
+  const int X = X0 + lane;
+  for (int r = 0; r < m; ++r) {
+    const int k = __shfl_sync(kFull, key, r);
+    const int hx = __shfl_sync(kFull, mine.x, r), hy = __shfl_sync(kFull, mine.y, r);
+    const int hz = __shfl_sync(kFull, mine.z, r), hw = __shfl_sync(kFull, mine.w, r);
+    if (X < hx || X >= hx + hz || hy >= Y0 + kTile || hy + hw <= Y0) continue;
+    int S;
+    const float* d = record_data(G, k, S) + (X - hx);
+#pragma unroll
+    for (int row = 0; row < kTile; ++row) {
+      const int dy = Y0 + row - hy;
+      if (dy >= 0 && dy < hw) acc[row] += d[dy * S];
+    }
+  }
+}
+
+// Ascending sort of one key per lane across the warp (bitonic network on shuffles).
+__device__ __forceinline__ int warp_sort(int key, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const int other = __shfl_xor_sync(kFull, key, stride);
+      const bool up = (lane & size) == 0 || size == 32;
+      const bool lower = (lane & stride) == 0;
+      key = (lower == up) ? min(key, other) : max(key, other);
+    }
+  }
+  return key;
+}
+
+// Tiles with at most kWarpList records (nearly all): one warp per tile, 8 tiles per CTA; the warp
+// sorts the slots (track order) and adds the records in that order into its registers.
+__global__ void __launch_bounds__(kGatherThreads) gather_warp_kernel(const __grid_constant__ AdjGather G) {
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * kGatherWarps + (threadIdx.x >> 5);
+  if (t >= G.total_tiles) return;  // warp-uniform
+  const int begin = G.off[t], n = G.off[t + 1] - begin;
+  if (n > kWarpList) return;       // gather_long_kernel
+  const AdjPlane& P = tile_plane(G, t);
   const int lt = t - P.tile_begin;
   const int X0 = (lt % P.tiles_x) * kTile, Y0 = (lt / P.tiles_x) * kTile;
-  const int begin = G.off[t], n = min(G.off[t + 1] - begin, G.list_cap);
-  int np2 = 1;
-  while (np2 < n) np2 <<= 1;
-  for (int k = tid; k < np2; k += kGatherThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
-  const int nw = min(kGatherWarps, max(1, n / 16));
-  for (int k = tid; k < nw * kTile * kTile; k += kGatherThreads) part[k] = 0.f;
-  __syncthreads();
-  // bitonic sort, ascending
-  for (int size = 2; size <= np2; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int k = tid; k < np2; k += kGatherThreads) {
-        const int o = k ^ stride;
-        if (o > k) {
-          const int a = keys[k], b = keys[o];
-          const bool up = (k & size) == 0;
-          if ((a > b) == up) {
-            keys[k] = b;
-            keys[o] = a;
+  const int key = warp_sort(lane < n ? G.list[begin + lane] : INT_MAX, lane);
+  float acc[kTile];
+#pragma unroll
+  for (int r = 0; r < kTile; ++r) acc[r] = 0.f;
+  warp_add_records(G, key, n, X0, Y0, acc, lane);
+  const int X = X0 + lane;
+  if (X < P.w) {
+#pragma unroll
+    for (int r = 0; r < kTile; ++r)
+      if (Y0 + r < P.h) P.dst[(size_t)(Y0 + r) * P.pitch + X] = acc[r];
+  }
+}
+
+// Tiles with more than kWarpList records (coarse levels), from the scan's list: a CTA sorts the
+// tile's slots, warp k adds the k-th contiguous part of the sorted list (32 records at a time) into
+// its registers, and the eight partial tiles are summed in warp order.
+__global__ void __launch_bounds__(kGatherThreads) gather_long_kernel(const __grid_constant__ AdjGather G) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  float* part = reinterpret_cast<float*>(gsm);                                  // [kGatherWarps][1024]
+  int* keys = reinterpret_cast<int*>(gsm + kGatherWarps * kTile * kTile * 4);  // [list_cap]
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nlong = *G.long_count;
+  for (int li = blockIdx.x; li < nlong; li += gridDim.x) {
+    const int t = G.long_tiles[li];
+    const AdjPlane& P = tile_plane(G, t);
+    const int lt = t - P.tile_begin;
+    const int X0 = (lt % P.tiles_x) * kTile, Y0 = (lt / P.tiles_x) * kTile;
+    const int begin = G.off[t], n = min(G.off[t + 1] - begin, G.list_cap);
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    __syncthreads();  // the previous tile's readers of keys and part are done
+    for (int k = tid; k < np2; k += kGatherThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
+    __syncthreads();
+    for (int size = 2; size <= np2; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int k = tid; k < np2; k += kGatherThreads) {
+          const int o = k ^ stride;
+          if (o > k) {
+            const int a = keys[k], b = keys[o];
+            if ((a > b) == ((k & size) == 0)) {
+              keys[k] = b;
+              keys[o] = a;
+            }
           }
         }
+        __syncthreads();
       }
-      __syncthreads();
     }
-  }
-  if (wid < nw) {
-    float* mine = part + wid * kTile * kTile;
-    const int r0 = (int)((long long)n * wid / nw), r1 = (int)((long long)n * (wid + 1) / nw);
-    const int per_q = G.L * G.total;
-    for (int k = r0; k < r1; ++k) {
-      const int s = keys[k];
-      const int4 h = G.hdr[s];
-      const int q = s / per_q;
-      const int S = q < 3 ? kRP : G.cur_s;
-      const float* d = q < 3 ? G.data_prev + (size_t)s * (kRP * kRP)
-                             : G.data_cur + (size_t)(s - 3 * per_q) * (G.cur_s * G.cur_s);
-      const int xa = max(h.x, X0), xb = min(h.x + h.z, X0 + kTile);
-      const int ya = max(h.y, Y0), yb = min(h.y + h.w, Y0 + kTile);
-      const int iw = xb - xa, ih = yb - ya;
-      if (iw > 0 && ih > 0) {
-        for (int idx = lane; idx < iw * ih; idx += 32) {
-          const int yy = idx / iw, xx = idx - yy * iw;
-          const int X = xa + xx, Y = ya + yy;
-          mine[(Y - Y0) * kTile + (X - X0)] += d[(Y - h.y) * S + (X - h.x)];
-        }
+    float acc[kTile];
+#pragma unroll
+    for (int r = 0; r < kTile; ++r) acc[r] = 0.f;
+    const int r0 = (int)((long long)n * wid / kGatherWarps), r1 = (int)((long long)n * (wid + 1) / kGatherWarps);
+    for (int g0 = r0; g0 < r1; g0 += 32) {
+      const int m = min(32, r1 - g0);
+      warp_add_records(G, lane < m ? keys[g0 + lane] : 0, m, X0, Y0, acc, lane);
+    }
+#pragma unroll
+    for (int r = 0; r < kTile; ++r) part[wid * kTile * kTile + r * kTile + lane] = acc[r];
+    __syncthreads();
+    for (int k = tid; k < kTile * kTile; k += kGatherThreads) {
+      const int X = X0 + (k & (kTile - 1)), Y = Y0 + k / kTile;
+      if (X < P.w && Y < P.h) {
+        float v = part[k];
+        for (int w = 1; w < kGatherWarps; ++w) v += part[w * kTile * kTile + k];
+        P.dst[(size_t)Y * P.pitch + X] = v;
       }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int k = tid; k < kTile * kTile; k += kGatherThreads) {
-    const int X = X0 + (k & (kTile - 1)), Y = Y0 + k / kTile;
-    if (X < P.w && Y < P.h) {
-      float v = part[k];
-      for (int w = 1; w < nw; ++w) v += part[w * kTile * kTile + k];
-      P.dst[(size_t)Y * P.pitch + X] = v;
     }
   }
 }
@@ -750,17 +826,13 @@ __device__ __forceinline__ float binom5(int k) {
   return k == 2 ? 6.f / 16.f : (k == 1 || k == 3) ? 4.f / 16.f : 1.f / 16.f;
 }
 
+// One launch per level; blockIdx.y = job (one pyramid of one camera), 32x8-pixel blocks.
 __global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_constant__ AdjPyrLevel L) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= L.total_px) return;
-  int lo = 0, hi = L.njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (L.job[mid].px_begin <= idx) lo = mid; else hi = mid - 1;
-  }
-  const AdjPyrJob& J = L.job[lo];
-  const int k = idx - J.px_begin;
-  const int y = k / J.w, x = k - y * J.w;
+  const AdjPyrJob& J = L.job[blockIdx.y];
+  const int bx = (J.w + 31) >> 5;
+  const int x = (int)(blockIdx.x % bx) * 32 + (threadIdx.x & 31);
+  const int y = (int)(blockIdx.x / bx) * 8 + (threadIdx.x >> 5);
+  if (x >= J.w || y >= J.h) return;
   float v = J.img[(size_t)y * J.pitch + x];
   if (J.gx) {
     // transposed 7-tap derivatives: gx(x') = sum_j D_j img(x' - 3 + j) for 2 < x' < w - 3
@@ -775,7 +847,20 @@ __global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_const
       if (yp > 2 && yp < J.h - 3) v = __fmaf_rn(dsp_tap(j), J.gy[(size_t)yp * J.gpitch + x], v);
     }
   }
-  if (J.up) {
+  if (J.up && x >= 2 && x <= J.w - 3 && y >= 2 && y <= J.h - 3) {
+    // interior: only unmirrored sources, 2X - 2 + k == x with k of x's parity (2 or 3 per axis)
+    for (int ky = y & 1; ky < 5; ky += 2) {
+      const int Y = (y + 2 - ky) >> 1;
+      if (Y >= J.up_h) continue;
+      const float* row = J.up + (size_t)Y * J.up_pitch;
+      const float wy = binom5(ky);
+      for (int kx = x & 1; kx < 5; kx += 2) {
+        const int X = (x + 2 - kx) >> 1;
+        if (X >= J.up_w) continue;
+        v = __fmaf_rn(__fmul_rn(wy, binom5(kx)), row[X], v);
+      }
+    }
+  } else if (J.up) {
     // transposed decimation: the outputs (X, Y) of the next level whose 5x5 taps read (x, y), either
     // directly (unmirrored source coordinate 2X - 2 + k == x) or through the mirror (-x-1 below 0,
     // 2n-x-1 above n-1); taps outside in both directions are skipped as the forward skips them
@@ -814,7 +899,7 @@ int lk_max_unrolled() { return kMaxRecIt; }
 size_t lk_record_bytes() { return sizeof(LkRecord); }
 
 cudaError_t adjoint_init() {
-  cudaError_t e = cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(gather_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kGatherWarps * kTile * kTile * 4 + kMaxSelectKeys * 4);
   return e;
 }
@@ -841,13 +926,14 @@ cudaError_t launch_adjoint_gather(const AdjGather& g, cudaStream_t s) {
   scan_kernel<<<1, 1024, 0, s>>>(g);
   if (nb > 0) bin_kernel<true><<<nb, 256, 0, s>>>(g);
   const size_t smem = kGatherWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4;
-  gather_kernel<<<g.total_tiles, kGatherThreads, smem, s>>>(g);
+  gather_warp_kernel<<<(g.total_tiles + kGatherWarps - 1) / kGatherWarps, kGatherThreads, 0, s>>>(g);
+  gather_long_kernel<<<kLongBlocks, kGatherThreads, smem, s>>>(g);
   return cudaGetLastError();
 }
 
 cudaError_t launch_pyramid_adjoint(const AdjPyrLevel& lv, cudaStream_t s) {
   if (lv.total_px <= 0) return cudaSuccess;
-  pyramid_adjoint_kernel<<<(lv.total_px + 255) / 256, 256, 0, s>>>(lv);
+  pyramid_adjoint_kernel<<<dim3(lv.max_blocks, lv.njobs), 256, 0, s>>>(lv);
   return cudaGetLastError();
 }
 

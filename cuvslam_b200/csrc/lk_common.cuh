@@ -137,13 +137,16 @@ __device__ __forceinline__ void sample_vg(const float* win, int stride, const Ta
   dy = __fsub_rn(bot, top);
 }
 
-// What the unrolled differentiable tracker did on each level, for its adjoint (per-warp shared
-// memory, written by lane 0): template position, the sampled iterates then the end position, the
-// number of steps, flags 1 = template built, 2 = level accepted.
+// What the unrolled differentiable tracker did on each level, for its adjoint (global memory, one
+// per track, written by lane 0): template position, the sampled iterates then the end position,
+// each step's update v and brightness offset delta = mean P2 - mean P1, the number of steps, flags
+// 1 = template built, 2 = level accepted.
 constexpr int kMaxRecIt = 16;
 struct LkRecord {
   float2 s[kMaxLevels];
   float2 it[kMaxLevels][kMaxRecIt + 1];
+  float2 v[kMaxLevels][kMaxRecIt];
+  float delta[kMaxLevels][kMaxRecIt];
   int K[kMaxLevels];
   int flags[kMaxLevels];
 };

@@ -151,6 +151,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
 #pragma unroll
       for (int e = 0; e < kNE; ++e) p2[e] = 0.f;
       int wbx = INT_MIN / 2, wby = INT_MIN / 2;  // current-frame window origin (none yet)
+      float last_delta = 0.f;
       // One Gauss-Newton step at (cx, cy): samples p2 and returns the update; false when the patch
       // leaves the level.
       auto gn_step = [&](float& vx, float& vy) -> bool {
@@ -179,6 +180,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
         }
         sc = warp_sum(sc);
         const float delta = __fmul_rn(__fsub_rn(sc, sp), rcp81);
+        last_delta = delta;
         float ex = 0.f, ey = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
@@ -211,6 +213,10 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
         }
         conv = HORIZ ? fabsf(vx) < 0.12f : __fmaf_rn(vx, vx, __fmul_rn(vy, vy)) < thr2;
         if (MODE != kModeUnrolled && conv) break;
+        if (MODE == kModeUnrolled && rec && lane == 0) {
+          rec->v[level][it] = make_float2(vx, vy);
+          rec->delta[level][it] = last_delta;
+        }
         cx = __fadd_rn(cx, vx);
         cy = __fadd_rn(cy, vy);
         ++steps;
