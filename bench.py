@@ -330,6 +330,7 @@ def main():
         pristine.append(td.clone())
         frames.append(CameraFrame(img_dev[i], cur_pyr[i], prev_pyr[i], td, counts[i], (0, 0, 0, 0)))
     batch = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)
+    tuning = batch.autotune(reps=10, stream=stream)  # restores the tracks it moved
     attempted = sum(len(t) for t in host_tracks)
     if args.profile == "step":
         for _ in range(args.warmup + args.steps):
@@ -462,7 +463,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "tracks_per_step": total_units, "cameras": len(shapes) * world,
-                       "l2": "working set > L2 (~600 MB of pyramids written per step)", "sampling": "texture"},
+                       "l2": "working set > L2 (~600 MB of pyramids written per step)", "sampling": "texture",
+                       "tuning": tuning},
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain / max(3, args.steps // 2)},
             "batched_over_plain": value / plain_value,
             "parts_ms": part_ms,

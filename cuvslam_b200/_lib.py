@@ -100,6 +100,9 @@ _SIGS = {
     "fe_batch_run_plain": (_I, [_P, _P]),
     "fe_batch_run_part": (_I, [_P, _I, _P]),
     "fe_batch_kernel_count": (_I, [_P]),
+    "fe_batch_autotune": (_I, [_P, _I, _P]),
+    "fe_batch_tuning": (_I, [_P, _P, _P, _P]),
+    "fe_batch_set_tuning": (_I, [_P, _I, _I, _I]),
     "fe_batch_destroy": (_I, [_P]),
     "fe_adjoint_create": (_I, [_P, ctypes.POINTER(FeAdjointJob), _I, _I, _I, ctypes.c_float, ctypes.POINTER(_P)]),
     "fe_adjoint_build_pyramids": (_I, [_P, _P]),

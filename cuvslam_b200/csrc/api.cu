@@ -88,6 +88,7 @@ fe::Pyr to_pyr(const fe_pyramid& p) {
 struct StageGroup {
   bool u8;
   int nl;
+  int kt;  // deepest-level tile of the generic stages (8 or 16)
   int tiles;
   fe::StageBatch batch;
 };
@@ -97,7 +98,7 @@ using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
 // writes levels 0..2; each later stage reads the deepest level of the previous one and writes up
 // to two more.
 int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan,
-                 float scale = 1.f) {
+                 float scale = 1.f, int kt = 8) {
   const fe::Pyr pyr = to_pyr(p);
   int s = 0;
   for (int stage = 0;; ++stage) {
@@ -113,7 +114,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.src_h = pyr.lv[s].h;
     for (int k = 0; k <= nl; ++k) job.out[k] = pyr.lv[s + k];
     const bool kind_u8 = stage == 0 && u8;
-    const int T = fe::stage_tile(kind_u8, nl);
+    const int T = fe::stage_tile(kind_u8, nl, kt);
     const fe::Level& deep = pyr.lv[s + nl];
     job.tiles_x = (deep.w + T - 1) / T;
     job.tiles_y = (deep.h + T - 1) / T;
@@ -128,6 +129,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
       memset(&g->batch, 0, sizeof(g->batch));
       g->u8 = kind_u8;
       g->nl = nl;
+      g->kt = kt;
       g->tiles = 0;
     }
     if (g->batch.njobs >= fe::kMaxCams) return FE_ERR_CAPACITY;
@@ -142,7 +144,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
 
 int run_plan(const StagePlan& plan, cudaStream_t st) {
   for (const auto& stage : plan)
-    for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, st));
+    for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, st));
   return FE_OK;
 }
 
@@ -488,6 +490,10 @@ struct fe_batch {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // shapes chosen by fe_batch_autotune (defaults until it runs)
+  int lk_shape = 0;      // LK block shape (fe::kLkShapes)
+  int overlap = 1;       // response tiles on a second stream beside LK
+  int stage_tile = 8;    // deepest-level tile of the generic pyramid stages
 };
 
 namespace {
@@ -517,9 +523,147 @@ int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side) {
   return FE_OK;
 }
 
+// (Re)captures the step with the batch's current shapes into its graph.
+int capture_batch(fe_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->lk.shape = b->lk_shape;
+  cudaError_t e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(e);
+  int rc = enqueue_batch(b, b->cap_stream, b->overlap ? b->side_stream : nullptr);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->cap_stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e);
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  return e == cudaSuccess ? FE_OK : cuda_fail(e);
+}
+
+// Re-plans the pyramid stages with the generic stages' tile `kt`.
+int replan_pyramids(fe_batch* b, int kt) {
+  StagePlan plan;
+  for (int i = 0; i < b->ncams; ++i) {
+    int rc = plan_pyramid(b->cams[i].image, b->cams[i].image_pitch_bytes, true, b->cur[i], plan, 1.f, kt);
+    if (rc) return rc;
+  }
+  b->plan = std::move(plan);
+  b->stage_tile = kt;
+  return FE_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
+  if (!b || reps <= 0) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the step moves the tracks: keep the originals and restore them before every timed step and at the end
+  size_t bytes = 0;
+  for (int i = 0; i < b->ncams; ++i)
+    if (b->has_prev[i]) bytes += (size_t)b->cams[i].n_tracks * sizeof(fe_track_data);
+  void* saved = nullptr;
+  if (bytes) FE_CUDA(cudaMalloc(&saved, bytes));
+  auto copy_tracks = [&](bool save) -> cudaError_t {
+    size_t o = 0;
+    for (int i = 0; i < b->ncams; ++i) {
+      if (!b->has_prev[i] || b->cams[i].n_tracks <= 0) continue;
+      const size_t n = (size_t)b->cams[i].n_tracks * sizeof(fe_track_data);
+      cudaError_t e = save ? cudaMemcpyAsync((char*)saved + o, b->cams[i].tracks, n, cudaMemcpyDeviceToDevice, st)
+                           : cudaMemcpyAsync(b->cams[i].tracks, (char*)saved + o, n, cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return e;
+      o += n;
+    }
+    return cudaSuccess;
+  };
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = FE_OK;
+  auto measure = [&](float* ms) -> int {
+    int r = capture_batch(b);
+    if (r) return r;
+    *ms = 0.f;
+    for (int k = 0; k < reps + 1; ++k) {  // the first step warms up
+      cudaError_t e = copy_tracks(false);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+      if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, st);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float t = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+      if (e != cudaSuccess) return cuda_fail(e);
+      if (k > 0) *ms += t;
+    }
+    return FE_OK;
+  };
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce == cudaSuccess) ce = copy_tracks(true);
+  if (ce != cudaSuccess) rc = cuda_fail(ce);
+  // coordinate descent over the three shapes, each candidate timed as whole graph launches
+  float best = 0.f;
+  if (!rc) rc = measure(&best);
+  for (int shape = 0; !rc && shape < fe::kLkShapes; ++shape) {
+    if (shape == b->lk_shape) continue;
+    const int keep = b->lk_shape;
+    b->lk_shape = shape;
+    float t = 0.f;
+    rc = measure(&t);
+    if (!rc && t < best) best = t;
+    else b->lk_shape = keep;
+  }
+  if (!rc && b->any_select && b->lk.total > 0) {
+    const int keep = b->overlap;
+    b->overlap = !keep;
+    float t = 0.f;
+    rc = measure(&t);
+    if (!rc && t < best) best = t;
+    else b->overlap = keep;
+  }
+  if (!rc) {
+    const int keep = b->stage_tile;
+    rc = replan_pyramids(b, keep == 8 ? 16 : 8);
+    float t = 0.f;
+    if (!rc) rc = measure(&t);
+    if (!rc && t < best) best = t;
+    else if (!rc) rc = replan_pyramids(b, keep);
+  }
+  if (!rc) rc = capture_batch(b);
+  if (!rc && bytes) {
+    ce = copy_tracks(false);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = cuda_fail(ce);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (saved) cudaFree(saved);
+  return rc;
+}
+
+int fe_batch_set_tuning(fe_batch* b, int lk_shape, int overlap, int stage_tile) {
+  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (stage_tile != 8 && stage_tile != 16))
+    return FE_ERR_INVALID_ARGUMENT;
+  b->lk_shape = lk_shape;
+  b->overlap = overlap ? 1 : 0;
+  if (stage_tile != b->stage_tile) {
+    int rc = replan_pyramids(b, stage_tile);
+    if (rc) return rc;
+  }
+  return capture_batch(b);
+}
+
+int fe_batch_tuning(const fe_batch* b, int32_t* lk_shape, int32_t* overlap, int32_t* stage_tile) {
+  if (!b) return FE_ERR_INVALID_ARGUMENT;
+  if (lk_shape) *lk_shape = b->lk_shape;
+  if (overlap) *overlap = b->overlap;
+  if (stage_tile) *stage_tile = b->stage_tile;
+  return FE_OK;
+}
 
 int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int sampling, fe_batch** out) {
   if (!ctx || !cams || !out || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
@@ -683,19 +827,8 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(cuda_fail(e));
-  e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return fail(cuda_fail(e));
-  int rc = enqueue_batch(b, b->cap_stream, b->side_stream);
-  cudaGraph_t g = nullptr;
-  e = cudaStreamEndCapture(b->cap_stream, &g);
-  if (rc) {
-    if (g) cudaGraphDestroy(g);
-    return fail(rc);
-  }
-  if (e != cudaSuccess) return fail(cuda_fail(e));
-  b->graph = g;
-  e = cudaGraphInstantiate(&b->exec, g, 0);
-  if (e != cudaSuccess) return fail(cuda_fail(e));
+  int rc = capture_batch(b);
+  if (rc) return fail(rc);
   *out = b;
   return FE_OK;
 }

@@ -29,12 +29,12 @@ struct StageBatch {
   StageJob job[kMaxCams];
 };
 
-int stage_tile(bool u8, int nl);  // deepest-level core tile edge of a stage kind
+int stage_tile(bool u8, int nl, int kt);  // deepest-level core tile edge of a stage kind (kt: 8 or 16)
 // Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
 // TMA alignment (the stage then stages its tile with ordinary loads).
 bool encode_frame_tmap(StageJob& job);
 cudaError_t pyramid_init();  // kernel attributes; call once per device before capture
-cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, cudaStream_t s);
+cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, cudaStream_t s);
 
 // ---------------------------------------------------------------- selection
 struct SelectCam {
@@ -118,11 +118,13 @@ struct LkLaunch {
   int mode;                     // kLk*
   int iters;                    // implicit: refinement steps at level 0; unrolled: steps per level
   float tol2;                   // implicit: squared step below which the refinement stops
+  int shape;                    // reference rule: block shape (kLkShapes), chosen by the batch autotuner
   lk::LkRecord* recs;           // unrolled: per-track records for the adjoint (may be null)
   LkCam single;                 // used when cams == nullptr
 };
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
+constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2
 
 // ---------------------------------------------------------------- LK adjoint
 // Per-track gradient contributions are written as window records (slot = (plane q, level l, track g),

@@ -34,15 +34,15 @@ namespace fe {
 
 namespace {
 
-constexpr int kWarps = 8;
 using namespace lk;
 
-template <int SAMPLING, bool HORIZ, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, 4) lk_kernel(const __grid_constant__ LkLaunch p) {
-  __shared__ WarpSmem smem[kWarps];
+// WARPS warps per block (one track each), at least MINB blocks per SM (which bounds the registers).
+template <int SAMPLING, bool HORIZ, int MODE, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) lk_kernel(const __grid_constant__ LkLaunch p) {
+  __shared__ WarpSmem smem[WARPS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const LkCam* cams = p.cams ? p.cams : &p.single;
-  int g = p.counter ? 0 : (int)blockIdx.x * kWarps + wid;
+  int g = p.counter ? 0 : (int)blockIdx.x * WARPS + wid;
   for (;;) {
     if (p.counter) {
       int v = 0;
@@ -70,25 +70,35 @@ __global__ void __launch_bounds__(kWarps * 32, 4) lk_kernel(const __grid_constan
   }
 }
 
-template <int SAMPLING, bool HORIZ, int MODE>
-int resident_blocks() {
-  static int blocks = 0;
-  if (!blocks) {
+template <int SAMPLING, bool HORIZ, int MODE, int WARPS, int MINB>
+cudaError_t launch_shape(const LkLaunch& p, cudaStream_t s) {
+  static int resident = 0;  // blocks of this shape resident on the device (persistent grid)
+  if (!resident) {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lk_kernel<SAMPLING, HORIZ, MODE>, kWarps * 32, 0);
-    blocks = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lk_kernel<SAMPLING, HORIZ, MODE, WARPS, MINB>, WARPS * 32, 0);
+    resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
-  return blocks;
+  int blocks = (p.total + WARPS - 1) / WARPS;
+  if (p.counter) blocks = min(blocks, resident);
+  lk_kernel<SAMPLING, HORIZ, MODE, WARPS, MINB><<<blocks, WARPS * 32, 0, s>>>(p);
+  return cudaGetLastError();
 }
 
+// Reference-rule launches take the block shape p.shape (kLkShapes); the differentiable modes use
+// the first.
 template <int SAMPLING, bool HORIZ, int MODE>
 cudaError_t launch(const LkLaunch& p, cudaStream_t s) {
-  int blocks = (p.total + kWarps - 1) / kWarps;
-  if (p.counter) blocks = min(blocks, resident_blocks<SAMPLING, HORIZ, MODE>());
-  lk_kernel<SAMPLING, HORIZ, MODE><<<blocks, kWarps * 32, 0, s>>>(p);
-  return cudaGetLastError();
+  if (MODE == kModeRef) {
+    switch (p.shape) {
+      case 1: return launch_shape<SAMPLING, HORIZ, MODE, 8, 3>(p, s);
+      case 2: return launch_shape<SAMPLING, HORIZ, MODE, 4, 8>(p, s);
+      case 3: return launch_shape<SAMPLING, HORIZ, MODE, 16, 2>(p, s);
+      default: break;
+    }
+  }
+  return launch_shape<SAMPLING, HORIZ, MODE, 8, 4>(p, s);
 }
 
 }  // namespace

@@ -29,15 +29,15 @@ namespace fe {
 
 namespace {
 
-constexpr int kT = 8;         // deepest-level core tile (generic stages: small levels, many CTAs)
+// Generic stages: the deepest level's core tile is KT x KT (8 or 16, chosen by the batch autotuner).
 constexpr int kThreads = 256;
 
-__host__ __device__ constexpr int region_size(int nl, int k) {
-  return k == nl ? kT + 6 : 2 * region_size(nl, k + 1) + 3;
+__host__ __device__ constexpr int region_size(int kt, int nl, int k) {
+  return k == nl ? kt + 6 : 2 * region_size(kt, nl, k + 1) + 3;
 }
-__host__ __device__ constexpr int smem_floats(int nl) {
+__host__ __device__ constexpr int smem_floats(int kt, int nl) {
   int s = 0;
-  for (int k = 0; k <= nl; ++k) s += region_size(nl, k) * region_size(nl, k);
+  for (int k = 0; k <= nl; ++k) s += region_size(kt, nl, k) * region_size(kt, nl, k);
   return s;
 }
 
@@ -77,7 +77,7 @@ __device__ __forceinline__ float downscale_px(const float* src, int stride, int 
   return acc;
 }
 
-template <typename InT, int NL>
+template <typename InT, int NL, int KT>
 __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_constant__ StageBatch batch) {
   extern __shared__ float smem[];
   // camera of this CTA: last job whose tile_begin <= blockIdx.x
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
   }
   const StageJob& job = batch.job[lo];
   const int t = (int)blockIdx.x - job.tile_begin;
-  const int X = (t % job.tiles_x) * kT, Y = (t / job.tiles_x) * kT;
+  const int X = (t % job.tiles_x) * KT, Y = (t / job.tiles_x) * KT;
 
   int a[NL + 1], S[NL + 1], off[NL + 1];
   a[NL] = X - 3;
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
   int o = 0;
 #pragma unroll
   for (int k = 0; k <= NL; ++k) {
-    S[k] = region_size(NL, k);
+    S[k] = region_size(KT, NL, k);
     off[k] = o;
     o += S[k] * S[k];
   }
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
 #pragma unroll
   for (int k = (job.write_level0 ? 0 : 1); k <= NL; ++k) {
     const Level& L = job.out[k];
-    const int C = kT << (NL - k);
+    const int C = KT << (NL - k);
     const int cx0 = X << (NL - k), cy0 = Y << (NL - k);
     const float* reg = smem + off[k];
     for (int i = threadIdx.x; i < C * C; i += kThreads) {
@@ -473,21 +473,35 @@ __global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_
 
 }  // namespace l012
 
-template <typename InT, int NL>
+template <typename InT, int NL, int KT>
 cudaError_t set_stage_attr() {
-  return cudaFuncSetAttribute(pyramid_stage_kernel<InT, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sizeof(float) * smem_floats(NL)));
+  return cudaFuncSetAttribute(pyramid_stage_kernel<InT, NL, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(float) * smem_floats(KT, NL)));
 }
 
 template <typename InT, int NL>
-cudaError_t launch_stage(const StageBatch& b, int tiles, cudaStream_t s) {
-  pyramid_stage_kernel<InT, NL><<<tiles, kThreads, sizeof(float) * smem_floats(NL), s>>>(b);
+cudaError_t launch_stage(const StageBatch& b, int tiles, int kt, cudaStream_t s) {
+  if (kt == 16)
+    pyramid_stage_kernel<InT, NL, 16><<<tiles, kThreads, sizeof(float) * smem_floats(16, NL), s>>>(b);
+  else
+    pyramid_stage_kernel<InT, NL, 8><<<tiles, kThreads, sizeof(float) * smem_floats(8, NL), s>>>(b);
   return cudaGetLastError();
+}
+
+template <int KT>
+cudaError_t set_stage_attrs() {
+  cudaError_t e;
+  if ((e = set_stage_attr<uint8_t, 0, KT>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<uint8_t, 1, KT>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<uint8_t, 2, KT>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<float, 0, KT>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<float, 1, KT>()) != cudaSuccess) return e;
+  return set_stage_attr<float, 2, KT>();
 }
 
 }  // namespace
 
-int stage_tile(bool u8, int nl) { return (u8 && nl == 2) ? l012::kT2 : kT; }
+int stage_tile(bool u8, int nl, int kt) { return (u8 && nl == 2) ? l012::kT2 : (kt == 16 ? 16 : 8); }
 
 bool encode_frame_tmap(StageJob& job) {
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -525,29 +539,25 @@ cudaError_t pyramid_init() {
   if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 l012::kSmem)) != cudaSuccess)
     return e;
-  if ((e = set_stage_attr<uint8_t, 0>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<uint8_t, 1>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<uint8_t, 2>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<float, 0>()) != cudaSuccess) return e;
-  if ((e = set_stage_attr<float, 1>()) != cudaSuccess) return e;
-  return set_stage_attr<float, 2>();
+  if ((e = set_stage_attrs<8>()) != cudaSuccess) return e;
+  return set_stage_attrs<16>();
 }
 
-cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, cudaStream_t s) {
+cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, cudaStream_t s) {
   if (tiles <= 0) return cudaSuccess;
   if (u8) {
     switch (nl) {
-      case 0: return launch_stage<uint8_t, 0>(b, tiles, s);
-      case 1: return launch_stage<uint8_t, 1>(b, tiles, s);
+      case 0: return launch_stage<uint8_t, 0>(b, tiles, kt, s);
+      case 1: return launch_stage<uint8_t, 1>(b, tiles, kt, s);
       default:
         l012::pyramid_l012_kernel<<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
         return cudaGetLastError();
     }
   }
   switch (nl) {
-    case 0: return launch_stage<float, 0>(b, tiles, s);
-    case 1: return launch_stage<float, 1>(b, tiles, s);
-    default: return launch_stage<float, 2>(b, tiles, s);
+    case 0: return launch_stage<float, 0>(b, tiles, kt, s);
+    case 1: return launch_stage<float, 1>(b, tiles, kt, s);
+    default: return launch_stage<float, 2>(b, tiles, kt, s);
   }
 }
 

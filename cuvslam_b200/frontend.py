@@ -256,6 +256,23 @@ class Batch:
     def kernel_count(self):
         return self.ctx.lib.fe_batch_kernel_count(self.handle)
 
+    def autotune(self, reps=10, stream=None):
+        """Chooses the LK block shape, the response-tile overlap and the pyramid stage tile by
+        timing the step (fe_batch_autotune); returns the chosen shapes."""
+        _lib.check(self.ctx.lib.fe_batch_autotune(self.handle, int(reps), _stream_handle(stream)), "fe_batch_autotune")
+        return self.tuning()
+
+    def set_tuning(self, lk_block="8x4", response_beside_lk=True, stage_tile=8):
+        shape = ["8x4", "8x3", "4x8", "16x2"].index(lk_block)
+        _lib.check(self.ctx.lib.fe_batch_set_tuning(self.handle, shape, int(bool(response_beside_lk)), int(stage_tile)),
+                   "fe_batch_set_tuning")
+
+    def tuning(self):
+        v = [ctypes.c_int32() for _ in range(3)]
+        _lib.check(self.ctx.lib.fe_batch_tuning(self.handle, *[ctypes.byref(x) for x in v]), "fe_batch_tuning")
+        shapes = ["8x4", "8x3", "4x8", "16x2"]
+        return {"lk_block": shapes[v[0].value], "response_beside_lk": bool(v[1].value), "stage_tile": v[2].value}
+
     def run_plain(self, stream=None):
         _lib.check(self.ctx.lib.fe_batch_run_plain(self.handle, _stream_handle(stream)), "fe_batch_run_plain")
 

@@ -100,3 +100,44 @@ def test_new_features_respect_budget_and_borders(ctx):
         if n:
             assert xy[:, 0].min() >= 3 and xy[:, 0].max() <= w - 1 - 4
             assert xy[:, 1].min() >= 1 and xy[:, 1].max() <= h - 1 - 2
+
+
+def test_autotuned_batch_gives_the_same_results(ctx):
+    """Every shape the autotuner can pick computes the same step: results after fe_batch_autotune
+    equal the default shapes' bit for bit, and the tracks are restored by the tuner."""
+    frames, prevs, host = _setup(ctx, SHAPES, seed=3)
+    b = Batch(ctx, frames)
+    b.run()
+    ref = _results(frames)
+    for f, t in zip(frames, host):
+        if f.tracks is not None:
+            f.tracks.copy_(tracks_to_device(t))
+    torch.cuda.synchronize()
+    tuned = b.autotune(reps=2)
+    assert tuned["lk_block"] in ("8x4", "8x3", "4x8", "16x2") and tuned["stage_tile"] in (8, 16)
+    for f, t in zip(frames, host):  # restored by the tuner
+        if f.tracks is not None:
+            assert_tracks_equal(tracks_from_device(f.tracks), t)
+    b.run()
+    got = _results(frames)
+    for (ta, na, pa), (tb, nb, pb) in zip(ref, got):
+        if ta is not None:
+            assert_tracks_equal(ta, tb)
+        np.testing.assert_array_equal(na, nb)
+        for x, y in zip(pa, pb):
+            np.testing.assert_array_equal(x, y)
+    # every combination of shapes, set directly
+    for block in ("8x4", "8x3", "4x8", "16x2"):
+        for beside in (True, False):
+            for tile in (8, 16):
+                b.set_tuning(block, beside, tile)
+                for f, t in zip(frames, host):
+                    if f.tracks is not None:
+                        f.tracks.copy_(tracks_to_device(t))
+                b.run()
+                for (ta, na, pa), (tb, nb, pb) in zip(ref, _results(frames)):
+                    if ta is not None:
+                        assert_tracks_equal(ta, tb)
+                    np.testing.assert_array_equal(na, nb)
+                    for x, y in zip(pa, pb):
+                        np.testing.assert_array_equal(x, y)
