@@ -88,6 +88,7 @@ fe::Pyr to_pyr(const fe_pyramid& p) {
 struct StageGroup {
   bool u8;
   int nl;
+  bool tail;  // jobs whose last CTA computes the remaining levels (more shared memory)
   int kt;  // deepest-level tile of the generic stages (8 or 16)
   int tiles;
   fe::StageBatch batch;
@@ -97,8 +98,12 @@ using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
 // Appends the stages of one camera's pyramid build: stage 0 reads the frame (uint8 or FP32) and
 // writes levels 0..2; each later stage reads the deepest level of the previous one and writes up
 // to two more.
+// `counters` (device, zeroed, one int per job, *ncounters used so far of counter_cap): when given, a
+// generic stage after which at most two small levels remain computes them in its last CTA (one
+// launch fewer per remaining stage).
 int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan,
-                 float scale = 1.f, int kt = 8) {
+                 float scale = 1.f, int kt = 8, int* counters = nullptr, int* ncounters = nullptr,
+                 int counter_cap = 0) {
   const fe::Pyr pyr = to_pyr(p);
   int s = 0;
   for (int stage = 0;; ++stage) {
@@ -119,16 +124,28 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.tiles_x = (deep.w + T - 1) / T;
     job.tiles_y = (deep.h + T - 1) / T;
     if (kind_u8 && nl == 2) fe::encode_frame_tmap(job);
+    const int rem = pyr.levels - 1 - (s + std::max(nl, 0));
+    if (!(kind_u8 && nl == 2) && nl > 0 && rem > 0 && rem <= 2 && counters && *ncounters < counter_cap) {
+      const fe::Level& deepest = pyr.lv[s + nl];
+      const fe::Level& next = pyr.lv[s + nl + 1];
+      if ((int64_t)deepest.w * deepest.h + (int64_t)next.w * next.h <= fe::kTailFloats) {
+        job.tail_levels = rem;
+        for (int k = 0; k < rem; ++k) job.tail[k] = pyr.lv[s + nl + 1 + k];
+        job.done = counters + (*ncounters)++;
+      }
+    }
     if ((int)plan.size() <= stage) plan.resize(stage + 1);
     StageGroup* g = nullptr;
+    const bool has_tail = job.tail_levels > 0;
     for (auto& gg : plan[stage])
-      if (gg.u8 == kind_u8 && gg.nl == nl) g = &gg;
+      if (gg.u8 == kind_u8 && gg.nl == nl && gg.tail == has_tail) g = &gg;
     if (!g) {
       plan[stage].emplace_back();
       g = &plan[stage].back();
       memset(&g->batch, 0, sizeof(g->batch));
       g->u8 = kind_u8;
       g->nl = nl;
+      g->tail = has_tail;
       g->kt = kt;
       g->tiles = 0;
     }
@@ -136,7 +153,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.tile_begin = g->tiles;
     g->batch.job[g->batch.njobs++] = job;
     g->tiles += job.tiles_x * job.tiles_y;
-    if (nl <= 0) break;
+    if (nl <= 0 || job.tail_levels > 0) break;
     s += nl;
   }
   return FE_OK;
@@ -144,7 +161,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
 
 int run_plan(const StagePlan& plan, cudaStream_t st) {
   for (const auto& stage : plan)
-    for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, st));
+    for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, g.tail, st));
   return FE_OK;
 }
 
@@ -491,6 +508,7 @@ struct fe_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   // shapes chosen by fe_batch_autotune (defaults until it runs)
+  int* stage_done = nullptr;  // pyramid-stage tail counters, two per camera
   int lk_shape = 0;      // LK block shape (fe::kLkShapes)
   int overlap = 1;       // response tiles on a second stream beside LK
   int stage_tile = 8;    // deepest-level tile of the generic pyramid stages
@@ -548,8 +566,10 @@ int capture_batch(fe_batch* b) {
 // Re-plans the pyramid stages with the generic stages' tile `kt`.
 int replan_pyramids(fe_batch* b, int kt) {
   StagePlan plan;
+  int used = 0;
   for (int i = 0; i < b->ncams; ++i) {
-    int rc = plan_pyramid(b->cams[i].image, b->cams[i].image_pitch_bytes, true, b->cur[i], plan, 1.f, kt);
+    int rc = plan_pyramid(b->cams[i].image, b->cams[i].image_pitch_bytes, true, b->cur[i], plan, 1.f, kt,
+                          b->stage_done, &used, 2 * b->ncams);
     if (rc) return rc;
   }
   b->plan = std::move(plan);
@@ -827,7 +847,12 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(cuda_fail(e));
-  int rc = capture_batch(b);
+  // pyramid stages with tails: the deep levels' counters, then the final plan
+  e = cudaMalloc((void**)&b->stage_done, sizeof(int) * 2 * ncams);
+  if (e == cudaSuccess) e = cudaMemset(b->stage_done, 0, sizeof(int) * 2 * ncams);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  int rc = replan_pyramids(b, b->stage_tile);
+  if (!rc) rc = capture_batch(b);
   if (rc) return fail(rc);
   *out = b;
   return FE_OK;
@@ -925,6 +950,7 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->d_lk) cudaFree(b->d_lk);
   if (b->lk_counter) cudaFree(b->lk_counter);
   if (b->sel_mem) cudaFree(b->sel_mem);
+  if (b->stage_done) cudaFree(b->stage_done);
   delete b->sel;
   delete b;
   return FE_OK;
@@ -1075,6 +1101,7 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   const size_t o_lk2 = take(mode == FE_ADJOINT_UNROLLED ? (size_t)njobs * sizeof(fe::LkCam) : 0);
   const size_t o_rtr = take(mode == FE_ADJOINT_UNROLLED ? (size_t)std::max(total, 1) * sizeof(fe_track_data) : 0);
   const size_t o_recs = take(mode == FE_ADJOINT_UNROLLED ? std::max(total, 1) * fe::lk_record_bytes() : 0);
+  const size_t o_done = take(sizeof(int) * 2 * njobs);
   const size_t o_ctr = take(256);
   cudaError_t e = cudaMalloc(&a->mem, o);
   if (e != cudaSuccess) return fail(cuda_fail(e));
@@ -1132,11 +1159,18 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
     a->lk_replay.cams = (const fe::LkCam*)(base + o_lk2);
     a->lk_replay.recs = a->recs;
   }
+  e = cudaMemset(base + o_done, 0, sizeof(int) * 2 * njobs);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  int used = 0;
   for (int j = 0; j < njobs; ++j) {
     const fe_adjoint_job& J = jobs[j];
     if (!J.prev_image) continue;
-    int rc = plan_pyramid(J.prev_image, J.image_pitch_bytes, false, *J.prev, a->build, J.image_scale);
-    if (!rc) rc = plan_pyramid(J.cur_image, J.image_pitch_bytes, false, *J.cur, a->build, J.image_scale);
+    int* done = (int*)(base + o_done);
+    int rc = plan_pyramid(J.prev_image, J.image_pitch_bytes, false, *J.prev, a->build, J.image_scale, 8, done, &used,
+                          2 * njobs);
+    if (!rc)
+      rc = plan_pyramid(J.cur_image, J.image_pitch_bytes, false, *J.cur, a->build, J.image_scale, 8, done, &used,
+                        2 * njobs);
     if (rc) return fail(rc);
   }
 

@@ -21,6 +21,10 @@ struct alignas(64) StageJob {
   int tiles_x, tiles_y;
   int tile_begin;           // first CTA of this job in the launch
   Level out[3];             // out[k] = level s + k; out[0] describes level s
+  // the levels after out[nl], computed by the job's last CTA from the complete out[nl] (0-2 of them)
+  int tail_levels;
+  int* done;                // the job's CTA counter (zero between launches; the last CTA resets it)
+  Level tail[2];
 };
 
 struct StageBatch {
@@ -30,11 +34,12 @@ struct StageBatch {
 };
 
 int stage_tile(bool u8, int nl, int kt);  // deepest-level core tile edge of a stage kind (kt: 8 or 16)
+constexpr int kTailFloats = 12 * 1024;  // shared-memory floats for a tail: the source level + one level
 // Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
 // TMA alignment (the stage then stages its tile with ordinary loads).
 bool encode_frame_tmap(StageJob& job);
 cudaError_t pyramid_init();  // kernel attributes; call once per device before capture
-cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, cudaStream_t s);
+cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, bool tail, cudaStream_t s);
 
 // ---------------------------------------------------------------- selection
 struct SelectCam {

@@ -77,6 +77,54 @@ __device__ __forceinline__ float downscale_px(const float* src, int stride, int 
   return acc;
 }
 
+// Levels tail[0..n) of one camera from the complete level `src` (global), by one CTA: the source
+// level is copied to shared memory (L2, bypassing L1), each tail level's image is computed there
+// with the 25-tap rule and its gradients from it.  `smem` holds kTailFloats floats.
+__device__ void stage_tail(const Level& src, const Level* tail, int n, float* smem) {
+  float* a = smem;                              // current source level (w x h, row stride w)
+  int sw = src.w, sh = src.h;
+  for (int i = threadIdx.x; i < sw * sh; i += kThreads) {
+    const int r = i / sw, c = i - r * sw;
+    cp_async4(a + i, src.img + (size_t)r * src.pitch + c);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int t = 0; t < n; ++t) {
+    const Level& L = tail[t];
+    float* b = a + sw * sh;                     // this level, right after its source
+    for (int i = threadIdx.x; i < L.w * L.h; i += kThreads) {
+      const int y = i / L.w, x = i - y * L.w;
+      const float v = downscale_px(a, sw, 0, 0, sw, sh, x, y);
+      b[i] = v;
+      L.img[(size_t)y * L.pitch + x] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < L.w * L.h; i += kThreads) {
+      const int y = i / L.w, x = i - y * L.w;
+      const float* p = b + i;
+      float gx = 0.f, gy = 0.f;
+      if (x > 2 && x < L.w - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) gx = __fmaf_rn(dsp_tap(j), p[j - 3], gx);
+      }
+      if (y > 2 && y < L.h - 3) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+          if (j != 3) gy = __fmaf_rn(dsp_tap(j), p[(j - 3) * L.w], gy);
+      }
+      L.gx[(size_t)y * L.pitch + x] = gx;
+      if (L.gy) L.gy[(size_t)y * L.pitch + x] = gy;
+    }
+    __syncthreads();
+    // the next level's source: move this level to the front (it is smaller than its source)
+    for (int i = threadIdx.x; i < L.w * L.h; i += kThreads) a[i] = b[i];  // disjoint ranges
+    __syncthreads();
+    sw = L.w;
+    sh = L.h;
+  }
+}
+
 template <typename InT, int NL, int KT>
 __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_constant__ StageBatch batch) {
   extern __shared__ float smem[];
@@ -181,6 +229,22 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
       if (L.gy) L.gy[o2] = sy;
     }
   }
+
+  // 4. tail: the last CTA of the job computes the remaining (small) levels from the complete
+  //    deepest level, in shared memory (threadfence + counter: every CTA's stores precede its count)
+  if (job.tail_levels > 0) {
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(job.done, 1) == job.tiles_x * job.tiles_y - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    stage_tail(job.out[NL], job.tail, job.tail_levels, smem);
+    if (threadIdx.x == 0) *job.done = 0;
+  }
 }
 
 // ---------------------------------------------------------------- levels 0-2 from the uint8 frame
@@ -226,6 +290,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     if (done) return true;
   }
   return false;
+}
+
+// Bytes k and k+1 of a word as exact floats: 0x4B0000bb is 2^23 + b, then subtract 2^23.
+__device__ __forceinline__ float2 bytes_to_float2(uint32_t wd, int k) {
+  const float lo = __uint_as_float(__byte_perm(wd, 0x4B000000u, 0x7540u + k));
+  const float hi = __uint_as_float(__byte_perm(wd, 0x4B000000u, 0x7540u + k + 1));
+  return __fadd2_rn(make_float2(lo, hi), make_float2(-8388608.f, -8388608.f));
 }
 
 // 25-tap value with the reference's corner rule (taps outside in x and y skipped), uint8 source.
@@ -367,44 +438,53 @@ __global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_
   __syncthreads();
 
   // 4. core outputs, four pixels per thread and store
-  // level 0: 128x128 from the uint8 tile
+  // level 0: 128x128 from the uint8 tile.  Bytes become floats exactly as (2^23 + b) - 2^23 (a byte
+  // permute into the mantissa, then one packed subtract per pair); the 7-tap derivatives of pixel
+  // pairs run as packed FP32x2 FMAs, each lane rounding exactly as the scalar FMA chain.
 #pragma unroll 1
   for (int q = tid; q < 128 * 32; q += kThreads) {
     const int y = 4 * Y2 + (q >> 5), x = 4 * X2 + (q & 31) * 4;
     if (y >= h0 || x >= w0) continue;
     const int r = y - a0y, c = x - a0x;
-    float v[12];
+    float2 v[6];  // horizontal neighbours x-4 .. x+7 as pairs
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c - 4 + 4 * k);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) v[4 * k + b] = (float)((wd >> (8 * b)) & 0xffu);
+      v[2 * k] = bytes_to_float2(wd, 0);
+      v[2 * k + 1] = bytes_to_float2(wd, 2);
     }
-    float col[7][4];
+    float2 col[7][2];  // rows y-3 .. y+3, pixel pairs (x, x+1) and (x+2, x+3)
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
       const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + (r - 3 + k) * kS0W + c);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) col[k][b] = (float)((wd >> (8 * b)) & 0xffu);
+      col[k][0] = bytes_to_float2(wd, 0);
+      col[k][1] = bytes_to_float2(wd, 2);
     }
-    float img[4], gx[4], gy[4];
+    // pixel x+i needs v at flat indices 1+i+j (j = 0..6); pairs (i, i+1) for i = 0, 2
+    auto hv = [&](int f) { return (f & 1) ? make_float2(v[f >> 1].y, v[(f >> 1) + 1].x) : v[f >> 1]; };
+    float2 gx2[2], gy2[2];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      float2 sx = make_float2(0.f, 0.f), sy = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        if (j == 3) continue;
+        const float2 d = make_float2(dsp_tap(j), dsp_tap(j));
+        sx = __ffma2_rn(d, hv(1 + 2 * p + j), sx);
+        sy = __ffma2_rn(d, col[j][p], sy);
+      }
+      gx2[p] = sx;
+      gy2[p] = sy;
+    }
+    const bool vin = y > 2 && y < h0 - 3;
+    float gx[4] = {gx2[0].x, gx2[0].y, gx2[1].x, gx2[1].y};
+    float gy[4] = {gy2[0].x, gy2[0].y, gy2[1].x, gy2[1].y};
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      img[i] = v[4 + i];
-      float sx = 0.f, sy = 0.f;
-      if (x + i > 2 && x + i < w0 - 3) {
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-          if (j != 3) sx = __fmaf_rn(dsp_tap(j), v[4 + i - 3 + j], sx);
-      }
-      if (y > 2 && y < h0 - 3) {
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-          if (j != 3) sy = __fmaf_rn(dsp_tap(j), col[j][i], sy);
-      }
-      gx[i] = sx;
-      gy[i] = sy;
+      if (!(x + i > 2 && x + i < w0 - 3)) gx[i] = 0.f;
+      if (!vin) gy[i] = 0.f;
     }
+    const float img[4] = {v[2].x, v[2].y, v[3].x, v[3].y};
     const int64_t o = (int64_t)y * L0.pitch + x;
     if (x + 3 < w0) {
       *reinterpret_cast<float4*>(L0.img + o) = make_float4(img[0], img[1], img[2], img[3]);
@@ -439,22 +519,26 @@ __global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_
       v[4 * k + 2] = f.z;
       v[4 * k + 3] = f.w;
     }
-    float gx[4], gy[4];
+    // pixel pairs (x, x+1), (x+2, x+3): packed FP32x2 FMA chains, vertical taps as 16-byte loads
+    float2 sx[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    float2 sy[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      if (j == 3) continue;
+      const float2 d = make_float2(dsp_tap(j), dsp_tap(j));
+      const float4 cv = *reinterpret_cast<const float4*>(T + (r - 3 + j) * stride + c);
+      sx[0] = __ffma2_rn(d, make_float2(v[1 + j], v[2 + j]), sx[0]);
+      sx[1] = __ffma2_rn(d, make_float2(v[3 + j], v[4 + j]), sx[1]);
+      sy[0] = __ffma2_rn(d, make_float2(cv.x, cv.y), sy[0]);
+      sy[1] = __ffma2_rn(d, make_float2(cv.z, cv.w), sy[1]);
+    }
+    float gx[4] = {sx[0].x, sx[0].y, sx[1].x, sx[1].y};
+    float gy[4] = {sy[0].x, sy[0].y, sy[1].x, sy[1].y};
+    const bool vin = y > 2 && y < L.h - 3;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      float sx = 0.f, sy = 0.f;
-      if (x + i > 2 && x + i < L.w - 3) {
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-          if (j != 3) sx = __fmaf_rn(dsp_tap(j), v[4 + i - 3 + j], sx);
-      }
-      if (y > 2 && y < L.h - 3) {
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-          if (j != 3) sy = __fmaf_rn(dsp_tap(j), T[(r - 3 + j) * stride + c + i], sy);
-      }
-      gx[i] = sx;
-      gy[i] = sy;
+      if (!(x + i > 2 && x + i < L.w - 3)) gx[i] = 0.f;
+      if (!vin) gy[i] = 0.f;
     }
     const int64_t o = (int64_t)y * L.pitch + x;
     if (x + 3 < L.w) {
@@ -473,18 +557,22 @@ __global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_
 
 }  // namespace l012
 
+constexpr size_t stage_smem(int kt, int nl, bool tail = true) {
+  return sizeof(float) * (tail && kTailFloats > smem_floats(kt, nl) ? kTailFloats : smem_floats(kt, nl));
+}
+
 template <typename InT, int NL, int KT>
 cudaError_t set_stage_attr() {
   return cudaFuncSetAttribute(pyramid_stage_kernel<InT, NL, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sizeof(float) * smem_floats(KT, NL)));
+                              (int)stage_smem(KT, NL));
 }
 
 template <typename InT, int NL>
-cudaError_t launch_stage(const StageBatch& b, int tiles, int kt, cudaStream_t s) {
+cudaError_t launch_stage(const StageBatch& b, int tiles, int kt, bool tail, cudaStream_t s) {
   if (kt == 16)
-    pyramid_stage_kernel<InT, NL, 16><<<tiles, kThreads, sizeof(float) * smem_floats(16, NL), s>>>(b);
+    pyramid_stage_kernel<InT, NL, 16><<<tiles, kThreads, stage_smem(16, NL, tail), s>>>(b);
   else
-    pyramid_stage_kernel<InT, NL, 8><<<tiles, kThreads, sizeof(float) * smem_floats(8, NL), s>>>(b);
+    pyramid_stage_kernel<InT, NL, 8><<<tiles, kThreads, stage_smem(8, NL, tail), s>>>(b);
   return cudaGetLastError();
 }
 
@@ -543,21 +631,21 @@ cudaError_t pyramid_init() {
   return set_stage_attrs<16>();
 }
 
-cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, cudaStream_t s) {
+cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, bool tail, cudaStream_t s) {
   if (tiles <= 0) return cudaSuccess;
   if (u8) {
     switch (nl) {
-      case 0: return launch_stage<uint8_t, 0>(b, tiles, kt, s);
-      case 1: return launch_stage<uint8_t, 1>(b, tiles, kt, s);
+      case 0: return launch_stage<uint8_t, 0>(b, tiles, kt, tail, s);
+      case 1: return launch_stage<uint8_t, 1>(b, tiles, kt, tail, s);
       default:
         l012::pyramid_l012_kernel<<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
         return cudaGetLastError();
     }
   }
   switch (nl) {
-    case 0: return launch_stage<float, 0>(b, tiles, kt, s);
-    case 1: return launch_stage<float, 1>(b, tiles, kt, s);
-    default: return launch_stage<float, 2>(b, tiles, kt, s);
+    case 0: return launch_stage<float, 0>(b, tiles, kt, tail, s);
+    case 1: return launch_stage<float, 1>(b, tiles, kt, tail, s);
+    default: return launch_stage<float, 2>(b, tiles, kt, tail, s);
   }
 }
 
