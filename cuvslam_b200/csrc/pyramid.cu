@@ -378,8 +378,19 @@ __global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_
       int col[5];
 #pragma unroll
       for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * x1 - 2 + l, w0) - a0x;
+      // away from the left/right edges the five taps are contiguous bytes: two aligned words, a byte
+      // permute to taps 0-3 and one dp4a with the weights (1, 4, 6, 4), plus tap 4
+      const bool contiguous = 2 * x1 - 2 >= 0 && 2 * x1 + 2 < w0;
+      const int wofs = col[0] & ~3;
+      const uint32_t sel = (col[0] & 3) ? 0x5432u : 0x3210u;
+      const int sh4 = (col[0] & 3) ? 16 : 0;
       auto H = [&](int r) {
         const uint8_t* p = B0 + (mirror_index(r, h0) - a0y) * kS0W;
+        if (contiguous) {
+          const uint32_t w0_ = *reinterpret_cast<const uint32_t*>(p + wofs);
+          const uint32_t w1_ = *reinterpret_cast<const uint32_t*>(p + wofs + 4);
+          return (int)__dp4a(__byte_perm(w0_, w1_, sel), 0x04060401u, (w1_ >> sh4) & 0xffu);
+        }
         return (int)p[col[0]] + (int)p[col[4]] + 4 * ((int)p[col[1]] + (int)p[col[3]]) + 6 * (int)p[col[2]];
       };
       int h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
