@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other BASELINE configs (stereo plain, 100-frame sequence, fwd+bwd stream)")
     ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled"], default=None,
                     help="for an ncu capture: run only this part of the step (inside NVTX ranges named "
                          "'part'), whole batched steps (ranges named 'step'), or the LK adjoint workload's "
@@ -260,6 +262,290 @@ def adjoint_bench(ctx, dev, stream, timed, reps=20):
     return out
 
 
+# ---------------------------------------------------------------- the other BASELINE configs
+SEQ_W, SEQ_H, SEQ_FRAMES, SEQ_FEATURES, SEQ_LEVELS = 1241, 376, 100, 1000, 5
+
+
+def _seq_frame(f):
+    from cuvslam_b200 import synthetic
+
+    img, pose = synthetic.sequence_frame(7, SEQ_W, SEQ_H, f)
+    return img, pose
+
+
+def sequence_frames():
+    """The single-camera 100-frame sequence (per-frame translation up to 30 px, rotation up to 3 deg),
+    drawn in a spawned pool before the timed work."""
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        return pool.map(_seq_frame, range(SEQ_FRAMES))
+
+
+def _gt_between(pose_a, pose_b, xy):
+    """Positions in frame b of texture-coordinate points xy of frame a (both views of the base scene)."""
+    bx, by = pose_a.inverse_apply(xy[:, 0] - 0.5, xy[:, 1] - 0.5)
+    x, y = pose_b.apply(bx, by)
+    return np.stack([x + 0.5, y + 0.5], 1)
+
+
+def _dev_stats(a, b, ok):
+    if ok.sum() == 0:
+        return {"median_px": None, "p99_px": None, "n": 0}
+    d = np.linalg.norm(a[ok] - b[ok], axis=1)
+    return {"median_px": float(np.median(d)), "p99_px": float(np.percentile(d, 99)), "n": int(ok.sum())}
+
+
+def config_sequence(ctx, dev, stream, frames):
+    """one camera, 1241x376, 100 frames, 5 levels, 1000 features kept by re-detection.
+    The plain GPU path (the drop-in call sequence: build, track, select with its blocking readback)
+    against the restated reference CPU tracker (single thread, one camera) in tracks/s; deviation of
+    the GPU tracks from the CPU tracker's on the same inputs, and both from the ground truth."""
+    import torch
+
+    from oracle import oracle as O
+    from cuvslam_b200.frontend import ImagePyramid, LKFeatureTracker, Selection, tracks_from_device, tracks_to_device
+    from cuvslam_b200.types import make_tracks
+
+    sel, lk = Selection(ctx), LKFeatureTracker(ctx)
+    pyr = [ImagePyramid(SEQ_W, SEQ_H, SEQ_LEVELS, device=dev) for _ in range(2)]
+    imgs = [torch.from_numpy(f).to(dev) for f, _ in frames]
+    pyr[0].build(ctx, imgs[0], stream=stream)
+    xy = sel.compute_gftt_and_select_features(pyr[0], 0, 0, 0, 0, None, None, SEQ_FEATURES, stream).cpu().numpy()
+    gpu_s, attempted, dev_gc, gt_g, gt_c = 0.0, 0, [], [], []
+    cpu_prev = O.CpuCamera(SEQ_W, SEQ_H).build(frames[0][0])
+    cpu_cur = O.CpuCamera(SEQ_W, SEQ_H)
+    cpu_s, cpu_xy = 0.0, cpu_prev.select(None, SEQ_FEATURES)
+    cpu_attempted = 0
+    for f in range(1, SEQ_FRAMES):
+        prev_p, cur_p = pyr[(f - 1) % 2], pyr[f % 2]
+        td = tracks_to_device(make_tracks(xy, None, float(SEQ_W), 0.8), dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cur_p.build(ctx, imgs[f], stream=stream)
+        lk.track_points(prev_p, cur_p, td, stream=stream)
+        out = tracks_from_device(td)
+        ok = out["track_status"] == 1
+        alive = torch.from_numpy(np.ascontiguousarray(out["track"][ok])).to(dev)
+        new = sel.compute_gftt_and_select_features(cur_p, 0, 0, 0, 0, None, alive,
+                                                   max(0, SEQ_FEATURES - int(ok.sum())), stream).cpu().numpy()
+        gpu_s += time.perf_counter() - t0
+        attempted += len(xy)
+        # the CPU tracker on the same inputs (deviation), and the ground truth
+        cpu_cur.build(frames[f][0])
+        cxy, cst = cpu_cur.track_from(cpu_prev, xy)
+        both = ok & (cst == 1)
+        dev_gc.append(np.linalg.norm(out["track"][both] - cxy[both], axis=1))
+        gt = _gt_between(frames[f - 1][1], frames[f][1], xy.astype(np.float64))
+        gt_g.append(np.linalg.norm(out["track"][ok] - gt[ok], axis=1))
+        gt_c.append(np.linalg.norm(cxy[cst == 1] - gt[cst == 1], axis=1))
+        xy = np.concatenate([out["track"][ok], new.reshape(-1, 2)]).astype(np.float32)
+        # the CPU tracker's own sequence (timed): track, then re-detect
+        t1 = time.perf_counter()
+        nxy, nst = cpu_cur.track_from(cpu_prev, cpu_xy)
+        keep = nxy[nst == 1]
+        add = cpu_cur.select(keep, max(0, SEQ_FEATURES - len(keep)))
+        cpu_s += time.perf_counter() - t1
+        cpu_attempted += len(cpu_xy)
+        cpu_xy = np.concatenate([keep, add.reshape(-1, 2)]).astype(np.float32)
+        cpu_prev, cpu_cur = cpu_cur, cpu_prev
+    d = np.concatenate(dev_gc)
+    g, c = np.concatenate(gt_g), np.concatenate(gt_c)
+    return {"workload": f"1 camera {SEQ_W}x{SEQ_H}, {SEQ_FRAMES} frames, {SEQ_LEVELS} levels, {SEQ_FEATURES} features",
+            "gpu_plain": {"value": attempted / gpu_s, "unit": UNIT, "ms_per_frame": gpu_s / (SEQ_FRAMES - 1) * 1e3,
+                          "timing": "host wall clock per frame (the plain path reads the selection back)"},
+            "cpu_reference": {"value": cpu_attempted / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+                              "ms_per_frame": cpu_s / (SEQ_FRAMES - 1) * 1e3},
+            "gpu_over_cpu": (attempted / gpu_s) / (cpu_attempted / cpu_s),
+            "deviation_gpu_vs_cpu_px": {"median": float(np.median(d)), "p99": float(np.percentile(d, 99)), "n": len(d)},
+            "error_vs_truth_px": {"gpu_median": float(np.median(g)), "cpu_median": float(np.median(c))}}
+
+
+def config_stereo_plain(ctx, dev, stream):
+    """one stereo pair plus next frame at 752x480, 4 levels, 512 features: the plain GPU
+    path (three pyramids, selection, LK left->next and the horizontal left->right) and the restated
+    reference CPU tracker (left->next), per-frame latency."""
+    import torch
+
+    from cuvslam_b200 import synthetic
+    from oracle import oracle as O
+    from cuvslam_b200.frontend import ImagePyramid, LKFeatureTracker, Selection, tracks_from_device, tracks_to_device
+    from cuvslam_b200.types import make_tracks
+
+    W, H = 752, 480
+    left, nxt, warp = synthetic.frame_pair(0, W, H)
+    right = synthetic.stereo_right(0, W, H)
+    imgs = [torch.from_numpy(a).to(dev) for a in (left, right, nxt)]
+    pyr = [ImagePyramid(W, H, 4, device=dev) for _ in range(3)]
+    sel, lk, lkh = Selection(ctx), LKFeatureTracker(ctx), LKFeatureTracker(ctx, horizontal=True)
+
+    def gpu_frame():
+        for p, im in zip(pyr, imgs):
+            p.build(ctx, im, stream=stream)
+        xy = sel.compute_gftt_and_select_features(pyr[0], 0, 0, 0, 0, None, None, 512, stream).cpu().numpy()
+        t = make_tracks(xy, None, float(W), 0.8)
+        a, b = tracks_to_device(t, dev), tracks_to_device(t, dev)
+        lk.track_points(pyr[0], pyr[2], a, stream=stream)
+        lkh.track_points(pyr[0], pyr[1], b, stream=stream)
+        return xy, tracks_from_device(a)
+
+    for _ in range(3):
+        gpu_frame()
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        xy, out = gpu_frame()
+    gpu_ms = (time.perf_counter() - t0) / reps * 1e3
+    cl, cn = O.CpuCamera(W, H), O.CpuCamera(W, H)
+    t1 = time.perf_counter()
+    for _ in range(3):
+        cl.build(left)
+        cn.build(nxt)
+        cxy = cl.select(None, 512)
+        cout, cst = cn.track_from(cl, cxy)
+    cpu_ms = (time.perf_counter() - t1) / 3 * 1e3
+    sxy, sst = cn.track_from(cl, xy)  # the CPU tracker on the GPU's features
+    ok = (out["track_status"] == 1) & (sst == 1)
+    gt = synthetic.flow_texture(warp, xy.astype(np.float64))
+    return {"workload": f"stereo pair + next frame {W}x{H}, 4 levels, 512 features",
+            "gpu_plain_ms_per_frame": gpu_ms, "cpu_reference_ms_per_frame": cpu_ms, "cpu_cores": 1,
+            "cpu_note": "the CPU arm tracks left->next only (the restated CPU tracker has no horizontal variant)",
+            "deviation_gpu_vs_cpu_px": _dev_stats(out["track"], sxy, ok),
+            "gpu_error_vs_truth_px": _dev_stats(out["track"], gt.astype(np.float32), out["track_status"] == 1)}
+
+
+STREAM_CAMS, STREAM_W, STREAM_H, STREAM_TRACKS, STREAM_FRAMES = 32, 1920, 1200, 8192, 30
+
+
+def _stream_base(c):
+    from cuvslam_b200 import synthetic
+
+    return synthetic.quantise(synthetic.Scene.draw(1000 + c, STREAM_W, STREAM_H).render())
+
+
+def stream_bases():
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        return pool.map(_stream_base, range(STREAM_CAMS))
+
+
+def config_stream(ctx, dev, stream, bases):
+    """16 stereo pairs (32 images) at 1920x1200, 30 consecutive frames, 8192 features
+    per image; per frame the forward tracker and the implicit adjoint of the mean squared distance to
+    ground truth run in one captured CUDA graph, the pyramids rebuilt for the backward instead of kept.
+    Frames: each camera's rendered base frame warped on the GPU by its per-frame similarity (a stand-in
+    for 30 rendered frames); features selected on frame 0, tracked from their true positions in frame
+    f to frame f + 1."""
+    import torch
+    import torch.nn.functional as F
+
+    from cuvslam_b200 import synthetic
+    from cuvslam_b200.diff import DiffTracker
+    from cuvslam_b200.frontend import ImagePyramid, Selection
+
+    B, W, H, N = STREAM_CAMS, STREAM_W, STREAM_H, STREAM_TRACKS
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    base = torch.from_numpy(np.stack(bases)).to(dev).float()
+    poses = [[synthetic.draw_similarity(2000 + f + 7919 * c, W, H) if f else synthetic.Similarity(cx=(W - 1) / 2,
+              cy=(H - 1) / 2) for f in range(STREAM_FRAMES + 1)] for c in range(B)]
+
+    def frame(f):
+        """(B, H, W) frames in [0, 1]: base sampled at pose_f^-1 (bilinear, border clamp)."""
+        ys, xs = torch.meshgrid(torch.arange(H, device=dev, dtype=torch.float64),
+                                torch.arange(W, device=dev, dtype=torch.float64), indexing="ij")
+        grids = []
+        for c in range(B):
+            P = poses[c][f]
+            m = np.linalg.inv(P._mat())
+            xc, yc = xs - P.cx - P.tx, ys - P.cy - P.ty
+            bx = m[0, 0] * xc + m[0, 1] * yc + P.cx
+            by = m[1, 0] * xc + m[1, 1] * yc + P.cy
+            grids.append(torch.stack([bx / (W - 1) * 2 - 1, by / (H - 1) * 2 - 1], -1))
+        g = torch.stack(grids).float()
+        out = F.grid_sample(base[:, None], g, mode="bilinear", padding_mode="border", align_corners=True)[:, 0]
+        return (out.round().clamp(0, 255) / 255.0).contiguous()
+
+    sel = Selection(ctx)
+    f0 = frame(0)
+    xy0 = []
+    for c in range(B):
+        pp = ImagePyramid(W, H, device=dev).build(ctx, (f0[c] * 255).round().to(torch.uint8))
+        v = sel.compute_gftt_and_select_features(pp, 0, 0, 0, 0, None, None, N).reshape(-1, 2).cpu()
+        xy0.append(torch.cat([v] * (N // max(len(v), 1) + 1))[:N].numpy())
+    t = DiffTracker(ctx, B, H, W, N, mode="implicit", recompute_pyramids=True)
+    xy_buf = torch.zeros((B, N, 2), dtype=torch.float32, device=dev)
+    gt_buf = torch.zeros_like(xy_buf)
+    n = B * N
+
+    def step():
+        t._fields_in[:, :, 0:2].copy_(xy_buf)
+        t._fields_in[:, :, 2:4].zero_()
+        t.build_pyramids()
+        t.forward_step()
+        pos, st = t.outputs()
+        t.grad_xy.copy_(torch.where(st[..., None], 2.0 * (pos - gt_buf) / n, torch.zeros_like(pos)))
+        t.build_pyramids()  # recomputed for the backward
+        t.backward_step()
+
+    def load(f):
+        t.prev_img.copy_(frame(f))
+        t.cur_img.copy_(frame(f + 1))
+        a, b = [], []
+        for c in range(B):
+            pa = synthetic.flow_texture(poses[c][f], xy0[c].astype(np.float64)) if f else xy0[c].astype(np.float64)
+            a.append(pa)
+            b.append(_gt_between(poses[c][f], poses[c][f + 1], pa))
+        xy_buf.copy_(torch.from_numpy(np.stack(a).astype(np.float32)))
+        gt_buf.copy_(torch.from_numpy(np.stack(b).astype(np.float32)))
+
+    load(0)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        step()
+    used = free0 - torch.cuda.mem_get_info(dev)[0]
+    ms, kept = 0.0, 0
+    for f in range(STREAM_FRAMES):
+        load(f)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        kept += int(t.outputs()[1].sum().item())
+    # forward and backward apart (same frame), for their ratio
+    fwd_ms = bwd_ms = 0.0
+    reps = 5
+    for _ in range(reps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        t.build_pyramids()
+        t.forward_step()
+        e[1].record()
+        t.build_pyramids()
+        t.backward_step()
+        e[2].record()
+        torch.cuda.synchronize()
+        fwd_ms += e[0].elapsed_time(e[1]) / reps
+        bwd_ms += e[1].elapsed_time(e[2]) / reps
+    del g
+    t.close()
+    return {"workload": f"{B} images {W}x{H} (16 stereo pairs), {STREAM_FRAMES} frames, {N} tracks per image, "
+                        "forward + implicit adjoint per frame in one CUDA graph, pyramids rebuilt for the backward",
+            "value": n * STREAM_FRAMES / (ms / 1e3), "unit": "tracks/s (forward + backward)",
+            "ms_per_frame": ms / STREAM_FRAMES, "tracks_kept_per_frame": kept / STREAM_FRAMES,
+            "fwd_ms": fwd_ms, "bwd_ms_with_pyramid_rebuild": bwd_ms, "bwd_over_fwd": bwd_ms / fwd_ms,
+            "device_memory_bytes": int(used)}
+
+
 def profile_adjoint(args, local):
     import torch
 
@@ -295,6 +581,9 @@ def main():
     if args.profile in ("implicit", "unrolled"):
         return profile_adjoint(args, local)
     shapes, counts, prevs, nexts = workload(seed_offset=rank)
+    want_configs = rank == 0 and world == 1 and not args.no_configs
+    seq_frames = sequence_frames() if want_configs else None
+    bases = stream_bases() if want_configs else None
     import torch
 
     torch.cuda.set_device(local)
@@ -456,6 +745,17 @@ def main():
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         adjoint = adjoint_bench(ctx, dev, stream, timed)
+    configs = None
+    if want_configs:
+        configs = {}
+        for name, fn in (("1_stereo_plain", lambda: config_stereo_plain(ctx, dev, stream)),
+                         ("2_sequence", lambda: config_sequence(ctx, dev, stream, seq_frames)),
+                         ("5_stream_fwd_bwd", lambda: config_stream(ctx, dev, stream, bases))):
+            try:
+                configs[name] = fn()
+            except Exception as ex:  # reported, not fatal: the headline line must still print
+                configs[name] = {"error": f"{type(ex).__name__}: {ex}"}
+            torch.cuda.synchronize()
 
     if rank == 0:
         line = {
@@ -476,6 +776,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": kernels_per_step * args.steps,
             "adjoint": adjoint,
+            "other_configs": configs,
         }
         print(json.dumps(line), flush=True)
     batch.close()
