@@ -159,6 +159,13 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
   return FE_OK;
 }
 
+// The launches of stages [first, last) of a plan.
+int run_stages(const StagePlan& plan, size_t first, size_t last, cudaStream_t st) {
+  for (size_t k = first; k < std::min(last, plan.size()); ++k)
+    for (const auto& g : plan[k]) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, g.tail, st));
+  return FE_OK;
+}
+
 int run_plan(const StagePlan& plan, cudaStream_t st) {
   for (const auto& stage : plan)
     for (const auto& g : stage) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, g.tail, st));
@@ -519,8 +526,11 @@ namespace {
 // One frame step.  After the pyramids the step forks: LK on `st` and the selection's response tiles
 // (which do not depend on tracking) on `side` run concurrently; the rest of the selection (burn of
 // the LK survivors, burned cells, quotas, order) joins after both.
-int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side) {
-  int rc = run_plan(b->plan, st);
+// overlap 1: the fork follows the whole pyramid (response tiles beside LK); overlap 2: it follows the
+// levels 0-2 stage (response tiles beside the deeper pyramid stages and LK).
+int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap = 1) {
+  const size_t split = overlap == 2 ? 1 : b->plan.size();
+  int rc = run_stages(b->plan, 0, split, st);
   if (rc) return rc;
   if (b->any_select) FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
   const bool fork = b->any_select && side;
@@ -531,6 +541,8 @@ int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side) {
   } else if (b->any_select) {
     FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   }
+  rc = run_stages(b->plan, split, b->plan.size(), st);
+  if (rc) return rc;
   if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
   if (fork) {
     FE_CUDA(cudaEventRecord(b->join_ev, side));
@@ -550,7 +562,7 @@ int capture_batch(fe_batch* b) {
   b->lk.shape = b->lk_shape;
   cudaError_t e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(e);
-  int rc = enqueue_batch(b, b->cap_stream, b->overlap ? b->side_stream : nullptr);
+  int rc = enqueue_batch(b, b->cap_stream, b->overlap ? b->side_stream : nullptr, b->overlap);
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(b->cap_stream, &g);
   if (rc) {
@@ -637,17 +649,20 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
     if (!rc && t < best) best = t;
     else b->lk_shape = keep;
   }
-  if (!rc && b->any_select && b->lk.total > 0) {
+  for (int ov = 0; !rc && b->any_select && ov < 3; ++ov) {
+    if (ov == b->overlap) continue;
     const int keep = b->overlap;
-    b->overlap = !keep;
+    b->overlap = ov;
     float t = 0.f;
     rc = measure(&t);
     if (!rc && t < best) best = t;
     else b->overlap = keep;
   }
-  if (!rc) {
+  const int tiles[4] = {8, 16, 8 | fe::kL012Three, 16 | fe::kL012Three};
+  for (int k = 0; !rc && k < 4; ++k) {
+    if (tiles[k] == b->stage_tile) continue;
     const int keep = b->stage_tile;
-    rc = replan_pyramids(b, keep == 8 ? 16 : 8);
+    rc = replan_pyramids(b, tiles[k]);
     float t = 0.f;
     if (!rc) rc = measure(&t);
     if (!rc && t < best) best = t;
@@ -666,10 +681,11 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
 }
 
 int fe_batch_set_tuning(fe_batch* b, int lk_shape, int overlap, int stage_tile) {
-  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (stage_tile != 8 && stage_tile != 16))
+  const int tile = stage_tile & ~fe::kL012Three;
+  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (tile != 8 && tile != 16) || overlap < 0 || overlap > 2)
     return FE_ERR_INVALID_ARGUMENT;
   b->lk_shape = lk_shape;
-  b->overlap = overlap ? 1 : 0;
+  b->overlap = overlap;
   if (stage_tile != b->stage_tile) {
     int rc = replan_pyramids(b, stage_tile);
     if (rc) return rc;

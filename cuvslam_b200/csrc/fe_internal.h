@@ -33,7 +33,10 @@ struct StageBatch {
   StageJob job[kMaxCams];
 };
 
-int stage_tile(bool u8, int nl, int kt);  // deepest-level core tile edge of a stage kind (kt: 8 or 16)
+// kt: the generic stages' deepest-level tile (8 or 16), plus kL012Three to run the levels 0-2 kernel
+// with registers for three CTAs per SM instead of two
+constexpr int kL012Three = 64;
+int stage_tile(bool u8, int nl, int kt);  // deepest-level core tile edge of a stage kind
 constexpr int kTailFloats = 12 * 1024;  // shared-memory floats for a tail: the source level + one level
 // Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
 // TMA alignment (the stage then stages its tile with ordinary loads).

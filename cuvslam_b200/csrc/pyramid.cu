@@ -312,7 +312,9 @@ __device__ float corner_l1(const uint8_t* B0, int a0x, int a0y, int w0, int h0, 
   return (float)acc * (1.f / 256.f);
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pyramid_l012_kernel(const __grid_constant__ StageBatch batch) {
+// MINB: CTAs resident per SM the registers are budgeted for (2, or 3 with fewer registers).
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __grid_constant__ StageBatch batch) {
   extern __shared__ __align__(128) unsigned char sm[];
   uint8_t* B0 = sm;
   float* B1 = reinterpret_cast<float*>(sm + kOffB1);
@@ -580,7 +582,7 @@ cudaError_t set_stage_attr() {
 
 template <typename InT, int NL>
 cudaError_t launch_stage(const StageBatch& b, int tiles, int kt, bool tail, cudaStream_t s) {
-  if (kt == 16)
+  if ((kt & 31) == 16)
     pyramid_stage_kernel<InT, NL, 16><<<tiles, kThreads, stage_smem(16, NL, tail), s>>>(b);
   else
     pyramid_stage_kernel<InT, NL, 8><<<tiles, kThreads, stage_smem(8, NL, tail), s>>>(b);
@@ -600,7 +602,7 @@ cudaError_t set_stage_attrs() {
 
 }  // namespace
 
-int stage_tile(bool u8, int nl, int kt) { return (u8 && nl == 2) ? l012::kT2 : (kt == 16 ? 16 : 8); }
+int stage_tile(bool u8, int nl, int kt) { return (u8 && nl == 2) ? l012::kT2 : ((kt & 31) == 16 ? 16 : 8); }
 
 bool encode_frame_tmap(StageJob& job) {
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -635,7 +637,10 @@ bool encode_frame_tmap(StageJob& job) {
 
 cudaError_t pyramid_init() {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                l012::kSmem)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 l012::kSmem)) != cudaSuccess)
     return e;
   if ((e = set_stage_attrs<8>()) != cudaSuccess) return e;
@@ -649,7 +654,10 @@ cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl
       case 0: return launch_stage<uint8_t, 0>(b, tiles, kt, tail, s);
       case 1: return launch_stage<uint8_t, 1>(b, tiles, kt, tail, s);
       default:
-        l012::pyramid_l012_kernel<<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
+        if (kt & kL012Three)
+          l012::pyramid_l012_kernel<3><<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
+        else
+          l012::pyramid_l012_kernel<2><<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
         return cudaGetLastError();
     }
   }

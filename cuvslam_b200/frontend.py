@@ -262,16 +262,20 @@ class Batch:
         _lib.check(self.ctx.lib.fe_batch_autotune(self.handle, int(reps), _stream_handle(stream)), "fe_batch_autotune")
         return self.tuning()
 
-    def set_tuning(self, lk_block="8x4", response_beside_lk=True, stage_tile=8):
+    OVERLAP = ["after LK", "beside LK", "beside deep pyramid stages and LK"]
+
+    def set_tuning(self, lk_block="8x4", response_overlap="beside LK", stage_tile=8, l012_ctas_per_sm=2):
         shape = ["8x4", "8x3", "4x8", "16x2"].index(lk_block)
-        _lib.check(self.ctx.lib.fe_batch_set_tuning(self.handle, shape, int(bool(response_beside_lk)), int(stage_tile)),
+        tile = int(stage_tile) | (64 if int(l012_ctas_per_sm) == 3 else 0)
+        _lib.check(self.ctx.lib.fe_batch_set_tuning(self.handle, shape, self.OVERLAP.index(response_overlap), tile),
                    "fe_batch_set_tuning")
 
     def tuning(self):
         v = [ctypes.c_int32() for _ in range(3)]
         _lib.check(self.ctx.lib.fe_batch_tuning(self.handle, *[ctypes.byref(x) for x in v]), "fe_batch_tuning")
         shapes = ["8x4", "8x3", "4x8", "16x2"]
-        return {"lk_block": shapes[v[0].value], "response_beside_lk": bool(v[1].value), "stage_tile": v[2].value}
+        return {"lk_block": shapes[v[0].value], "response_overlap": self.OVERLAP[v[1].value],
+                "stage_tile": v[2].value & 31, "l012_ctas_per_sm": 3 if v[2].value & 64 else 2}
 
     def run_plain(self, stream=None):
         _lib.check(self.ctx.lib.fe_batch_run_plain(self.handle, _stream_handle(stream)), "fe_batch_run_plain")

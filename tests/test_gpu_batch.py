@@ -115,6 +115,7 @@ def test_autotuned_batch_gives_the_same_results(ctx):
     torch.cuda.synchronize()
     tuned = b.autotune(reps=2)
     assert tuned["lk_block"] in ("8x4", "8x3", "4x8", "16x2") and tuned["stage_tile"] in (8, 16)
+    assert tuned["response_overlap"] in Batch.OVERLAP and tuned["l012_ctas_per_sm"] in (2, 3)
     for f, t in zip(frames, host):  # restored by the tuner
         if f.tracks is not None:
             assert_tracks_equal(tracks_from_device(f.tracks), t)
@@ -128,9 +129,9 @@ def test_autotuned_batch_gives_the_same_results(ctx):
             np.testing.assert_array_equal(x, y)
     # every combination of shapes, set directly
     for block in ("8x4", "8x3", "4x8", "16x2"):
-        for beside in (True, False):
-            for tile in (8, 16):
-                b.set_tuning(block, beside, tile)
+        for overlap in Batch.OVERLAP:
+            for tile, ctas in ((8, 2), (16, 3)):
+                b.set_tuning(block, overlap, tile, ctas)
                 for f, t in zip(frames, host):
                     if f.tracks is not None:
                         f.tracks.copy_(tracks_to_device(t))
