@@ -414,6 +414,137 @@ def config_stereo_plain(ctx, dev, stream):
             "gpu_error_vs_truth_px": _dev_stats(out["track"], gt.astype(np.float32), out["track_status"] == 1)}
 
 
+def config_l2r(ctx, dev, stream, npairs=8):
+    """Left-to-right stereo matching: npairs rectified 752x480 pairs (seeded scenes, right view at a
+    smoothed U(5, 40) px disparity), 4 levels, 512 Shi-Tomasi features per primary, candidates from
+    the epipolar table of a pinhole pair (fx 458 px, baseline 0.11 m, auto depth range).  Times the
+    folded scan (fe_track_stereo: all pairs, all candidate rounds, one launch) against the reference's
+    launch pattern driven with the same horizontal LK kernel (one launch per candidate round, records
+    up and down, a stream synchronisation per round, the host loop in Python), and the oracle's CPU
+    restatement of the scan on one pair (1 core)."""
+    import ctypes
+
+    import torch
+
+    from cuvslam_b200 import _lib, synthetic
+    from cuvslam_b200.frontend import ImagePyramid, Selection, _stream_handle
+    from cuvslam_b200.stereo import EpipolarCurves, StereoMatcher, StereoPair, cross_cam_search_radius
+    from cuvslam_b200.types import TRACK_DTYPE, level_sizes, make_tracks
+    from oracle import oracle as O
+
+    W, H, L, NF = 752, 480, 4, 512
+    sizes = level_sizes(W, H, L)
+    top = len(sizes) - 1
+    k = (458.0, 458.0, 367.0, 248.0)
+    table = EpipolarCurves.pinhole(k, k, (np.eye(3), (-0.11, 0.0, 0.0)), top, sizes[top][0], sizes[top][1], device=dev)
+    lefts = [synthetic.quantise(synthetic.Scene.draw(1000 + c, W, H).render()) for c in range(npairs)]
+    rights = [synthetic.stereo_right(c, W, H) for c in range(npairs)]
+    pl = [ImagePyramid(W, H, L, device=dev).build(ctx, torch.from_numpy(a).to(dev)) for a in lefts]
+    pr = [ImagePyramid(W, H, L, device=dev).build(ctx, torch.from_numpy(a).to(dev)) for a in rights]
+    sel = Selection(ctx)
+    uvs = [sel.compute_gftt_and_select_features(p, 0, 0, 0, 0, None, None, NF, stream).contiguous() for p in pl]
+    pairs = [StereoPair(a, b, uv, curves=table) for a, b, uv in zip(pl, pr, uvs)]
+    radius = cross_cam_search_radius(top)
+    m = StereoMatcher(ctx)
+    outs = m.track_primary_to_secondary(pairs, stream=stream)
+    outs1 = m.track_primary_to_secondary(pairs[:1], stream=stream)
+    torch.cuda.synchronize()
+
+    def dev_ms(fn, reps=50):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    folded_ms = dev_ms(lambda: m.track_primary_to_secondary(pairs, outputs=outs, stream=stream))
+    folded1_ms = dev_ms(lambda: m.track_primary_to_secondary(pairs[:1], outputs=outs1, stream=stream))
+    n_points = sum(int(u.shape[0]) for u in uvs)
+
+    # the reference's launch pattern with the same tracker: candidates on the host, one horizontal LK
+    # launch per round over all points, records copied up and down, a synchronisation per round
+    cw, ch, inv = table.width, table.height, table.inv_scale
+    lib = ctx.lib
+    hs = _stream_handle(stream)
+
+    def multi_launch_setup(i):
+        uv = uvs[i].cpu().numpy()
+        off, cxy = O.epipolar_candidates(cw, ch, inv, table.offsets_host, table.xy_host, uv)
+        n = len(uv)
+        host = torch.from_numpy(make_tracks(uv, None, radius, 0.8).view(np.uint8).reshape(n, 80).copy()).pin_memory()
+        back = torch.empty_like(host).pin_memory()
+        d = torch.empty((n, 80), dtype=torch.uint8, device=dev)
+        return uv, off, cxy, host, back, d
+
+    setups = [multi_launch_setup(i) for i in range(npairs)]
+
+    def multi_launch(i):
+        uv, off, cxy, host, back, d = setups[i]
+        n = len(uv)
+        lens = np.diff(off)
+        rec = host.numpy().view(TRACK_DTYPE).reshape(n)
+        out = back.numpy().view(TRACK_DTYPE).reshape(n)
+        won = np.zeros(n, bool)
+        winner = np.full(n, -1, np.int32)
+        tracked = 0
+        for kk in range(int(lens.max(initial=0))):
+            active = ~won & (kk < lens)
+            if not active.any():
+                break
+            rec["track"] = uv
+            rec["track_status"] = 0
+            rec["info"] = 0.0
+            idx = np.where(active, off[:-1] + kk, 0)
+            rec["offset"] = np.where(active[:, None], cxy[np.minimum(idx, max(len(cxy) - 1, 0))] - uv, 0.0)
+            d.copy_(host, non_blocking=True)
+            _lib.check(lib.fe_track(ctx.handle, ctypes.byref(pl[i].desc), ctypes.byref(pr[i].desc),
+                                    ctypes.c_void_p(d.data_ptr()), n, 1, _lib.FE_SAMPLE_TEXTURE, hs), "fe_track")
+            back.copy_(d, non_blocking=True)
+            stream.synchronize()
+            new = active & (out["track_status"] != 0)
+            winner[new] = kk
+            won |= new
+            tracked += int(new.sum())
+            if np.float32(tracked) >= np.float32(0.8) * np.float32(n):
+                break
+        return winner
+
+    wins = [multi_launch(i) for i in range(npairs)]
+    same = all(np.array_equal(w, o[1].cpu().numpy()) for w, o in zip(wins, outs))
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for i in range(npairs):
+            multi_launch(i)
+    multi_ms = (time.perf_counter() - t0) / reps * 1e3
+    rounds = [int(o[2].cpu().numpy()[1]) for o in outs]
+    matched = [int(o[2].cpu().numpy()[0]) for o in outs]
+    attempts = [int(o[2].cpu().numpy()[2]) for o in outs]
+
+    # the oracle's CPU restatement of the scan, one pair, 1 core
+    opl, opr = O.pyramid(lefts[0], L), O.pyramid(rights[0], L)
+    uv0, off0, cxy0 = setups[0][:3]
+    t1 = time.perf_counter()
+    cpu_reps = 3
+    for _ in range(cpu_reps):
+        _, cwin, _ = O.stereo_scan(opl, opr, uv0, off0, cxy0, None, radius, 0.8, 0.8)
+    cpu_ms = (time.perf_counter() - t1) / cpu_reps * 1e3
+    return {"workload": f"{npairs} rectified {W}x{H} stereo pairs, {L} levels, {NF} features per primary, "
+                        "epipolar-table candidates (fx 458, baseline 0.11 m)",
+            "points": n_points, "matched": matched, "rounds_per_pair": rounds, "attempts_per_pair": attempts,
+            "folded_ms_all_pairs": folded_ms, "folded_ms_one_pair": folded1_ms,
+            "points_per_s_folded": n_points / (folded_ms / 1e3),
+            "multi_launch_ms_all_pairs": multi_ms, "folded_speedup_vs_multi_launch": multi_ms / folded_ms,
+            "winners_equal_multi_launch": bool(same),
+            "winners_equal_cpu_oracle_pair0": bool(np.array_equal(cwin, outs[0][1].cpu().numpy())),
+            "cpu_oracle_ms_one_pair": cpu_ms, "cpu_cores": 1}
+
+
 STREAM_CAMS, STREAM_W, STREAM_H, STREAM_TRACKS, STREAM_FRAMES = 32, 1920, 1200, 8192, 30
 
 
@@ -786,6 +917,7 @@ def main():
         configs = {}
         for name, fn in (("1_stereo_plain", lambda: config_stereo_plain(ctx, dev, stream)),
                          ("2_sequence", lambda: config_sequence(ctx, dev, stream, seq_frames)),
+                         ("l2r_stereo", lambda: config_l2r(ctx, dev, stream)),
                          ("5_stream_fwd_bwd", lambda: config_stream(ctx, dev, stream, bases))):
             try:
                 configs[name] = fn()

@@ -70,6 +70,36 @@ FE_ADJOINT_IMPLICIT = 0
 FE_ADJOINT_UNROLLED = 1
 
 
+class FeEpipolarCurves(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("inv_scale", ctypes.c_float),
+        ("offsets", ctypes.c_void_p),
+        ("xy", ctypes.c_void_p),
+        ("max_length", ctypes.c_int32),
+    ]
+
+
+class FeStereoPair(ctypes.Structure):
+    _fields_ = [
+        ("primary", ctypes.POINTER(FePyramid)),
+        ("secondary", ctypes.POINTER(FePyramid)),
+        ("uv", ctypes.c_void_p),
+        ("valid", ctypes.c_void_p),
+        ("n", ctypes.c_int32),
+        ("cand_offsets", ctypes.c_void_p),
+        ("cand_xy", ctypes.c_void_p),
+        ("max_candidates", ctypes.c_int32),
+        ("curves", ctypes.POINTER(FeEpipolarCurves)),
+        ("search_radius", ctypes.c_float),
+        ("ncc_threshold", ctypes.c_float),
+        ("out", ctypes.c_void_p),
+        ("winner", ctypes.c_void_p),
+        ("stats", ctypes.c_void_p),
+    ]
+
+
 class FeError(RuntimeError):
     pass
 
@@ -95,6 +125,7 @@ _SIGS = {
     "fe_select_noalloc": (_I, [ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
     "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "fe_track": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _P]),
+    "fe_track_stereo": (_I, [_P, ctypes.POINTER(FeStereoPair), _I, ctypes.c_float, _I, _P]),
     "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),
     "fe_batch_run": (_I, [_P, _P]),
     "fe_batch_run_plain": (_I, [_P, _P]),

@@ -196,6 +196,8 @@ struct fe_context {
   int device = 0;
   SelectScratch sel;
   int* lk_counter = nullptr;  // persistent LK warps' track counter
+  void* stereo_mem = nullptr;  // left-to-right matching scratch (grown on demand)
+  size_t stereo_bytes = 0;
   bool debug = false;
 };
 
@@ -348,6 +350,7 @@ int fe_destroy(fe_context* ctx) {
   if (!ctx) return FE_ERR_INVALID_ARGUMENT;
   if (ctx->sel.mem) cudaFree(ctx->sel.mem);
   if (ctx->lk_counter) cudaFree(ctx->lk_counter);
+  if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
   if (ctx->sel.resp) cudaFree(ctx->sel.resp);
   if (ctx->sel.nms) cudaFree(ctx->sel.nms);
   delete ctx;
@@ -487,6 +490,114 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
   p.single.n = n;
   p.single.begin = 0;
   FE_CUDA(fe::launch_lk(p, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, float early_exit_fraction,
+                    int sampling, fe_stream stream) {
+  if (!ctx || !pairs || npairs <= 0) return FE_ERR_INVALID_ARGUMENT;
+  if (npairs > fe::kMaxStereoPairs) return FE_ERR_CAPACITY;
+  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  if (!(early_exit_fraction == early_exit_fraction)) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  // scratch layout: [counter, done, per pair: attempts, cnt[maxc]] zeroed; [per pair: stop, best[n]]
+  // set to all ones; [per pair: pos[n * maxc]] uninitialised
+  int64_t zero_words = 2, ones_words = 0, pos_elems = 0, round = 0;
+  int rounds = 0;
+  for (int q = 0; q < npairs; ++q) {
+    const fe_stereo_pair& P = pairs[q];
+    if (!valid_pyramid(P.primary) || !valid_pyramid(P.secondary)) return FE_ERR_INVALID_ARGUMENT;
+    if (P.secondary->levels < P.primary->levels) return FE_ERR_INVALID_ARGUMENT;
+    if (P.n < 0 || (P.n > 0 && (!P.uv || !P.out))) return FE_ERR_INVALID_ARGUMENT;
+    if ((uintptr_t)P.out % 16 != 0 || (uintptr_t)P.uv % 8 != 0) return FE_ERR_INVALID_ARGUMENT;
+    int maxc = 0;
+    if (P.cand_offsets) {
+      if (P.max_candidates < 0 || (P.max_candidates > 0 && !P.cand_xy) || (uintptr_t)P.cand_xy % 8 != 0)
+        return FE_ERR_INVALID_ARGUMENT;
+      maxc = P.max_candidates;
+    } else {
+      const fe_epipolar_curves* c = P.curves;
+      if (!c || c->width < 1 || c->height < 1 || !c->offsets || c->max_length < 0 || !(c->inv_scale > 0.f) ||
+          (c->max_length > 0 && !c->xy) || (uintptr_t)c->xy % 8 != 0)
+        return FE_ERR_INVALID_ARGUMENT;
+      maxc = c->max_length;
+    }
+    if (P.n > 0 && maxc > (INT32_MAX / 4) / P.n) return FE_ERR_CAPACITY;
+    zero_words += 1 + maxc;
+    ones_words += 1 + P.n;
+    pos_elems += (int64_t)P.n * maxc;
+    round += P.n;
+    rounds = std::max(rounds, maxc);
+  }
+  if (round == 0) {
+    for (int q = 0; q < npairs; ++q)
+      if (pairs[q].stats) FE_CUDA(cudaMemsetAsync(pairs[q].stats, 0, 4 * sizeof(int32_t), s));
+    return FE_OK;
+  }
+  if ((int64_t)rounds * round > (int64_t)INT32_MAX - (1 << 24)) return FE_ERR_CAPACITY;
+  const int64_t zero_bytes = align_up(zero_words * 4, kAlign), ones_bytes = align_up(ones_words * 4, kAlign);
+  const int64_t need = zero_bytes + ones_bytes + pos_elems * 8;
+  if ((size_t)need > ctx->stereo_bytes) {
+    if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
+    ctx->stereo_mem = nullptr;
+    ctx->stereo_bytes = 0;
+    FE_CUDA(cudaMalloc(&ctx->stereo_mem, (size_t)need));
+    ctx->stereo_bytes = (size_t)need;
+  }
+  char* base = (char*)ctx->stereo_mem;
+  int* zw = (int*)base;
+  unsigned* ow = (unsigned*)(base + zero_bytes);
+  float2* pw = (float2*)(base + zero_bytes + ones_bytes);
+  fe::StereoLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.npairs = npairs;
+  L.round = (int)round;
+  L.rounds = rounds;
+  L.counter = zw;
+  L.done = zw + 1;
+  L.sampling = sampling;
+  zw += 2;
+  int begin = 0;
+  for (int q = 0; q < npairs; ++q) {
+    const fe_stereo_pair& P = pairs[q];
+    fe::StereoPair& D = L.pair[q];
+    D.lk.prev = to_pyr(*P.primary);
+    D.lk.cur = to_pyr(*P.secondary);
+    D.uv = (const float2*)P.uv;
+    D.valid = P.valid;
+    D.n = P.n;
+    D.begin = begin;
+    begin += P.n;
+    if (P.cand_offsets) {
+      D.maxc = P.max_candidates;
+      D.cand_off = P.cand_offsets;
+      D.cand_xy = (const float2*)P.cand_xy;
+    } else {
+      D.maxc = P.curves->max_length;
+      D.cw = P.curves->width;
+      D.ch = P.curves->height;
+      D.inv_scale = P.curves->inv_scale;
+      D.c_off = P.curves->offsets;
+      D.c_xy = (const float2*)P.curves->xy;
+    }
+    D.radius = P.search_radius;
+    D.ncc_thr = P.ncc_threshold;
+    D.need = early_exit_fraction * (float)P.n;  // kL2REarlyExitFraction * n, as the reference computes it
+    D.out = P.out;
+    D.winner = P.winner;
+    D.stats = P.stats;
+    D.attempts = zw;
+    D.cnt = zw + 1;
+    zw += 1 + D.maxc;
+    D.stop = ow;
+    D.best = ow + 1;
+    ow += 1 + P.n;
+    D.pos = pw;
+    pw += (size_t)P.n * D.maxc;
+  }
+  FE_CUDA(cudaMemsetAsync(base, 0, (size_t)zero_words * 4, s));
+  FE_CUDA(cudaMemsetAsync(base + zero_bytes, 0xff, (size_t)ones_words * 4, s));
+  FE_CUDA(fe::launch_stereo(L, s));
   return FE_OK;
 }
 

@@ -134,6 +134,47 @@ struct LkLaunch {
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
 constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2
 
+// ---------------------------------------------------------------- left-to-right matching
+constexpr int kMaxStereoPairs = 16;
+
+struct StereoPair {
+  LkCam lk;                     // prev = primary (image + grad_x), cur = secondary (image)
+  const float2* uv;
+  const uint8_t* valid;         // optional
+  int n;
+  int begin;                    // first point of this pair in a round of the flattened list
+  int maxc;                     // candidate rounds of this pair
+  const int* cand_off;          // explicit candidates (n + 1 offsets), or nullptr: curves
+  const float2* cand_xy;
+  int cw, ch;                   // epipolar table: corners per row, corner rows
+  float inv_scale;
+  const int* c_off;
+  const float2* c_xy;
+  float radius, ncc_thr;
+  float need;                   // early-exit count: frac * n
+  fe_track_data* out;
+  int* winner;                  // optional
+  int* stats;                   // optional
+  // scratch
+  int* cnt;                     // [maxc]: points whose first success is at a round <= r (zeroed)
+  int* attempts;                // attempts tracked (zeroed)
+  unsigned* stop;               // earliest round known to meet the early-exit count (all ones)
+  unsigned* best;               // [n]: lowest successful candidate index (all ones = none)
+  float2* pos;                  // [n * maxc]: tracked position of each successful attempt
+};
+
+struct StereoLaunch {
+  int npairs;
+  int round;                    // points per round (sum of n)
+  int rounds;                   // largest maxc
+  int* counter;                 // attempt counter of the persistent warps (zeroed)
+  int* done;                    // CTA counter (zeroed): the last CTA publishes the results
+  int sampling;
+  StereoPair pair[kMaxStereoPairs];
+};
+
+cudaError_t launch_stereo(const StereoLaunch& p, cudaStream_t s);
+
 // ---------------------------------------------------------------- LK adjoint
 // Per-track gradient contributions are written as window records (slot = (plane q, level l, track g),
 // q: 0 previous image, 1 previous grad_x, 2 previous grad_y, 3 current image), then summed per

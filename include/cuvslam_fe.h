@@ -177,6 +177,66 @@ FE_API int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* c
              int horizontal, int sampling, fe_stream stream);
 
 /* ---------------------------------------------------------------------------------------- */
+/* Left-to-right (primary -> secondary camera) matching                                      */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Precomputed epipolar candidate table of one camera pair (EpipolarCurves, epipolar_curves.h:26-64):
+ * for each corner (u, v) of the primary pyramid's top level, 0 <= u < width = top_width + 1,
+ * 0 <= v < height = top_height + 1, a curve of secondary base-level positions.  Device memory. */
+typedef struct {
+  int32_t width, height;  /* corners per row, corner rows */
+  float inv_scale;        /* 1 / 2^top_level */
+  const int32_t* offsets; /* width * height + 1: corner (u, v)'s curve is xy[offsets[v*width+u] ..
+                             offsets[v*width+u+1]) (x, y pairs) */
+  const float* xy;
+  int32_t max_length;     /* longest curve (a bound on the candidates of any point) */
+} fe_epipolar_curves;
+
+/* One primary -> secondary pair of a left-to-right match. */
+typedef struct {
+  const fe_pyramid* primary;   /* host descriptor: primary frame's image + grad_x pyramid */
+  const fe_pyramid* secondary; /* host descriptor: secondary frame's image pyramid */
+  const float* uv;             /* device, n x 2: primary positions (base-level pixels) */
+  const uint8_t* valid;        /* device, n, or NULL: 0 = the point has no candidates (the caller could
+                                  not project it; the reference then reports track (0, 0)) */
+  int32_t n;
+  /* candidates: an explicit list (cand_offsets != NULL) or the pair's epipolar table (curves) */
+  const int32_t* cand_offsets; /* device, n + 1: point i's candidates are cand_xy[cand_offsets[i] ..
+                                  cand_offsets[i+1]) (secondary base-level x, y pairs) */
+  const float* cand_xy;
+  int32_t max_candidates;      /* with cand_offsets: the longest list (longer lists are cut, and
+                                  stats[3] gets bit 0) */
+  const fe_epipolar_curves* curves; /* host descriptor, used when cand_offsets == NULL:
+                                       candidates interpolated as EpipolarCurves::Candidates
+                                       (epipolar_curves.cpp:64-101) */
+  float search_radius;         /* search_radius_px of every attempt (CrossCamSearchRadius,
+                                  sof_multicamera_base.cpp:31-37: 3 * 2^(top_level + 1)) */
+  float ncc_threshold;         /* 0.8 in the reference */
+  fe_track_data* out;          /* device, n records: the winning attempt's record; failed points
+                                  get track = uv (or (0, 0) when not valid) and track_status = 0 */
+  int32_t* winner;             /* device, n, or NULL: index of the winning candidate, -1 = none */
+  int32_t* stats;              /* device, 4, or NULL: points matched, candidate rounds the
+                                  reference would run, attempts tracked here, flags */
+} fe_stereo_pair;
+
+/* Left-to-right matching of npairs (<= 16) camera pairs in ONE launch: for each primary point,
+ * horizontal LK (lk_track_horizontal_kernel, lk_tracker.cu:381-665) from its position in the
+ * primary frame towards each of its candidates in turn, the first candidate that tracks wins.
+ * Results equal MultiSOFGPU::LaunchTrackingPrimaryToSecondary (sof_multicamera_gpu.cpp:69-190),
+ * which launches one tracking pass per candidate index k and synchronises after each, including
+ * its early exit: after round k it stops once at least early_exit_fraction (kL2REarlyExitFraction
+ * = 0.8, sof_multicamera_base.h:40) of the pair's points are matched, so points whose first
+ * successful candidate comes after that round stay unmatched.  Here the (point, candidate)
+ * attempts run in round order over persistent warps; an attempt is skipped once its point has an
+ * earlier success or its round lies beyond a round that already met the early-exit count, so
+ * the stop round and every result are those of the reference, whatever the scheduling.
+ * Scratch (in the context) grows to the largest sum over pairs of n x max_candidates seen so far:
+ * make the first call at the largest size before capturing a graph.  One call at a time per
+ * context.  sampling as in fe_track. */
+FE_API int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, float early_exit_fraction,
+                           int sampling, fe_stream stream);
+
+/* ---------------------------------------------------------------------------------------- */
 /* Batched multi-camera frame step                                                           */
 /* ---------------------------------------------------------------------------------------- */
 

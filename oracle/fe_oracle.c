@@ -677,6 +677,99 @@ void or_lk_track_horizontal(int levels, const int* ws, const int* hs, const floa
   for (int k = 0; k < n; ++k) lk_one(levels, ws, hs, prev_gx, prev_gx, prev_img, cur_img, &td[k], mode, 1);
 }
 
+/* EpipolarCurves::Candidates (libs/sof/epipolar_curves.cpp:64-101): the corner grid position of the
+ * point at the top level, nothing outside the grid (or when the right or bottom corner is missing),
+ * else the four corner curves blended with bilinear weights up to the shortest of them, each
+ * coordinate ((w00 c00 + w01 c01) + w10 c10) + w11 c11 in FP32. */
+int or_epipolar_candidates(int cw, int ch, float inv_scale, const int32_t* offsets, const float* xy, float u, float v,
+                           float* out, int cap) {
+  const float vf = v * inv_scale, uf = u * inv_scale;
+  if (!(vf >= 0.f && vf < (float)ch && uf >= 0.f && uf < (float)cw)) return 0;
+  const int v0 = (int)vf, u0 = (int)uf;
+  if (v0 + 1 >= ch || u0 + 1 >= cw) return 0;
+  const float dv = vf - (float)v0, du = uf - (float)u0;
+  const float w00 = (1.0f - du) * (1.0f - dv);
+  const float w01 = du * (1.0f - dv);
+  const float w10 = (1.0f - du) * dv;
+  const float w11 = du * dv;
+  const int i00 = v0 * cw + u0, i01 = i00 + 1, i10 = i00 + cw, i11 = i10 + 1;
+  int n = offsets[i00 + 1] - offsets[i00];
+  const int n01 = offsets[i01 + 1] - offsets[i01], n10 = offsets[i10 + 1] - offsets[i10];
+  const int n11 = offsets[i11 + 1] - offsets[i11];
+  if (n01 < n) n = n01;
+  if (n10 < n) n = n10;
+  if (n11 < n) n = n11;
+  if (n > cap) n = cap;
+  const float* c00 = xy + 2 * (size_t)offsets[i00];
+  const float* c01 = xy + 2 * (size_t)offsets[i01];
+  const float* c10 = xy + 2 * (size_t)offsets[i10];
+  const float* c11 = xy + 2 * (size_t)offsets[i11];
+  for (int k = 0; k < n; ++k)
+    for (int d = 0; d < 2; ++d)
+      out[2 * k + d] = w00 * c00[2 * k + d] + w01 * c01[2 * k + d] + w10 * c10[2 * k + d] + w11 * c11[2 * k + d];
+  return n;
+}
+
+/* The unmatched record of the scan: track = uv, everything the tracker would write cleared. */
+static void stereo_record(or_track_data* t, float x, float y, float radius, float ncc_thr) {
+  memset(t, 0, sizeof(*t));
+  t->track[0] = x;
+  t->track[1] = y;
+  t->cache_index = -1;
+  t->initial_guess_map[0] = 1.f;
+  t->initial_guess_map[3] = 1.f;
+  t->search_radius_px = radius;
+  t->ncc_threshold = ncc_thr;
+}
+
+/* MultiSOFGPU::LaunchTrackingPrimaryToSecondary (libs/sof/sof_multicamera_gpu.cpp:118-190): round k
+ * tracks candidate k of every point without a match that has one (the reference's sentinel
+ * entries, tracked with a zero offset and discarded, are left out); no round when none has; after
+ * round k, stop once matched >= early_exit_fraction * n (kL2REarlyExitFraction). */
+void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const* prim_gx,
+                    const float* const* prim_img, const float* const* sec_img, const float* uv, const uint8_t* valid,
+                    int n, const int32_t* cand_off, const float* cand_xy, float search_radius, float ncc_threshold,
+                    float early_exit_fraction, int mode, or_track_data* out, int32_t* winner, int32_t* stats) {
+  int max_candidates = 0;
+  for (int i = 0; i < n; ++i) {
+    const int len = (valid && !valid[i]) ? 0 : cand_off[i + 1] - cand_off[i];
+    if (len > max_candidates) max_candidates = len;
+    winner[i] = -1;
+    if (valid && !valid[i])
+      stereo_record(&out[i], 0.f, 0.f, search_radius, ncc_threshold);
+    else
+      stereo_record(&out[i], uv[2 * i], uv[2 * i + 1], search_radius, ncc_threshold);
+  }
+  int tracked = 0, rounds = 0, attempts = 0;
+  for (int k = 0; k < max_candidates; ++k) {
+    int any_active = 0;
+    for (int i = 0; i < n; ++i) {
+      const int len = (valid && !valid[i]) ? 0 : cand_off[i + 1] - cand_off[i];
+      if (winner[i] >= 0 || k >= len) continue;
+      any_active = 1;
+      or_track_data t;
+      stereo_record(&t, uv[2 * i], uv[2 * i + 1], search_radius, ncc_threshold);
+      const float* c = cand_xy + 2 * ((size_t)cand_off[i] + k);
+      t.offset[0] = c[0] - uv[2 * i];
+      t.offset[1] = c[1] - uv[2 * i + 1];
+      lk_one(levels, ws, hs, prim_gx, prim_gx, prim_img, sec_img, &t, mode, 1);
+      ++attempts;
+      if (t.track_status) {
+        out[i] = t;
+        winner[i] = k;
+        ++tracked;
+      }
+    }
+    if (!any_active) break;
+    rounds = k + 1;
+    if ((float)tracked >= early_exit_fraction * (float)n) break;
+  }
+  stats[0] = tracked;
+  stats[1] = rounds;
+  stats[2] = attempts;
+  stats[3] = 0;
+}
+
 /* FP64 restatement of the same LK (exact bilinear weights, double arithmetic, plain summation
  * order).  Used only to state per-track error of the FP32 paths. */
 static double samp64(const float* img, int w, int h, double x, double y) {

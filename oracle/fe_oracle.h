@@ -64,6 +64,22 @@ void or_lk_track_f64(int levels, const int* ws, const int* hs, const float* cons
                      const float* const* prev_gy, const float* const* prev_img, const float* const* cur_img,
                      or_track_data* td, int n);
 
+/* Candidates of a primary base-level point (u, v) from an epipolar table of cw x ch corner curves
+ * in CSR form (offsets[cw * ch + 1], xy pairs): EpipolarCurves::Candidates
+ * (libs/sof/epipolar_curves.cpp:64-101).  Writes up to `cap` x, y pairs, returns the count. */
+int or_epipolar_candidates(int cw, int ch, float inv_scale, const int32_t* offsets, const float* xy, float u, float v,
+                           float* out, int cap);
+/* Left-to-right candidate scan of one camera pair: MultiSOFGPU::LaunchTrackingPrimaryToSecondary
+ * (libs/sof/sof_multicamera_gpu.cpp:118-190) with horizontal LK per round (or_lk_track_horizontal).
+ * Candidates of point i: cand_xy[cand_off[i] .. cand_off[i+1]) (x, y pairs); valid may be NULL.
+ * Writes out[n] (matched: the winning attempt's record; unmatched: track = uv or (0, 0) when not
+ * valid, offset and info 0, status 0), winner[n] (-1 = none) and stats[4] = {matched, rounds run,
+ * attempts, 0}. */
+void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const* prim_gx,
+                    const float* const* prim_img, const float* const* sec_img, const float* uv, const uint8_t* valid,
+                    int n, const int32_t* cand_off, const float* cand_xy, float search_radius, float ncc_threshold,
+                    float early_exit_fraction, int mode, or_track_data* out, int32_t* winner, int32_t* stats);
+
 /* FP64 differentiable LK tracker and its adjoint (lk_adjoint64.c). */
 enum { OR64_IMPLICIT = 0, OR64_UNROLLED = 1 };
 typedef struct or64_cam or64_cam;

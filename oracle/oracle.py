@@ -45,6 +45,9 @@ def lib():
         L.or_lk_track.argtypes = [I, P, P, P, P, P, P, P, I, I]
         L.or_lk_track_horizontal.argtypes = [I, P, P, P, P, P, P, I, I]
         L.or_lk_track_f64.argtypes = [I, P, P, P, P, P, P, P, I]
+        L.or_epipolar_candidates.argtypes = [I, I, F, P, P, F, F, P, I]
+        L.or_epipolar_candidates.restype = I
+        L.or_stereo_scan.argtypes = [I, P, P, P, P, P, P, P, I, P, P, F, F, F, I, P, P, P]
         for name, args, res in _CPU_SIGS:
             fn = getattr(L, name, None)
             if fn is None:
@@ -189,6 +192,60 @@ def lk(prev_pyr, cur_pyr, tracks, mode=TEXTURE, horizontal=False, f64=False):
         L.or_lk_track(levels, _p(ws), _p(hs), pgx, pgy, pim, cim, _p(t), len(t), mode)
     del keep1, keep2, keep3, keep4
     return t
+
+
+def epipolar_candidates(cw, ch, inv_scale, offsets, xy, uv, valid=None):
+    """Candidate lists of the points uv (n x 2) from an epipolar table (cw x ch corners, CSR
+    offsets and x, y pairs), as (offsets (n + 1,) int32, xy (m, 2) float32); points with valid == 0
+    get none."""
+    L = lib()
+    offsets = np.ascontiguousarray(offsets, np.int32)
+    xy = np.ascontiguousarray(xy, np.float32)
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    cap = int(max(np.diff(offsets).max(initial=0), 0))
+    buf = np.zeros((max(cap, 1), 2), np.float32)
+    out_off = [0]
+    out_xy = []
+    for i, (u, v) in enumerate(uv):
+        n = 0
+        if valid is None or valid[i]:
+            n = L.or_epipolar_candidates(cw, ch, float(inv_scale), _p(offsets), _p(xy), float(u), float(v), _p(buf), cap)
+        out_xy.append(buf[:n].copy())
+        out_off.append(out_off[-1] + n)
+    xy_all = np.concatenate(out_xy) if out_off[-1] else np.zeros((0, 2), np.float32)
+    return np.array(out_off, np.int32), xy_all.astype(np.float32)
+
+
+def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_radius=48.0, ncc_threshold=0.8,
+                early_exit_fraction=0.8, mode=TEXTURE):
+    """The reference's left-to-right candidate scan (or_stereo_scan) on host pyramids [(img, gx, gy)]
+    per level.  Returns (TRACK_DTYPE records, winner int32, stats int32[4])."""
+    from cuvslam_b200.types import TRACK_DTYPE
+    L = lib()
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    n = len(uv)
+    levels = len(prim_pyr)
+    ws = np.array([p[0].shape[1] for p in prim_pyr] + [0] * (10 - levels), np.int32)
+    hs = np.array([p[0].shape[0] for p in prim_pyr] + [0] * (10 - levels), np.int32)
+    keep1, pgx = _level_ptrs([p[1] for p in prim_pyr])
+    keep2, pim = _level_ptrs([p[0] for p in prim_pyr])
+    keep3, sim = _level_ptrs([p[0] for p in sec_pyr[:levels]])
+    cand_off = np.ascontiguousarray(cand_off, np.int32)
+    cand_xy = np.ascontiguousarray(cand_xy, np.float32).reshape(-1, 2)
+    if len(cand_xy) == 0:
+        cand_xy = np.zeros((1, 2), np.float32)
+    vp = None
+    if valid is not None:
+        valid = np.ascontiguousarray(valid, np.uint8)
+        vp = _p(valid)
+    out = np.zeros(max(n, 1), TRACK_DTYPE)
+    win = np.zeros(max(n, 1), np.int32)
+    stats = np.zeros(4, np.int32)
+    L.or_stereo_scan(levels, _p(ws), _p(hs), pgx, pim, sim, _p(uv), vp, n, _p(cand_off), _p(cand_xy),
+                     float(search_radius), float(ncc_threshold), float(early_exit_fraction), mode, _p(out), _p(win),
+                     _p(stats))
+    del keep1, keep2, keep3
+    return out[:n], win[:n], stats
 
 
 class CpuCamera:

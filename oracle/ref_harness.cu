@@ -13,6 +13,7 @@
 //   - GPUGradientPyramid::set                                           (gradient_pyramid.cpp:83-118)
 //   - GPUSelection::computeGFTTAndSelectFeatures incl. host quota loop  (selection_v2.cpp:27-184)
 //   - GPULKFeatureTracker::track_points                                 (cuda_modules/lk_tracker.cpp:24-73)
+//   - MultiSOFGPU::LaunchTrackingPrimaryToSecondary's candidate scan    (sof/sof_multicamera_gpu.cpp:118-190)
 // Every entry point takes and returns HOST buffers and synchronises; it is a checker, not fast.
 
 #include <cuda_runtime.h>
@@ -332,6 +333,83 @@ int ref_lk(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int ma
   HCHECK(cudaDeviceSynchronize());
   HCHECK(cudaMemcpy(tracks, d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToHost));
   cudaFree(d);
+  return 0;
+}
+
+// MultiSOFGPU::LaunchTrackingPrimaryToSecondary's scan between the pyramids of a primary and a
+// secondary u8 image: one lk_track_horizontal launch per candidate index k over all n points, a copy
+// back and a synchronisation, first success wins, early exit once matched >= frac * n.  Candidates
+// of point i: cand_xy[cand_off[i] .. cand_off[i+1]); valid may be null.  out: n TrackData records as
+// the reference publishes them; winner[i]: winning candidate or -1; stats: matched, rounds launched.
+int ref_stereo_scan(const uint8_t* prim_img, const uint8_t* sec_img, int w, int h, int max_levels, const float* uv,
+                    const uint8_t* valid, int n, const int* cand_off, const float* cand_xy, float radius,
+                    float ncc_thr, float frac, void* out, int* winner, int* stats) {
+  int rc = init_tables();
+  if (rc) return rc;
+  Pyr pp, sp;
+  rc = build(prim_img, w, h, max_levels, pp, 0);
+  if (rc) return rc;
+  rc = build(sec_img, w, h, max_levels, sp, 0);
+  if (rc) return rc;
+  std::vector<TrackData> data((size_t)(n > 0 ? n : 1)), win((size_t)(n > 0 ? n : 1));
+  std::vector<int> len((size_t)(n > 0 ? n : 1));
+  int max_candidates = 0;
+  for (int i = 0; i < n; ++i) {
+    len[i] = (valid && !valid[i]) ? 0 : cand_off[i + 1] - cand_off[i];
+    if (len[i] > max_candidates) max_candidates = len[i];
+    win[i] = TrackData{};
+    winner[i] = -1;
+  }
+  TrackData* d = nullptr;
+  HCHECK(cudaMalloc((void**)&d, sizeof(TrackData) * data.size()));
+  Pyramid gx = make_pyr(pp, pp.gx), pi = make_pyr(pp, pp.img), si = make_pyr(sp, sp.img);
+  auto uv_of = [&](int i, int c) { return (valid && !valid[i]) ? 0.f : uv[2 * i + c]; };
+  int tracked = 0, rounds = 0;
+  for (int k = 0; k < max_candidates; ++k) {
+    bool any_active = false;
+    for (int i = 0; i < n; ++i) {
+      TrackData& t = data[i];
+      t.ncc_threshold = ncc_thr;
+      t.track = {uv_of(i, 0), uv_of(i, 1)};
+      t.track_status = false;
+      t.search_radius_px = radius;
+      for (int q = 0; q < 4; ++q) t.info[q] = 0.f;
+      if (win[i].track_status || k >= len[i]) {
+        t.offset = {0.f, 0.f};
+      } else {
+        const float* c = cand_xy + 2 * ((size_t)cand_off[i] + k);
+        t.offset = {c[0] - uv_of(i, 0), c[1] - uv_of(i, 1)};
+        any_active = true;
+      }
+    }
+    if (!any_active) break;
+    HCHECK(cudaMemcpy(d, data.data(), sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
+    HCHECK(lk_track_horizontal(gx, pi, si, d, n, 0));
+    HCHECK(cudaMemcpy(data.data(), d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToHost));
+    HCHECK(cudaDeviceSynchronize());
+    rounds = k + 1;
+    for (int i = 0; i < n; ++i) {
+      if (win[i].track_status || k >= len[i]) continue;
+      if (data[i].track_status) {
+        win[i] = data[i];
+        winner[i] = k;
+        ++tracked;
+      }
+    }
+    if ((float)tracked >= frac * (float)n) break;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (win[i].track_status) {
+      data[i] = win[i];
+    } else {
+      data[i].track_status = false;
+      data[i].track = {uv_of(i, 0), uv_of(i, 1)};
+    }
+  }
+  cudaFree(d);
+  if (n > 0) memcpy(out, data.data(), sizeof(TrackData) * (size_t)n);
+  stats[0] = tracked;
+  stats[1] = rounds;
   return 0;
 }
 

@@ -2,6 +2,8 @@
 
 Step 1 (any machine, no GPU):   python tests/golden/make_golden.py inputs
     Draws the seeded synthetic input frames and writes tests/golden/inputs.npz.
+    (`stereo-inputs` likewise writes tests/golden/stereo_inputs.npz: a rectified right image of the
+    c1 scene, primary points and their candidate lists for the left-to-right scan.)
 Step 2 (a B200, after oracle/build_ref.sh built oracle/_ref/libcuvslam_ref.so):
     python tests/golden/make_golden.py reference --out DIR
     Runs the reference's own CUDA kernels (compiled unchanged from cuVSLAM by oracle/build_ref.sh)
@@ -9,6 +11,9 @@ Step 2 (a B200, after oracle/build_ref.sh built oracle/_ref/libcuvslam_ref.so):
     the sorted keypoints, the selected features, the LK results and a texture-sampling probe) and
     DIR/reference_full.npz (every intermediate array, for debugging; not committed).
 The committed tests/golden/reference.npz is the step-2 output.
+`stereo-reference --out DIR` runs the reference's multi-launch left-to-right scan
+(lk_track_horizontal per candidate round, oracle/ref_harness.cu) on stereo_inputs.npz and writes
+DIR/stereo_reference.npz.
 """
 
 import argparse
@@ -191,12 +196,89 @@ def make_reference(out_dir):
     print("wrote", out_dir)
 
 
+# Left-to-right scan fixtures: the c1 scene (left: inputs.npz c1/prev) and its rectified right view (disparity 5-40 px), 4-level
+# pyramids (top level 3), primary points, and two candidate sets: the epipolar table of a pinhole
+# pair (fx 458, baseline 0.11 m) and random lists of 0-12 candidates left of each point.
+STEREO_LEVELS = 4
+STEREO_RUNS = {  # name -> (candidate set, early-exit fraction)
+    "curves": ("curves", 0.8),
+    "random": ("random", 0.8),
+    "random_full": ("random", 1.0),
+    "random_low": ("random", 0.3),
+}
+
+
+def make_stereo_inputs(path):
+    from cuvslam_b200 import stereo
+    from oracle import oracle
+
+    w, h, cam = CASES["c1"]
+    left = np.load(os.path.join(HERE, "inputs.npz"))["c1/prev"]
+    right = synthetic.stereo_right(cam, w, h)
+    rng = np.random.default_rng(61)
+    n = 700
+    uv = np.stack([rng.uniform(6.0, w - 6.0, n), rng.uniform(6.0, h - 6.0, n)], 1).astype(np.float32)
+    uv[:6] = [[0.5, 0.5], [w - 0.5, h - 0.5], [w - 1.0, 10.0], [3.0, h / 2], [w / 2, 0.0], [w / 2, h - 1.0]]
+    valid = (rng.uniform(size=n) > 0.03).astype(np.uint8)
+    sizes = level_sizes(w, h, STEREO_LEVELS)
+    top = len(sizes) - 1
+    k = (458.0, 458.0, 367.0, 248.0)
+    curves = stereo.pinhole_curves(k, k, (np.eye(3), (-0.11, 0.0, 0.0)), top, sizes[top][0], sizes[top][1])
+    cw, ch, c_off, c_xy = stereo.curves_csr(curves)
+    inv_scale = 1.0 / float(1 << top)
+    off_c, xy_c = oracle.epipolar_candidates(cw, ch, inv_scale, c_off, c_xy, uv, valid)
+    counts = rng.integers(0, 13, n)
+    off_r = np.zeros(n + 1, np.int32)
+    np.cumsum(counts, out=off_r[1:])
+    xs = np.repeat(uv[:, 0], counts) - rng.uniform(0.0, 80.0, off_r[-1])
+    ys = np.repeat(uv[:, 1], counts) + rng.normal(0.0, 0.5, off_r[-1])
+    xy_r = np.stack([xs, ys], 1).astype(np.float32)
+    np.savez_compressed(path, right=right, uv=uv, valid=valid, top=np.int32(top),
+                        curves_wh=np.array([cw, ch], np.int32), curves_inv_scale=np.float32(inv_scale),
+                        curves_offsets=c_off, curves_xy=c_xy, curves_cand_off=off_c, curves_cand_xy=xy_c,
+                        random_cand_off=off_r, random_cand_xy=xy_r)
+
+
+def make_stereo_reference(out_dir):
+    lib = _lib()
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.ref_stereo_scan.argtypes = [P, P, I, I, I, P, P, I, P, P, F, F, F, P, P, P]
+    inp = np.load(os.path.join(HERE, "stereo_inputs.npz"))
+    left = np.ascontiguousarray(np.load(os.path.join(HERE, "inputs.npz"))["c1/prev"])
+    right = np.ascontiguousarray(inp["right"])
+    h, w = left.shape
+    uv = np.ascontiguousarray(inp["uv"], np.float32)
+    valid = np.ascontiguousarray(inp["valid"], np.uint8)
+    n = len(uv)
+    radius = 3.0 * float(1 << (int(inp["top"]) + 1))
+    compact = {}
+    for run, (cset, frac) in STEREO_RUNS.items():
+        off = np.ascontiguousarray(inp[f"{cset}_cand_off"], np.int32)
+        xy = np.ascontiguousarray(inp[f"{cset}_cand_xy"], np.float32)
+        out = np.zeros(n, TRACK_DTYPE)
+        win = np.zeros(n, np.int32)
+        stats = np.zeros(2, np.int32)
+        rc = lib.ref_stereo_scan(_ptr(left), _ptr(right), w, h, STEREO_LEVELS, _ptr(uv), _ptr(valid), n, _ptr(off),
+                                 _ptr(xy), radius, 0.8, frac, _ptr(out), _ptr(win), _ptr(stats))
+        assert rc == 0, rc
+        compact[f"{run}/out"] = out
+        compact[f"{run}/winner"] = win
+        compact[f"{run}/stats"] = stats
+        print(run, "matched", stats[0], "rounds", stats[1])
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "stereo_reference.npz"), **compact)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["inputs", "reference"])
+    ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if a.step == "inputs":
         make_inputs(os.path.join(HERE, "inputs.npz"))
+    elif a.step == "stereo-inputs":
+        make_stereo_inputs(os.path.join(HERE, "stereo_inputs.npz"))
+    elif a.step == "stereo-reference":
+        make_stereo_reference(a.out)
     else:
         make_reference(a.out)

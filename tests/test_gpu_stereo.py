@@ -1,0 +1,196 @@
+"""Left-to-right matching on the GPU (fe_track_stereo): the candidate scan of every camera pair in one
+launch, bit-identical to the oracle's restatement of the reference's multi-launch scan, and
+within 0.01 px median / 0.05 px p99 of the reference's own kernels run in that scan."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ROOT, assert_tracks_equal, gpu_pyramid
+from cuvslam_b200 import _lib
+from cuvslam_b200.stereo import EpipolarCurves, StereoMatcher, StereoPair, cross_cam_search_radius
+from cuvslam_b200.types import TRACK_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+LEVELS = 4
+RUNS = {"curves": ("curves", 0.8), "random": ("random", 0.8), "random_full": ("random", 1.0),
+        "random_low": ("random", 0.3)}
+
+
+@pytest.fixture(scope="module")
+def stereo_case(ctx, oracle):
+    inp = np.load(os.path.join(GOLD, "stereo_inputs.npz"))
+    left = np.load(os.path.join(GOLD, "inputs.npz"))["c1/prev"]
+    right = inp["right"]
+    pp, sp = gpu_pyramid(ctx, left, LEVELS), gpu_pyramid(ctx, right, LEVELS)
+    opp, osp = oracle.pyramid(left, LEVELS), oracle.pyramid(right, LEVELS)
+    return inp, pp, sp, opp, osp
+
+
+def _records(t):
+    return t.cpu().numpy().reshape(-1).view(TRACK_DTYPE).copy()
+
+
+def _explicit_pair(pp, sp, inp, cset, uv=None, valid="fixture"):
+    uv = inp["uv"] if uv is None else uv
+    off = inp[f"{cset}_cand_off"]
+    return StereoPair(pp, sp, torch.from_numpy(np.ascontiguousarray(uv)).cuda(),
+                      cand_offsets=torch.from_numpy(off).cuda(),
+                      cand_xy=torch.from_numpy(np.ascontiguousarray(inp[f"{cset}_cand_xy"])).cuda(),
+                      max_candidates=int(np.diff(off).max(initial=0)),
+                      valid=torch.from_numpy(inp["valid"]).cuda() if isinstance(valid, str) else valid)
+
+
+def _oracle_run(oracle, opp, osp, inp, cset, frac, radius):
+    return oracle.stereo_scan(opp, osp, inp["uv"], inp[f"{cset}_cand_off"], inp[f"{cset}_cand_xy"], inp["valid"],
+                              radius, 0.8, frac)
+
+
+@pytest.mark.parametrize("run", list(RUNS))
+def test_matches_oracle_and_reference(ctx, oracle, stereo_case, run):
+    inp, pp, sp, opp, osp = stereo_case
+    cset, frac = RUNS[run]
+    radius = cross_cam_search_radius(pp.levels - 1)
+    (out, win, st), = StereoMatcher(ctx, early_exit_fraction=frac).track_primary_to_secondary(
+        [_explicit_pair(pp, sp, inp, cset)])
+    torch.cuda.synchronize()
+    got, gwin, gst = _records(out), win.cpu().numpy(), st.cpu().numpy()
+    want, wwin, wst = _oracle_run(oracle, opp, osp, inp, cset, frac, radius)
+    assert_tracks_equal(got, want)
+    np.testing.assert_array_equal(gwin, wwin)
+    np.testing.assert_array_equal(gst[:2], wst[:2])
+    assert gst[2] >= wst[2]  # attempts: the reference's, plus speculative ones whose point won earlier
+    path = os.path.join(GOLD, "stereo_reference.npz")
+    if os.path.exists(path):
+        # the reference's texture unit rounds its 4-tap sums differently from the FP32 emulation, so a
+        # marginal attempt (NCC or step right at its threshold) may decide the other way
+        ref = np.load(path)
+        rwin, rst, rout = ref[f"{run}/winner"], ref[f"{run}/stats"], ref[f"{run}/out"]
+        assert np.mean(gwin == rwin) >= 0.995
+        assert gst[1] == rst[1] and abs(int(gst[0]) - int(rst[0])) <= max(2, rst[0] // 100)
+        same = (gwin == rwin) & (gwin >= 0)
+        d = np.linalg.norm(got["track"][same] - rout["track"][same], axis=1)
+        assert np.median(d) <= 0.01 and np.percentile(d, 99) <= 0.05
+        np.testing.assert_array_equal(got["track"][(gwin < 0) & (rwin < 0)], rout["track"][(gwin < 0) & (rwin < 0)])
+
+
+def test_curves_on_device_equal_explicit_lists(ctx, oracle, stereo_case):
+    """Candidates interpolated from the epipolar table inside the kernel equal the oracle's
+    EpipolarCurves::Candidates lists given explicitly."""
+    inp, pp, sp, opp, osp = stereo_case
+    cw, ch = (int(v) for v in inp["curves_wh"])
+    curves = [[inp["curves_xy"][inp["curves_offsets"][v * cw + u]:inp["curves_offsets"][v * cw + u + 1]]
+               for u in range(cw)] for v in range(ch)]
+    table = EpipolarCurves(curves, int(inp["top"]))
+    assert table.inv_scale == float(inp["curves_inv_scale"])
+    uv = torch.from_numpy(inp["uv"]).cuda()
+    valid = torch.from_numpy(inp["valid"]).cuda()
+    m = StereoMatcher(ctx)
+    (o1, w1, s1), (o2, w2, s2) = m.track_primary_to_secondary(
+        [StereoPair(pp, sp, uv, curves=table, valid=valid), _explicit_pair(pp, sp, inp, "curves")])
+    torch.cuda.synchronize()
+    assert_tracks_equal(_records(o1), _records(o2))
+    np.testing.assert_array_equal(w1.cpu().numpy(), w2.cpu().numpy())
+    np.testing.assert_array_equal(s1.cpu().numpy()[:2], s2.cpu().numpy()[:2])
+
+
+def test_pairs_in_one_launch_are_independent(ctx, oracle, stereo_case):
+    """Three pairs (different point sets, candidate sets, an empty pair and a pair without any
+    candidate) in one launch give each pair's own scan; early exit is per pair."""
+    inp, pp, sp, opp, osp = stereo_case
+    radius = cross_cam_search_radius(pp.levels - 1)
+    rng = np.random.default_rng(3)
+    sub = np.sort(rng.choice(len(inp["uv"]), 250, replace=False))
+    uv_sub = inp["uv"][sub]
+    off = inp["random_cand_off"]
+    lists = [inp["random_cand_xy"][off[i]:off[i + 1]] for i in sub]
+    off_sub = np.zeros(len(sub) + 1, np.int32)
+    np.cumsum([len(c) for c in lists], out=off_sub[1:])
+    xy_sub = np.concatenate(lists).astype(np.float32)
+    frac = 0.3
+    pair_a = _explicit_pair(pp, sp, inp, "curves")
+    pair_b = StereoPair(pp, sp, torch.from_numpy(uv_sub).cuda(), cand_offsets=torch.from_numpy(off_sub).cuda(),
+                        cand_xy=torch.from_numpy(xy_sub).cuda(), max_candidates=int(np.diff(off_sub).max()))
+    pair_c = StereoPair(pp, sp, torch.zeros((0, 2), dtype=torch.float32, device="cuda"),
+                        cand_offsets=torch.zeros(1, dtype=torch.int32, device="cuda"),
+                        cand_xy=torch.zeros((1, 2), dtype=torch.float32, device="cuda"), max_candidates=0)
+    pair_d = StereoPair(pp, sp, torch.from_numpy(uv_sub[:40]).cuda(),
+                        cand_offsets=torch.zeros(41, dtype=torch.int32, device="cuda"),
+                        cand_xy=torch.zeros((1, 2), dtype=torch.float32, device="cuda"), max_candidates=0)
+    res = StereoMatcher(ctx, early_exit_fraction=frac).track_primary_to_secondary([pair_a, pair_b, pair_c, pair_d])
+    torch.cuda.synchronize()
+    wa = oracle.stereo_scan(opp, osp, inp["uv"], inp["curves_cand_off"], inp["curves_cand_xy"], inp["valid"], radius,
+                            0.8, frac)
+    wb = oracle.stereo_scan(opp, osp, uv_sub, off_sub, xy_sub, None, radius, 0.8, frac)
+    wd = oracle.stereo_scan(opp, osp, uv_sub[:40], np.zeros(41, np.int32), np.zeros((0, 2), np.float32), None,
+                            radius, 0.8, frac)
+    for (out, win, st), (wo, ww, ws) in zip([res[0], res[1], res[3]], [wa, wb, wd]):
+        assert_tracks_equal(_records(out), wo)
+        np.testing.assert_array_equal(win.cpu().numpy(), ww)
+        np.testing.assert_array_equal(st.cpu().numpy()[:2], ws[:2])
+    assert res[2][0].shape[0] == 0 and res[2][2].cpu().numpy()[0] == 0
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.1, 2.0])
+def test_early_exit_edges(ctx, oracle, stereo_case, frac):
+    """frac * n <= 0 stops after round 0 whatever it matched; frac > 1 never stops early."""
+    inp, pp, sp, opp, osp = stereo_case
+    radius = cross_cam_search_radius(pp.levels - 1)
+    (out, win, st), = StereoMatcher(ctx, early_exit_fraction=frac).track_primary_to_secondary(
+        [_explicit_pair(pp, sp, inp, "random")])
+    torch.cuda.synchronize()
+    want, wwin, wst = _oracle_run(oracle, opp, osp, inp, "random", frac, radius)
+    assert_tracks_equal(_records(out), want)
+    np.testing.assert_array_equal(win.cpu().numpy(), wwin)
+    np.testing.assert_array_equal(st.cpu().numpy()[:2], wst[:2])
+
+
+def test_exact_sampling_and_determinism(ctx, oracle, stereo_case):
+    inp, pp, sp, opp, osp = stereo_case
+    radius = cross_cam_search_radius(pp.levels - 1)
+    m = StereoMatcher(ctx, sampling=_lib.FE_SAMPLE_EXACT)
+    first = None
+    for _ in range(3):
+        (out, win, st), = m.track_primary_to_secondary([_explicit_pair(pp, sp, inp, "random")])
+        torch.cuda.synchronize()
+        got = (_records(out), win.cpu().numpy())
+        if first is None:
+            first = got
+        else:
+            assert_tracks_equal(got[0], first[0])
+            np.testing.assert_array_equal(got[1], first[1])
+    want, wwin, _ = oracle.stereo_scan(opp, osp, inp["uv"], inp["random_cand_off"], inp["random_cand_xy"],
+                                       inp["valid"], radius, 0.8, 0.8, mode=oracle.EXACT)
+    assert_tracks_equal(first[0], want)
+    np.testing.assert_array_equal(first[1], wwin)
+
+
+def test_cut_lists_are_flagged(ctx, oracle, stereo_case):
+    """Lists longer than max_candidates are cut to it (and stats[3] says so)."""
+    inp, pp, sp, opp, osp = stereo_case
+    pair = _explicit_pair(pp, sp, inp, "random")
+    pair.max_candidates = 3
+    (out, win, st), = StereoMatcher(ctx).track_primary_to_secondary([pair])
+    torch.cuda.synchronize()
+    off = inp["random_cand_off"]
+    lists = [inp["random_cand_xy"][off[i]:off[i] + min(3, off[i + 1] - off[i])] for i in range(len(off) - 1)]
+    off3 = np.zeros(len(lists) + 1, np.int32)
+    np.cumsum([len(c) for c in lists], out=off3[1:])
+    want, wwin, wst = oracle.stereo_scan(opp, osp, inp["uv"], off3, np.concatenate(lists), inp["valid"],
+                                         cross_cam_search_radius(pp.levels - 1), 0.8, 0.8)
+    assert_tracks_equal(_records(out), want)
+    np.testing.assert_array_equal(win.cpu().numpy(), wwin)
+    assert st.cpu().numpy()[3] & 1
+
+
+def test_bad_arguments(ctx, stereo_case):
+    inp, pp, sp, opp, osp = stereo_case
+    lib = ctx.lib
+    pairs = (_lib.FeStereoPair * 1)()
+    assert lib.fe_track_stereo(ctx.handle, pairs, 0, 0.8, 0, None) == 1
+    assert lib.fe_track_stereo(ctx.handle, pairs, 17, 0.8, 0, None) == 4
+    assert lib.fe_track_stereo(ctx.handle, pairs, 1, 0.8, 0, None) == 1  # no pyramids
