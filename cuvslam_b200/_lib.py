@@ -14,6 +14,7 @@ MAX_LEVELS = 10
 FE_OK = 0
 FE_SAMPLE_TEXTURE = 0
 FE_SAMPLE_EXACT = 1
+FE_SAMPLE_TEXTURE_WIDE = 2
 
 
 class FePyramid(ctypes.Structure):

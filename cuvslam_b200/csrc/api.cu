@@ -470,7 +470,7 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
              int horizontal, int sampling, fe_stream stream) {
   if (!ctx || !valid_pyramid(prev) || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
   if (cur->levels < prev->levels) return FE_ERR_INVALID_ARGUMENT;
-  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
   if (!horizontal)
     for (int l = 0; l < prev->levels; ++l)
       if (!prev->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
@@ -497,7 +497,7 @@ int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, fl
                     int sampling, fe_stream stream) {
   if (!ctx || !pairs || npairs <= 0) return FE_ERR_INVALID_ARGUMENT;
   if (npairs > fe::kMaxStereoPairs) return FE_ERR_CAPACITY;
-  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
   if (!(early_exit_fraction == early_exit_fraction)) return FE_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
   // scratch layout: [counter, done, per pair: attempts, cnt[maxc]] zeroed; [per pair: stop, best[n]]
@@ -815,7 +815,7 @@ int fe_batch_tuning(const fe_batch* b, int32_t* lk_shape, int32_t* overlap, int3
 int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int sampling, fe_batch** out) {
   if (!ctx || !cams || !out || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
   if (ncams > fe::kMaxCams) return FE_ERR_CAPACITY;
-  if (sampling != FE_SAMPLE_TEXTURE && sampling != FE_SAMPLE_EXACT) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   fe_batch* b = new (std::nothrow) fe_batch;
   if (!b) return FE_ERR_OUT_OF_MEMORY;

@@ -19,8 +19,9 @@
 // stop when |v|^2 < 0.12^2 (|v| < 0.12 horizontally), level search-radius gate, 5x5 NCC gate, and
 // coordinates scaled by 2 about (0.5, 0.5) between levels.  Texture sampling is restated in
 // software: FE_SAMPLE_TEXTURE uses cudaFilterModeLinear's 8-bit-fraction weight rule (round-half-up
-// fractions; corner products rounded half up, cross products half down), FE_SAMPLE_EXACT exact
-// weights.  Divisions are IEEE (the reference's __fdividef differs by <= 2 ulp).
+// fractions; corner products rounded half up, cross products half down) with an FP32 multiply-add
+// chain, FE_SAMPLE_TEXTURE_WIDE the same weights with the 4-tap sum rounded once (FP64), and
+// FE_SAMPLE_EXACT exact weights.  Divisions are IEEE (the reference's __fdividef differs by <= 2 ulp).
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -113,6 +114,9 @@ cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s) {
   if (p.mode == kLkUnrolled) return launch<FE_SAMPLE_EXACT, false, kModeUnrolled>(p, s);
   if (p.sampling == FE_SAMPLE_EXACT)
     return p.horizontal ? launch<FE_SAMPLE_EXACT, true, kModeRef>(p, s) : launch<FE_SAMPLE_EXACT, false, kModeRef>(p, s);
+  if (p.sampling == FE_SAMPLE_TEXTURE_WIDE)
+    return p.horizontal ? launch<FE_SAMPLE_TEXTURE_WIDE, true, kModeRef>(p, s)
+                        : launch<FE_SAMPLE_TEXTURE_WIDE, false, kModeRef>(p, s);
   return p.horizontal ? launch<FE_SAMPLE_TEXTURE, true, kModeRef>(p, s) : launch<FE_SAMPLE_TEXTURE, false, kModeRef>(p, s);
 }
 

@@ -39,6 +39,9 @@ struct TapSet {
   float fr;      // this lane's column/row fraction
 };
 
+// Texture-unit weight rule (8-bit fractions) in both texture modes.
+constexpr bool quantised(int sampling) { return sampling != FE_SAMPLE_EXACT; }
+
 template <int SAMPLING>
 __device__ __forceinline__ TapSet make_taps(float xmin, float ymin, int bx, int by, int stride, int lane) {
   TapSet s;
@@ -48,15 +51,15 @@ __device__ __forceinline__ TapSet make_taps(float xmin, float ymin, int bx, int 
   const float fl = floorf(pb);
   s.fr = __fsub_rn(pb, fl);
   s.base = (int)fl;
-  s.q = (SAMPLING == FE_SAMPLE_TEXTURE) ? (int)floorf(__fmaf_rn(s.fr, 256.f, 0.5f)) : 0;
+  s.q = quantised(SAMPLING) ? (int)floorf(__fmaf_rn(s.fr, 256.f, 0.5f)) : 0;
   const int base0x = __shfl_sync(kFull, s.base, 0), base0y = __shfl_sync(kFull, s.base, 16);
   const int q0x = __shfl_sync(kFull, s.q, 0), q0y = __shfl_sync(kFull, s.q, 16);
   const float fr0x = __shfl_sync(kFull, s.fr, 0), fr0y = __shfl_sync(kFull, s.fr, 16);
   bool ok = true;
-  if (is_col) ok = s.base == base0x + lane && (SAMPLING == FE_SAMPLE_TEXTURE ? s.q == q0x : s.fr == fr0x);
-  if (is_row) ok = s.base == base0y + (lane - 16) && (SAMPLING == FE_SAMPLE_TEXTURE ? s.q == q0y : s.fr == fr0y);
+  if (is_col) ok = s.base == base0x + lane && (quantised(SAMPLING) ? s.q == q0x : s.fr == fr0x);
+  if (is_row) ok = s.base == base0y + (lane - 16) && (quantised(SAMPLING) ? s.q == q0y : s.fr == fr0y);
   s.uniform = __all_sync(kFull, ok);
-  if (SAMPLING == FE_SAMPLE_TEXTURE) {
+  if (quantised(SAMPLING)) {
     tex_weights(q0x, q0y, s.u);
   } else {
     s.u.w00 = fr0x;
@@ -79,7 +82,7 @@ __device__ __forceinline__ Tap tap_of(const TapSet& s, int ix, int iy, int bx, i
   Tap t;
   const int bxe = __shfl_sync(kFull, s.base, ix), bye = __shfl_sync(kFull, s.base, 16 + iy);
   t.off = (bye - by) * stride + (bxe - bx);
-  if (SAMPLING == FE_SAMPLE_TEXTURE) {
+  if (quantised(SAMPLING)) {
     tex_weights(__shfl_sync(kFull, s.q, ix), __shfl_sync(kFull, s.q, 16 + iy), t);
   } else {
     t.w00 = __shfl_sync(kFull, s.fr, ix);
@@ -93,6 +96,13 @@ template <int SAMPLING>
 __device__ __forceinline__ float sample(const float* win, int stride, const Tap& t) {
   const float t00 = win[t.off], t10 = win[t.off + 1];
   const float t01 = win[t.off + stride], t11 = win[t.off + stride + 1];
+  if (SAMPLING == FE_SAMPLE_TEXTURE_WIDE) {
+    // w * t is exact in FP64 (9 + 24 significant bits): the sum is rounded to FP32 once
+    double v = __dmul_rn((double)t.w00, (double)t00);
+    v = __fma_rn((double)t.w10, (double)t10, v);
+    v = __fma_rn((double)t.w01, (double)t01, v);
+    return __double2float_rn(__fma_rn((double)t.w11, (double)t11, v));
+  }
   if (SAMPLING == FE_SAMPLE_TEXTURE) {
     float v = __fmul_rn(t.w00, t00);
     v = __fmaf_rn(t.w10, t10, v);

@@ -267,7 +267,9 @@ cudaError_t launch_sampling(const StereoLaunch& p, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_stereo(const StereoLaunch& p, cudaStream_t s) {
-  return p.sampling == FE_SAMPLE_EXACT ? launch_sampling<FE_SAMPLE_EXACT>(p, s) : launch_sampling<FE_SAMPLE_TEXTURE>(p, s);
+  if (p.sampling == FE_SAMPLE_EXACT) return launch_sampling<FE_SAMPLE_EXACT>(p, s);
+  if (p.sampling == FE_SAMPLE_TEXTURE_WIDE) return launch_sampling<FE_SAMPLE_TEXTURE_WIDE>(p, s);
+  return launch_sampling<FE_SAMPLE_TEXTURE>(p, s);
 }
 
 }  // namespace fe

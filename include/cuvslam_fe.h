@@ -79,8 +79,12 @@ typedef struct {
 
 /* Bilinear sampling of LK patches. */
 typedef enum {
-  FE_SAMPLE_TEXTURE = 0, /* cudaFilterModeLinear's 8-bit-fraction weights: matches the reference */
-  FE_SAMPLE_EXACT = 1,   /* exact FP32 weights (differentiable; used by the adjoint) */
+  FE_SAMPLE_TEXTURE = 0,      /* cudaFilterModeLinear's 8-bit-fraction weights, FP32 multiply-add chain:
+                                 matches the reference to well under 0.01 px */
+  FE_SAMPLE_EXACT = 1,        /* exact FP32 weights (differentiable; used by the adjoint) */
+  FE_SAMPLE_TEXTURE_WIDE = 2, /* the texture weights with each 4-tap sum rounded to FP32 once (FP64
+                                 arithmetic), as the texture unit does: equals the hardware's samples
+                                 more often, so marginal accept/reject decisions follow the reference */
 } fe_sampling;
 
 /* ---------------------------------------------------------------------------------------- */

@@ -19,6 +19,7 @@ F = ctypes.c_float
 
 TEXTURE = 0
 EXACT = 1
+TEXTURE_WIDE = 2  # texture weights, each 4-tap sum rounded once (closest to the texture unit)
 
 
 def build():

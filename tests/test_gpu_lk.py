@@ -42,6 +42,25 @@ def test_matches_oracle_and_reference(ctx, oracle, golden, name, run):
         assert np.median(d) <= 0.01 and np.percentile(d, 99) <= 0.05
 
 
+@pytest.mark.parametrize("name", ["c1", "half", "odd"])
+@pytest.mark.parametrize("run", ["lk_zero", "lk_pred", "lk_horiz"])
+def test_wide_texture_sampling(ctx, oracle, golden, name, run):
+    """FE_SAMPLE_TEXTURE_WIDE (4-tap sums rounded once): bit-identical to the oracle's
+    OR_SAMPLE_TEXTURE_WIDE, and within 1e-3 px of the reference kernel with the same statuses."""
+    inp, ref = golden
+    src = {"lk_horiz": "lk_zero"}.get(run, run)
+    tin, tout = ref[f"{name}/{src}/in"], ref[f"{name}/{run}/out"]
+    horizontal = run == "lk_horiz"
+    pp, cp = gpu_pyramid(ctx, inp[f"{name}/prev"]), gpu_pyramid(ctx, inp[f"{name}/next"])
+    got = _run(ctx, pp, cp, tin, horizontal, sampling=_lib.FE_SAMPLE_TEXTURE_WIDE)
+    want = oracle.lk(oracle.pyramid(inp[f"{name}/prev"]), oracle.pyramid(inp[f"{name}/next"]), tin,
+                     horizontal=horizontal, mode=oracle.TEXTURE_WIDE)
+    assert_tracks_equal(got, want)
+    np.testing.assert_array_equal(got["track_status"], tout["track_status"])
+    ok = got["track_status"] == 1
+    assert np.abs(got["track"][ok] - tout["track"][ok]).max(initial=0.0) < 1e-3
+
+
 def test_exact_sampling_matches_oracle(ctx, oracle, golden):
     inp, ref = golden
     tin = ref["half/lk_pred/in"]

@@ -78,6 +78,34 @@ def test_matches_oracle_and_reference(ctx, oracle, stereo_case, run):
         np.testing.assert_array_equal(got["track"][(gwin < 0) & (rwin < 0)], rout["track"][(gwin < 0) & (rwin < 0)])
 
 
+@pytest.mark.parametrize("run", list(RUNS))
+def test_wide_sampling_follows_the_reference(ctx, oracle, stereo_case, run):
+    """With FE_SAMPLE_TEXTURE_WIDE every attempt decides as the reference's texture unit did:
+    winners, statuses and counts equal the reference scan, positions within 1e-3 px; bit-identical
+    to the oracle in the same mode."""
+    path = os.path.join(GOLD, "stereo_reference.npz")
+    if not os.path.exists(path):
+        pytest.skip("stereo_reference.npz not generated")
+    inp, pp, sp, opp, osp = stereo_case
+    cset, frac = RUNS[run]
+    (out, win, st), = StereoMatcher(ctx, sampling=_lib.FE_SAMPLE_TEXTURE_WIDE, early_exit_fraction=frac) \
+        .track_primary_to_secondary([_explicit_pair(pp, sp, inp, cset)])
+    torch.cuda.synchronize()
+    got, gwin, gst = _records(out), win.cpu().numpy(), st.cpu().numpy()
+    radius = cross_cam_search_radius(pp.levels - 1)
+    want, wwin, wst = oracle.stereo_scan(opp, osp, inp["uv"], inp[f"{cset}_cand_off"], inp[f"{cset}_cand_xy"],
+                                         inp["valid"], radius, 0.8, frac, mode=oracle.TEXTURE_WIDE)
+    assert_tracks_equal(got, want)
+    np.testing.assert_array_equal(gwin, wwin)
+    ref = np.load(path)
+    np.testing.assert_array_equal(gwin, ref[f"{run}/winner"])
+    np.testing.assert_array_equal(gst[:2], ref[f"{run}/stats"])
+    rout = ref[f"{run}/out"]
+    np.testing.assert_array_equal(got["track_status"], rout["track_status"])
+    ok = got["track_status"] == 1
+    assert np.abs(got["track"][ok] - rout["track"][ok]).max(initial=0.0) < 1e-3
+
+
 def test_curves_on_device_equal_explicit_lists(ctx, oracle, stereo_case):
     """Candidates interpolated from the epipolar table inside the kernel equal the oracle's
     EpipolarCurves::Candidates lists given explicitly."""

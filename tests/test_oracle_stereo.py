@@ -135,7 +135,7 @@ def test_scan_matches_reference(oracle, case, run):
     # the texture unit's single rounding of each 4-tap sum (OR_SAMPLE_TEXTURE_WIDE) decides every
     # attempt as the hardware did: identical winners, statuses and counts
     out, win, st = oracle.stereo_scan(pp, sp, inp["uv"], inp[f"{cset}_cand_off"], inp[f"{cset}_cand_xy"],
-                                      inp["valid"], radius, 0.8, frac, mode=2)
+                                      inp["valid"], radius, 0.8, frac, mode=oracle.TEXTURE_WIDE)
     np.testing.assert_array_equal(win, rwin)
     np.testing.assert_array_equal(st[:2], rst)
     np.testing.assert_array_equal(out["track_status"], rout["track_status"])
