@@ -126,7 +126,7 @@ _SIGS = {
     "fe_select_noalloc": (_I, [ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
     "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "fe_track": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _P]),
-    "fe_track_stereo": (_I, [_P, ctypes.POINTER(FeStereoPair), _I, ctypes.c_float, _I, _P]),
+    "fe_track_stereo": (_I, [_P, ctypes.POINTER(FeStereoPair), _I, ctypes.c_float, _I, _I, _P]),
     "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),
     "fe_batch_run": (_I, [_P, _P]),
     "fe_batch_run_plain": (_I, [_P, _P]),

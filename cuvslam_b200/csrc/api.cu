@@ -494,7 +494,7 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
 }
 
 int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, float early_exit_fraction,
-                    int sampling, fe_stream stream) {
+                    int horizontal, int sampling, fe_stream stream) {
   if (!ctx || !pairs || npairs <= 0) return FE_ERR_INVALID_ARGUMENT;
   if (npairs > fe::kMaxStereoPairs) return FE_ERR_CAPACITY;
   if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
@@ -508,6 +508,9 @@ int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, fl
     const fe_stereo_pair& P = pairs[q];
     if (!valid_pyramid(P.primary) || !valid_pyramid(P.secondary)) return FE_ERR_INVALID_ARGUMENT;
     if (P.secondary->levels < P.primary->levels) return FE_ERR_INVALID_ARGUMENT;
+    if (!horizontal)
+      for (int l = 0; l < P.primary->levels; ++l)
+        if (!P.primary->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
     if (P.n < 0 || (P.n > 0 && (!P.uv || !P.out))) return FE_ERR_INVALID_ARGUMENT;
     if ((uintptr_t)P.out % 16 != 0 || (uintptr_t)P.uv % 8 != 0) return FE_ERR_INVALID_ARGUMENT;
     int maxc = 0;
@@ -556,6 +559,7 @@ int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, fl
   L.counter = zw;
   L.done = zw + 1;
   L.sampling = sampling;
+  L.horizontal = horizontal ? 1 : 0;
   zw += 2;
   int begin = 0;
   for (int q = 0; q < npairs; ++q) {

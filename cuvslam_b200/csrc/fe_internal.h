@@ -170,6 +170,7 @@ struct StereoLaunch {
   int* counter;                 // attempt counter of the persistent warps (zeroed)
   int* done;                    // CTA counter (zeroed): the last CTA publishes the results
   int sampling;
+  int horizontal;               // 1-D (x only) LK for rectified pairs
   StereoPair pair[kMaxStereoPairs];
 };
 

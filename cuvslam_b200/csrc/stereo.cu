@@ -1,5 +1,5 @@
-// Left-to-right matching: horizontal LK from each primary point towards its epipolar candidates,
-// first success wins, every camera pair of a rig in one launch.
+// Left-to-right matching: LK (horizontal for rectified pairs, 2-D otherwise) from each primary point
+// towards its epipolar candidates, first success wins, every camera pair of a rig in one launch.
 //
 // The reference (MultiSOFGPU::LaunchTrackingPrimaryToSecondary, sof_multicamera_gpu.cpp:118-190)
 // runs rounds k = 0, 1, ...: round k tracks candidate k of every point that has no success yet and
@@ -112,7 +112,7 @@ __device__ __forceinline__ int pair_of(const StereoLaunch& p, int g) {
   return lo;
 }
 
-template <int SAMPLING>
+template <int SAMPLING, bool HORIZ>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) stereo_kernel(const __grid_constant__ StereoLaunch p) {
   __shared__ WarpSmem smem[kWarps];
   __shared__ fe_track_data tds[kWarps];
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) stereo_kernel(const _
       reinterpret_cast<uint32_t*>(&td)[lane] = w;
     }
     __syncwarp();
-    track_one<SAMPLING, true, kModeRef>(P.lk, td, smem[wid], lane, 0, 0.f);
+    track_one<SAMPLING, HORIZ, kModeRef>(P.lk, td, smem[wid], lane, 0, 0.f);
     __syncwarp();
     const bool ok = td.track_status != 0;
     unsigned old = kNone;
@@ -248,28 +248,33 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) stereo_kernel(const _
   }
 }
 
-template <int SAMPLING>
+template <int SAMPLING, bool HORIZ>
 cudaError_t launch_sampling(const StereoLaunch& p, cudaStream_t s) {
   static int resident = 0;
   if (!resident) {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stereo_kernel<SAMPLING>, kWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stereo_kernel<SAMPLING, HORIZ>, kWarps * 32, 0);
     resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   const long long total = (long long)p.rounds * p.round;
   const int blocks = (int)max(1LL, min((long long)resident, (total + kWarps - 1) / kWarps));
-  stereo_kernel<SAMPLING><<<blocks, kWarps * 32, 0, s>>>(p);
+  stereo_kernel<SAMPLING, HORIZ><<<blocks, kWarps * 32, 0, s>>>(p);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_stereo(const StereoLaunch& p, cudaStream_t s) {
-  if (p.sampling == FE_SAMPLE_EXACT) return launch_sampling<FE_SAMPLE_EXACT>(p, s);
-  if (p.sampling == FE_SAMPLE_TEXTURE_WIDE) return launch_sampling<FE_SAMPLE_TEXTURE_WIDE>(p, s);
-  return launch_sampling<FE_SAMPLE_TEXTURE>(p, s);
+  if (p.horizontal) {
+    if (p.sampling == FE_SAMPLE_EXACT) return launch_sampling<FE_SAMPLE_EXACT, true>(p, s);
+    if (p.sampling == FE_SAMPLE_TEXTURE_WIDE) return launch_sampling<FE_SAMPLE_TEXTURE_WIDE, true>(p, s);
+    return launch_sampling<FE_SAMPLE_TEXTURE, true>(p, s);
+  }
+  if (p.sampling == FE_SAMPLE_EXACT) return launch_sampling<FE_SAMPLE_EXACT, false>(p, s);
+  if (p.sampling == FE_SAMPLE_TEXTURE_WIDE) return launch_sampling<FE_SAMPLE_TEXTURE_WIDE, false>(p, s);
+  return launch_sampling<FE_SAMPLE_TEXTURE, false>(p, s);
 }
 
 }  // namespace fe

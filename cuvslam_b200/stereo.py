@@ -156,10 +156,14 @@ class StereoPair:
 class StereoMatcher:
     """fe_track_stereo over a fixed set of camera pairs; owns the output buffers."""
 
-    def __init__(self, ctx, sampling=_lib.FE_SAMPLE_TEXTURE, early_exit_fraction=L2R_EARLY_EXIT_FRACTION):
+    def __init__(self, ctx, sampling=_lib.FE_SAMPLE_TEXTURE, early_exit_fraction=L2R_EARLY_EXIT_FRACTION,
+                 horizontal=True):
+        """horizontal: the 1-D tracker of rectified pairs (lr_tracker = LKHorizontal), else 2-D LK
+        (lr_tracker = LK, the reference's default)."""
         self.ctx = ctx
         self.sampling = int(sampling)
         self.frac = float(early_exit_fraction)
+        self.horizontal = bool(horizontal)
 
     def track_primary_to_secondary(self, pairs, outputs=None, stream=None):
         """Matches every pair in one launch.  Returns [(tracks (n, 80) uint8 TrackData records,
@@ -203,6 +207,7 @@ class StereoMatcher:
             d.winner = win.data_ptr()
             d.stats = st.data_ptr()
         _lib.check(self.ctx.lib.fe_track_stereo(self.ctx.handle, descs, len(pairs), ctypes.c_float(self.frac),
-                                                self.sampling, _stream_handle(stream)), "fe_track_stereo")
+                                                int(self.horizontal), self.sampling, _stream_handle(stream)),
+                   "fe_track_stereo")
         self._keep = keep  # inputs stay alive until the next call (the launch is asynchronous)
         return outputs

@@ -198,7 +198,7 @@ typedef struct {
 
 /* One primary -> secondary pair of a left-to-right match. */
 typedef struct {
-  const fe_pyramid* primary;   /* host descriptor: primary frame's image + grad_x pyramid */
+  const fe_pyramid* primary;   /* host descriptor: primary frame's image + gradient pyramid */
   const fe_pyramid* secondary; /* host descriptor: secondary frame's image pyramid */
   const float* uv;             /* device, n x 2: primary positions (base-level pixels) */
   const uint8_t* valid;        /* device, n, or NULL: 0 = the point has no candidates (the caller could
@@ -223,9 +223,11 @@ typedef struct {
                                   reference would run, attempts tracked here, flags */
 } fe_stereo_pair;
 
-/* Left-to-right matching of npairs (<= 16) camera pairs in ONE launch: for each primary point,
- * horizontal LK (lk_track_horizontal_kernel, lk_tracker.cu:381-665) from its position in the
- * primary frame towards each of its candidates in turn, the first candidate that tracks wins.
+/* Left-to-right matching of npairs (<= 16) camera pairs in ONE launch: for each primary point, LK
+ * from its position in the primary frame towards each of its candidates in turn, the first
+ * candidate that tracks wins.  horizontal != 0: the 1-D tracker of rectified pairs
+ * (lk_track_horizontal_kernel, lk_tracker.cu:381-665; lr_tracker = LKHorizontal); 0: the 2-D
+ * tracker (lk_track_kernel, the default lr_tracker = LK; the primary pyramid needs grad_y).
  * Results equal MultiSOFGPU::LaunchTrackingPrimaryToSecondary (sof_multicamera_gpu.cpp:69-190),
  * which launches one tracking pass per candidate index k and synchronises after each, including
  * its early exit: after round k it stops once at least early_exit_fraction (kL2REarlyExitFraction
@@ -238,7 +240,7 @@ typedef struct {
  * make the first call at the largest size before capturing a graph.  One call at a time per
  * context.  sampling as in fe_track. */
 FE_API int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, float early_exit_fraction,
-                           int sampling, fe_stream stream);
+                           int horizontal, int sampling, fe_stream stream);
 
 /* ---------------------------------------------------------------------------------------- */
 /* Batched multi-camera frame step                                                           */

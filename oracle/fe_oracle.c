@@ -722,14 +722,16 @@ static void stereo_record(or_track_data* t, float x, float y, float radius, floa
   t->ncc_threshold = ncc_thr;
 }
 
-/* MultiSOFGPU::LaunchTrackingPrimaryToSecondary (libs/sof/sof_multicamera_gpu.cpp:118-190): round k
+/* MultiSOFGPU::LaunchTrackingPrimaryToSecondary (libs/sof/sof_multicamera_gpu.cpp:118-190), with the
+ * horizontal (lr_tracker = LKHorizontal) or the 2-D tracker (LK): round k
  * tracks candidate k of every point without a match that has one (the reference's sentinel
  * entries, tracked with a zero offset and discarded, are left out); no round when none has; after
  * round k, stop once matched >= early_exit_fraction * n (kL2REarlyExitFraction). */
 void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const* prim_gx,
-                    const float* const* prim_img, const float* const* sec_img, const float* uv, const uint8_t* valid,
-                    int n, const int32_t* cand_off, const float* cand_xy, float search_radius, float ncc_threshold,
-                    float early_exit_fraction, int mode, or_track_data* out, int32_t* winner, int32_t* stats) {
+                    const float* const* prim_gy, const float* const* prim_img, const float* const* sec_img,
+                    const float* uv, const uint8_t* valid, int n, const int32_t* cand_off, const float* cand_xy,
+                    float search_radius, float ncc_threshold, float early_exit_fraction, int horizontal, int mode,
+                    or_track_data* out, int32_t* winner, int32_t* stats) {
   int max_candidates = 0;
   for (int i = 0; i < n; ++i) {
     const int len = (valid && !valid[i]) ? 0 : cand_off[i + 1] - cand_off[i];
@@ -752,7 +754,7 @@ void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const
       const float* c = cand_xy + 2 * ((size_t)cand_off[i] + k);
       t.offset[0] = c[0] - uv[2 * i];
       t.offset[1] = c[1] - uv[2 * i + 1];
-      lk_one(levels, ws, hs, prim_gx, prim_gx, prim_img, sec_img, &t, mode, 1);
+      lk_one(levels, ws, hs, prim_gx, horizontal ? prim_gx : prim_gy, prim_img, sec_img, &t, mode, horizontal);
       ++attempts;
       if (t.track_status) {
         out[i] = t;

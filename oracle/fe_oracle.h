@@ -70,15 +70,16 @@ void or_lk_track_f64(int levels, const int* ws, const int* hs, const float* cons
 int or_epipolar_candidates(int cw, int ch, float inv_scale, const int32_t* offsets, const float* xy, float u, float v,
                            float* out, int cap);
 /* Left-to-right candidate scan of one camera pair: MultiSOFGPU::LaunchTrackingPrimaryToSecondary
- * (libs/sof/sof_multicamera_gpu.cpp:118-190) with horizontal LK per round (or_lk_track_horizontal).
+ * (libs/sof/sof_multicamera_gpu.cpp:118-190) with horizontal (or 2-D) LK per round.
  * Candidates of point i: cand_xy[cand_off[i] .. cand_off[i+1]) (x, y pairs); valid may be NULL.
  * Writes out[n] (matched: the winning attempt's record; unmatched: track = uv or (0, 0) when not
  * valid, offset and info 0, status 0), winner[n] (-1 = none) and stats[4] = {matched, rounds run,
  * attempts, 0}. */
 void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const* prim_gx,
-                    const float* const* prim_img, const float* const* sec_img, const float* uv, const uint8_t* valid,
-                    int n, const int32_t* cand_off, const float* cand_xy, float search_radius, float ncc_threshold,
-                    float early_exit_fraction, int mode, or_track_data* out, int32_t* winner, int32_t* stats);
+                    const float* const* prim_gy, const float* const* prim_img, const float* const* sec_img,
+                    const float* uv, const uint8_t* valid, int n, const int32_t* cand_off, const float* cand_xy,
+                    float search_radius, float ncc_threshold, float early_exit_fraction, int horizontal, int mode,
+                    or_track_data* out, int32_t* winner, int32_t* stats);
 
 /* FP64 differentiable LK tracker and its adjoint (lk_adjoint64.c). */
 enum { OR64_IMPLICIT = 0, OR64_UNROLLED = 1 };

@@ -48,7 +48,7 @@ def lib():
         L.or_lk_track_f64.argtypes = [I, P, P, P, P, P, P, P, I]
         L.or_epipolar_candidates.argtypes = [I, I, F, P, P, F, F, P, I]
         L.or_epipolar_candidates.restype = I
-        L.or_stereo_scan.argtypes = [I, P, P, P, P, P, P, P, I, P, P, F, F, F, I, P, P, P]
+        L.or_stereo_scan.argtypes = [I, P, P, P, P, P, P, P, P, I, P, P, F, F, F, I, I, P, P, P]
         for name, args, res in _CPU_SIGS:
             fn = getattr(L, name, None)
             if fn is None:
@@ -218,7 +218,7 @@ def epipolar_candidates(cw, ch, inv_scale, offsets, xy, uv, valid=None):
 
 
 def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_radius=48.0, ncc_threshold=0.8,
-                early_exit_fraction=0.8, mode=TEXTURE):
+                early_exit_fraction=0.8, mode=TEXTURE, horizontal=True):
     """The reference's left-to-right candidate scan (or_stereo_scan) on host pyramids [(img, gx, gy)]
     per level.  Returns (TRACK_DTYPE records, winner int32, stats int32[4])."""
     from cuvslam_b200.types import TRACK_DTYPE
@@ -229,6 +229,7 @@ def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_rad
     ws = np.array([p[0].shape[1] for p in prim_pyr] + [0] * (10 - levels), np.int32)
     hs = np.array([p[0].shape[0] for p in prim_pyr] + [0] * (10 - levels), np.int32)
     keep1, pgx = _level_ptrs([p[1] for p in prim_pyr])
+    keep4, pgy = _level_ptrs([p[2] for p in prim_pyr])
     keep2, pim = _level_ptrs([p[0] for p in prim_pyr])
     keep3, sim = _level_ptrs([p[0] for p in sec_pyr[:levels]])
     cand_off = np.ascontiguousarray(cand_off, np.int32)
@@ -242,10 +243,10 @@ def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_rad
     out = np.zeros(max(n, 1), TRACK_DTYPE)
     win = np.zeros(max(n, 1), np.int32)
     stats = np.zeros(4, np.int32)
-    L.or_stereo_scan(levels, _p(ws), _p(hs), pgx, pim, sim, _p(uv), vp, n, _p(cand_off), _p(cand_xy),
-                     float(search_radius), float(ncc_threshold), float(early_exit_fraction), mode, _p(out), _p(win),
-                     _p(stats))
-    del keep1, keep2, keep3
+    L.or_stereo_scan(levels, _p(ws), _p(hs), pgx, pgy, pim, sim, _p(uv), vp, n, _p(cand_off), _p(cand_xy),
+                     float(search_radius), float(ncc_threshold), float(early_exit_fraction), int(bool(horizontal)),
+                     mode, _p(out), _p(win), _p(stats))
+    del keep1, keep2, keep3, keep4
     return out[:n], win[:n], stats
 
 

@@ -337,13 +337,13 @@ int ref_lk(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int ma
 }
 
 // MultiSOFGPU::LaunchTrackingPrimaryToSecondary's scan between the pyramids of a primary and a
-// secondary u8 image: one lk_track_horizontal launch per candidate index k over all n points, a copy
+// secondary u8 image: one lk_track_horizontal (or lk_track) launch per candidate index k over all n points, a copy
 // back and a synchronisation, first success wins, early exit once matched >= frac * n.  Candidates
 // of point i: cand_xy[cand_off[i] .. cand_off[i+1]); valid may be null.  out: n TrackData records as
 // the reference publishes them; winner[i]: winning candidate or -1; stats: matched, rounds launched.
 int ref_stereo_scan(const uint8_t* prim_img, const uint8_t* sec_img, int w, int h, int max_levels, const float* uv,
                     const uint8_t* valid, int n, const int* cand_off, const float* cand_xy, float radius,
-                    float ncc_thr, float frac, void* out, int* winner, int* stats) {
+                    float ncc_thr, float frac, int horizontal, void* out, int* winner, int* stats) {
   int rc = init_tables();
   if (rc) return rc;
   Pyr pp, sp;
@@ -362,7 +362,7 @@ int ref_stereo_scan(const uint8_t* prim_img, const uint8_t* sec_img, int w, int 
   }
   TrackData* d = nullptr;
   HCHECK(cudaMalloc((void**)&d, sizeof(TrackData) * data.size()));
-  Pyramid gx = make_pyr(pp, pp.gx), pi = make_pyr(pp, pp.img), si = make_pyr(sp, sp.img);
+  Pyramid gx = make_pyr(pp, pp.gx), gy = make_pyr(pp, pp.gy), pi = make_pyr(pp, pp.img), si = make_pyr(sp, sp.img);
   auto uv_of = [&](int i, int c) { return (valid && !valid[i]) ? 0.f : uv[2 * i + c]; };
   int tracked = 0, rounds = 0;
   for (int k = 0; k < max_candidates; ++k) {
@@ -384,7 +384,10 @@ int ref_stereo_scan(const uint8_t* prim_img, const uint8_t* sec_img, int w, int 
     }
     if (!any_active) break;
     HCHECK(cudaMemcpy(d, data.data(), sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
-    HCHECK(lk_track_horizontal(gx, pi, si, d, n, 0));
+    if (horizontal)
+      HCHECK(lk_track_horizontal(gx, pi, si, d, n, 0));
+    else
+      HCHECK(lk_track(gx, gy, pi, si, d, n, 0));
     HCHECK(cudaMemcpy(data.data(), d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToHost));
     HCHECK(cudaDeviceSynchronize());
     rounds = k + 1;

@@ -200,11 +200,13 @@ def make_reference(out_dir):
 # pyramids (top level 3), primary points, and two candidate sets: the epipolar table of a pinhole
 # pair (fx 458, baseline 0.11 m) and random lists of 0-12 candidates left of each point.
 STEREO_LEVELS = 4
-STEREO_RUNS = {  # name -> (candidate set, early-exit fraction)
-    "curves": ("curves", 0.8),
-    "random": ("random", 0.8),
-    "random_full": ("random", 1.0),
-    "random_low": ("random", 0.3),
+STEREO_RUNS = {  # name -> (candidate set, early-exit fraction, horizontal tracker)
+    "curves": ("curves", 0.8, True),
+    "random": ("random", 0.8, True),
+    "random_full": ("random", 1.0, True),
+    "random_low": ("random", 0.3, True),
+    "curves_2d": ("curves", 0.8, False),
+    "random_2d": ("random", 0.3, False),
 }
 
 
@@ -242,7 +244,7 @@ def make_stereo_inputs(path):
 def make_stereo_reference(out_dir):
     lib = _lib()
     P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
-    lib.ref_stereo_scan.argtypes = [P, P, I, I, I, P, P, I, P, P, F, F, F, P, P, P]
+    lib.ref_stereo_scan.argtypes = [P, P, I, I, I, P, P, I, P, P, F, F, F, I, P, P, P]
     inp = np.load(os.path.join(HERE, "stereo_inputs.npz"))
     left = np.ascontiguousarray(np.load(os.path.join(HERE, "inputs.npz"))["c1/prev"])
     right = np.ascontiguousarray(inp["right"])
@@ -252,14 +254,14 @@ def make_stereo_reference(out_dir):
     n = len(uv)
     radius = 3.0 * float(1 << (int(inp["top"]) + 1))
     compact = {}
-    for run, (cset, frac) in STEREO_RUNS.items():
+    for run, (cset, frac, horizontal) in STEREO_RUNS.items():
         off = np.ascontiguousarray(inp[f"{cset}_cand_off"], np.int32)
         xy = np.ascontiguousarray(inp[f"{cset}_cand_xy"], np.float32)
         out = np.zeros(n, TRACK_DTYPE)
         win = np.zeros(n, np.int32)
         stats = np.zeros(2, np.int32)
         rc = lib.ref_stereo_scan(_ptr(left), _ptr(right), w, h, STEREO_LEVELS, _ptr(uv), _ptr(valid), n, _ptr(off),
-                                 _ptr(xy), radius, 0.8, frac, _ptr(out), _ptr(win), _ptr(stats))
+                                 _ptr(xy), radius, 0.8, frac, int(horizontal), _ptr(out), _ptr(win), _ptr(stats))
         assert rc == 0, rc
         compact[f"{run}/out"] = out
         compact[f"{run}/winner"] = win

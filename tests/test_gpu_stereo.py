@@ -2,6 +2,7 @@
 launch, bit-identical to the oracle's restatement of the reference's multi-launch scan, and
 within 0.01 px median / 0.05 px p99 of the reference's own kernels run in that scan."""
 
+import ctypes
 import os
 
 import numpy as np
@@ -17,8 +18,8 @@ pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(ROOT, "tests", "golden")
 LEVELS = 4
-RUNS = {"curves": ("curves", 0.8), "random": ("random", 0.8), "random_full": ("random", 1.0),
-        "random_low": ("random", 0.3)}
+RUNS = {"curves": ("curves", 0.8, True), "random": ("random", 0.8, True), "random_full": ("random", 1.0, True),
+        "random_low": ("random", 0.3, True), "curves_2d": ("curves", 0.8, False), "random_2d": ("random", 0.3, False)}
 
 
 @pytest.fixture(scope="module")
@@ -45,27 +46,27 @@ def _explicit_pair(pp, sp, inp, cset, uv=None, valid="fixture"):
                       valid=torch.from_numpy(inp["valid"]).cuda() if isinstance(valid, str) else valid)
 
 
-def _oracle_run(oracle, opp, osp, inp, cset, frac, radius):
+def _oracle_run(oracle, opp, osp, inp, cset, frac, radius, horizontal=True, mode=0):
     return oracle.stereo_scan(opp, osp, inp["uv"], inp[f"{cset}_cand_off"], inp[f"{cset}_cand_xy"], inp["valid"],
-                              radius, 0.8, frac)
+                              radius, 0.8, frac, mode=mode, horizontal=horizontal)
 
 
 @pytest.mark.parametrize("run", list(RUNS))
 def test_matches_oracle_and_reference(ctx, oracle, stereo_case, run):
     inp, pp, sp, opp, osp = stereo_case
-    cset, frac = RUNS[run]
+    cset, frac, horizontal = RUNS[run]
     radius = cross_cam_search_radius(pp.levels - 1)
-    (out, win, st), = StereoMatcher(ctx, early_exit_fraction=frac).track_primary_to_secondary(
+    (out, win, st), = StereoMatcher(ctx, early_exit_fraction=frac, horizontal=horizontal).track_primary_to_secondary(
         [_explicit_pair(pp, sp, inp, cset)])
     torch.cuda.synchronize()
     got, gwin, gst = _records(out), win.cpu().numpy(), st.cpu().numpy()
-    want, wwin, wst = _oracle_run(oracle, opp, osp, inp, cset, frac, radius)
+    want, wwin, wst = _oracle_run(oracle, opp, osp, inp, cset, frac, radius, horizontal)
     assert_tracks_equal(got, want)
     np.testing.assert_array_equal(gwin, wwin)
     np.testing.assert_array_equal(gst[:2], wst[:2])
     assert gst[2] >= wst[2]  # attempts: the reference's, plus speculative ones whose point won earlier
     path = os.path.join(GOLD, "stereo_reference.npz")
-    if os.path.exists(path):
+    if os.path.exists(path) and f"{run}/winner" in np.load(path):
         # the reference's texture unit rounds its 4-tap sums differently from the FP32 emulation, so a
         # marginal attempt (NCC or step right at its threshold) may decide the other way
         ref = np.load(path)
@@ -84,17 +85,16 @@ def test_wide_sampling_follows_the_reference(ctx, oracle, stereo_case, run):
     winners, statuses and counts equal the reference scan, positions within 1e-3 px; bit-identical
     to the oracle in the same mode."""
     path = os.path.join(GOLD, "stereo_reference.npz")
-    if not os.path.exists(path):
-        pytest.skip("stereo_reference.npz not generated")
+    if not os.path.exists(path) or f"{run}/winner" not in np.load(path):
+        pytest.skip("stereo_reference.npz has no such run")
     inp, pp, sp, opp, osp = stereo_case
-    cset, frac = RUNS[run]
-    (out, win, st), = StereoMatcher(ctx, sampling=_lib.FE_SAMPLE_TEXTURE_WIDE, early_exit_fraction=frac) \
-        .track_primary_to_secondary([_explicit_pair(pp, sp, inp, cset)])
+    cset, frac, horizontal = RUNS[run]
+    (out, win, st), = StereoMatcher(ctx, sampling=_lib.FE_SAMPLE_TEXTURE_WIDE, early_exit_fraction=frac,
+                                    horizontal=horizontal).track_primary_to_secondary([_explicit_pair(pp, sp, inp, cset)])
     torch.cuda.synchronize()
     got, gwin, gst = _records(out), win.cpu().numpy(), st.cpu().numpy()
     radius = cross_cam_search_radius(pp.levels - 1)
-    want, wwin, wst = oracle.stereo_scan(opp, osp, inp["uv"], inp[f"{cset}_cand_off"], inp[f"{cset}_cand_xy"],
-                                         inp["valid"], radius, 0.8, frac, mode=oracle.TEXTURE_WIDE)
+    want, wwin, wst = _oracle_run(oracle, opp, osp, inp, cset, frac, radius, horizontal, oracle.TEXTURE_WIDE)
     assert_tracks_equal(got, want)
     np.testing.assert_array_equal(gwin, wwin)
     ref = np.load(path)
@@ -219,6 +219,11 @@ def test_bad_arguments(ctx, stereo_case):
     inp, pp, sp, opp, osp = stereo_case
     lib = ctx.lib
     pairs = (_lib.FeStereoPair * 1)()
-    assert lib.fe_track_stereo(ctx.handle, pairs, 0, 0.8, 0, None) == 1
-    assert lib.fe_track_stereo(ctx.handle, pairs, 17, 0.8, 0, None) == 4
-    assert lib.fe_track_stereo(ctx.handle, pairs, 1, 0.8, 0, None) == 1  # no pyramids
+    assert lib.fe_track_stereo(ctx.handle, pairs, 0, 0.8, 1, 0, None) == 1
+    assert lib.fe_track_stereo(ctx.handle, pairs, 17, 0.8, 1, 0, None) == 4
+    assert lib.fe_track_stereo(ctx.handle, pairs, 1, 0.8, 1, 0, None) == 1  # no pyramids
+    d = (_lib.FeStereoPair * 1)()
+    d[0].primary = ctypes.pointer(pp.desc)
+    d[0].secondary = ctypes.pointer(sp.desc)
+    assert lib.fe_track_stereo(ctx.handle, d, 1, 0.8, 1, 3, None) == 1  # bad sampling mode
+    assert lib.fe_track_stereo(ctx.handle, d, 1, float("nan"), 1, 0, None) == 1
