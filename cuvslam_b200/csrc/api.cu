@@ -84,6 +84,38 @@ fe::Pyr to_pyr(const fe_pyramid& p) {
 }
 
 // ------------------------------------------------------------------ pyramid planning
+// The deeper-level items of a levels 0-2 job (levels 3 .. of `pyr`): the rest item starts at the
+// first level r (level 3, 4 or 5) from which every remaining level fits in the kernel's shared
+// memory together; each level before it is a banded phase (its gradients and the next level's
+// image, a band of rows per item).  False when no such split exists (the job then keeps the
+// generic stages).
+bool plan_deep_items(const fe::Pyr& pyr, fe::StageJob& job) {
+  const int n = pyr.levels - 3, cap = fe::l012_deep_floats();
+  if (n <= 0) return false;
+  int r = -1;
+  for (int k = 0; k < std::min(n, 3) && r < 0; ++k) {
+    int64_t need = (int64_t)((pyr.lv[3 + k].w + 3) & ~3) * pyr.lv[3 + k].h;
+    for (int m = k + 1; m < n; ++m) need += (int64_t)pyr.lv[3 + m].w * pyr.lv[3 + m].h;
+    if (need <= cap) r = k;
+  }
+  if (r < 0) return false;
+  job.deep_rest = r;
+  job.deep_bands[0] = job.deep_bands[1] = 0;
+  job.deep_band_rows[0] = job.deep_band_rows[1] = 0;
+  job.deep_items = 1;
+  for (int p = 0; p < r; ++p) {
+    const int ws = (pyr.lv[3 + p].w + 3) & ~3;
+    const int rows = (cap / ws - 6) / 2;  // level 3+p+1 rows per band: 2 rows + 6 halo rows staged each
+    if (rows < 1) return false;
+    job.deep_band_rows[p] = rows;
+    job.deep_bands[p] = (pyr.lv[4 + p].h + rows - 1) / rows;
+    job.deep_items += job.deep_bands[p];
+  }
+  job.tail_levels = n;
+  for (int k = 0; k < n; ++k) job.tail[k] = pyr.lv[3 + k];
+  return true;
+}
+
 // Launches of one stage index that share the source kind and the number of produced levels.
 struct StageGroup {
   bool u8;
@@ -125,7 +157,11 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.tiles_y = (deep.h + T - 1) / T;
     if (kind_u8 && nl == 2) fe::encode_frame_tmap(job);
     const int rem = pyr.levels - 1 - (s + std::max(nl, 0));
-    if (!(kind_u8 && nl == 2) && nl > 0 && rem > 0 && rem <= 2 && counters && *ncounters < counter_cap) {
+    if (kind_u8 && nl == 2 && rem > 0 && counters && *ncounters + 4 <= counter_cap && plan_deep_items(pyr, job)) {
+      // the levels 0-2 launch also computes every deeper level (work items after the tiles)
+      job.done = counters + *ncounters;
+      *ncounters += 4;
+    } else if (!(kind_u8 && nl == 2) && nl > 0 && rem > 0 && rem <= 2 && counters && *ncounters < counter_cap) {
       const fe::Level& deepest = pyr.lv[s + nl];
       const fe::Level& next = pyr.lv[s + nl + 1];
       if ((int64_t)deepest.w * deepest.h + (int64_t)next.w * next.h <= fe::kTailFloats) {
@@ -138,7 +174,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     StageGroup* g = nullptr;
     const bool has_tail = job.tail_levels > 0;
     for (auto& gg : plan[stage])
-      if (gg.u8 == kind_u8 && gg.nl == nl && gg.tail == has_tail) g = &gg;
+      if (gg.u8 == kind_u8 && gg.nl == nl && gg.tail == has_tail && gg.batch.njobs < fe::kMaxStageJobs) g = &gg;
     if (!g) {
       plan[stage].emplace_back();
       g = &plan[stage].back();
@@ -149,7 +185,6 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
       g->kt = kt;
       g->tiles = 0;
     }
-    if (g->batch.njobs >= fe::kMaxCams) return FE_ERR_CAPACITY;
     job.tile_begin = g->tiles;
     g->batch.job[g->batch.njobs++] = job;
     g->tiles += job.tiles_x * job.tiles_y;
@@ -163,6 +198,38 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
 int run_stages(const StagePlan& plan, size_t first, size_t last, cudaStream_t st) {
   for (size_t k = first; k < std::min(last, plan.size()); ++k)
     for (const auto& g : plan[k]) FE_CUDA(fe::launch_pyramid_stage(g.batch, g.tiles, g.u8, g.nl, g.kt, g.tail, st));
+  return FE_OK;
+}
+
+// Lays out the work queue of each levels 0-2 launch whose jobs compute their deeper levels: jobs by
+// frame size, largest first (their deeper levels are the most work), each job's tiles, and each
+// job's deeper-level items after the next job's tiles (by then its tiles are usually done).
+// `queues`: two zeroed ints per such launch (*nqueues used so far of queue_cap).
+int finish_l012_plan(StagePlan& plan, int* queues, int* nqueues, int queue_cap) {
+  if (plan.empty()) return FE_OK;
+  for (auto& g : plan[0]) {
+    if (!(g.u8 && g.nl == 2 && g.tail)) continue;
+    fe::StageJob* J = g.batch.job;
+    const int n = g.batch.njobs;
+    std::stable_sort(J, J + n, [](const fe::StageJob& a, const fe::StageJob& b) {
+      return (int64_t)a.src_w * a.src_h > (int64_t)b.src_w * b.src_h;
+    });
+    int q = 0;
+    for (int i = 0; i < n; ++i) {
+      J[i].tile_begin = q;
+      q += J[i].tiles_x * J[i].tiles_y;
+      if (i > 0) {
+        J[i - 1].q_deep = q;
+        q += J[i - 1].deep_items;
+      }
+    }
+    J[n - 1].q_deep = q;
+    q += J[n - 1].deep_items;
+    if (*nqueues + 2 > queue_cap) return FE_ERR_CAPACITY;
+    g.batch.queue = queues + *nqueues;
+    *nqueues += 2;
+    g.tiles = q;
+  }
   return FE_OK;
 }
 
@@ -196,6 +263,9 @@ struct fe_context {
   int device = 0;
   SelectScratch sel;
   int* lk_counter = nullptr;  // persistent LK warps' track counter
+  int* stage_done = nullptr;  // fe_build_pyramid's CTA counters (the levels 0-2 kernel's last CTA per
+                              // frame computes the deeper levels): 64, used in turn
+  unsigned stage_slot = 0;
   void* stereo_mem = nullptr;  // left-to-right matching scratch (grown on demand)
   size_t stereo_bytes = 0;
   bool debug = false;
@@ -338,7 +408,11 @@ int fe_create(int device, fe_context** out) {
   c->device = device;
   c->debug = getenv("CUVSLAM_FE_DEBUG_MAPS") != nullptr;
   cudaError_t e = cudaMalloc((void**)&c->lk_counter, 256);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->stage_done, 64 * 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->stage_done, 0, 64 * 8 * sizeof(int));
   if (e != cudaSuccess) {
+    if (c->lk_counter) cudaFree(c->lk_counter);
+    if (c->stage_done) cudaFree(c->stage_done);
     delete c;
     return cuda_fail(e);
   }
@@ -350,6 +424,7 @@ int fe_destroy(fe_context* ctx) {
   if (!ctx) return FE_ERR_INVALID_ARGUMENT;
   if (ctx->sel.mem) cudaFree(ctx->sel.mem);
   if (ctx->lk_counter) cudaFree(ctx->lk_counter);
+  if (ctx->stage_done) cudaFree(ctx->stage_done);
   if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
   if (ctx->sel.resp) cudaFree(ctx->sel.resp);
   if (ctx->sel.nms) cudaFree(ctx->sel.nms);
@@ -399,7 +474,11 @@ int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_
   if (pyr->width[0] != width || pyr->height[0] != height || image_pitch_bytes < width) return FE_ERR_INVALID_ARGUMENT;
   if (!pyr->grad_y[0]) return FE_ERR_INVALID_ARGUMENT;
   StagePlan plan;
-  int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan);
+  // one of the context's 64 counter sets per call, in turn (at most 64 builds in flight per context)
+  int used = 0, nq = 0;
+  int* done = ctx->stage_done + 8 * (ctx->stage_slot++ & 63);
+  int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan, 1.f, 8, done, &used, 4);
+  if (!rc) rc = finish_l012_plan(plan, done + 4, &nq, 2);
   if (rc) return rc;
   return run_plan(plan, (cudaStream_t)stream);
 }
@@ -630,7 +709,7 @@ struct fe_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   // shapes chosen by fe_batch_autotune (defaults until it runs)
-  int* stage_done = nullptr;  // pyramid-stage tail counters, two per camera
+  int* stage_done = nullptr;  // pyramid counters: four per camera, then the levels 0-2 launches' queues
   int lk_shape = 0;      // LK block shape (fe::kLkShapes)
   int overlap = 1;       // response tiles on a second stream beside LK
   int stage_tile = 8;    // deepest-level tile of the generic pyramid stages
@@ -696,9 +775,12 @@ int replan_pyramids(fe_batch* b, int kt) {
   int used = 0;
   for (int i = 0; i < b->ncams; ++i) {
     int rc = plan_pyramid(b->cams[i].image, b->cams[i].image_pitch_bytes, true, b->cur[i], plan, 1.f, kt,
-                          b->stage_done, &used, 2 * b->ncams);
+                          b->stage_done, &used, 4 * b->ncams);
     if (rc) return rc;
   }
+  int nq = 0;
+  int rc = finish_l012_plan(plan, b->stage_done + 4 * b->ncams, &nq, 8);
+  if (rc) return rc;
   b->plan = std::move(plan);
   b->stage_tile = kt;
   return FE_OK;
@@ -979,8 +1061,8 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(cuda_fail(e));
   // pyramid stages with tails: the deep levels' counters, then the final plan
-  e = cudaMalloc((void**)&b->stage_done, sizeof(int) * 2 * ncams);
-  if (e == cudaSuccess) e = cudaMemset(b->stage_done, 0, sizeof(int) * 2 * ncams);
+  e = cudaMalloc((void**)&b->stage_done, sizeof(int) * (4 * ncams + 8));
+  if (e == cudaSuccess) e = cudaMemset(b->stage_done, 0, sizeof(int) * (4 * ncams + 8));
   if (e != cudaSuccess) return fail(cuda_fail(e));
   int rc = replan_pyramids(b, b->stage_tile);
   if (!rc) rc = capture_batch(b);

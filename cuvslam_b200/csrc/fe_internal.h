@@ -19,25 +19,39 @@ struct alignas(64) StageJob {
   int use_tma;              // frame meets TMA alignment (16-byte base and pitch)
   float scale;              // factor on the staged source (FP32 first stage; 1 otherwise)
   int tiles_x, tiles_y;
-  int tile_begin;           // first CTA of this job in the launch
+  int tile_begin;           // first CTA (queue position, when the launch has a queue) of this job's tiles
   Level out[3];             // out[k] = level s + k; out[0] describes level s
-  // the levels after out[nl], computed by the job's last CTA from the complete out[nl] (0-2 of them)
+  // the levels after out[nl], computed by the job's last CTA from the complete out[nl]: at most two
+  // small ones after a generic stage, all the remaining ones after the levels 0-2 kernel
   int tail_levels;
-  int* done;                // the job's CTA counter (zero between launches; the last CTA resets it)
-  Level tail[2];
+  int* done;                // the job's CTA counter (zero between launches; the last CTA resets it);
+                            // levels 0-2 kernel: [0] tiles, [1] phase-3 bands, [2] phase-4 bands
+  // levels 0-2 kernel: queue positions [q_deep, q_deep + deep_items) hold this job's deeper-level
+  // items: deep_bands[p] band items of phase p (deep_band_rows[p] rows of tail[p + 1] each), then the
+  // rest item from tail[deep_rest]
+  int q_deep, deep_items, deep_rest;
+  int deep_bands[2], deep_band_rows[2];
+  Level tail[kMaxLevels - 3];
 };
+
+constexpr int kMaxStageJobs = 48;  // jobs per launch (the job table is a kernel parameter)
 
 struct StageBatch {
   int njobs;
-  int* status;              // device flags: bit 0 = a TMA wait ran out (tile skipped)
-  StageJob job[kMaxCams];
+  int* status;              // device flags: bit 0 = a TMA wait ran out (tile skipped), bit 1 = a
+                            // deeper-level item's wait ran out (item skipped)
+  int* queue;               // levels 0-2 kernel with deeper-level items: [0] next item, [1] CTAs
+                            // finished (zero between launches), or nullptr: item = blockIdx.x
+  StageJob job[kMaxStageJobs];
 };
+static_assert(sizeof(StageBatch) <= 32000, "stage job table exceeds the kernel parameter limit");
 
 // kt: the generic stages' deepest-level tile (8 or 16), plus kL012Three to run the levels 0-2 kernel
 // with registers for three CTAs per SM instead of two
 constexpr int kL012Three = 64;
 int stage_tile(bool u8, int nl, int kt);  // deepest-level core tile edge of a stage kind
 constexpr int kTailFloats = 12 * 1024;  // shared-memory floats for a tail: the source level + one level
+int l012_deep_floats();  // shared-memory floats a deeper-level item of the levels 0-2 kernel stages
 // Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
 // TMA alignment (the stage then stages its tile with ordinary loads).
 bool encode_frame_tmap(StageJob& job);

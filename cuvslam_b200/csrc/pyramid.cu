@@ -312,23 +312,155 @@ __device__ float corner_l1(const uint8_t* B0, int a0x, int a0y, int w0, int h0, 
   return (float)acc * (1.f / 256.f);
 }
 
-// MINB: CTAs resident per SM the registers are budgeted for (2, or 3 with fewer registers).
-template <int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __grid_constant__ StageBatch batch) {
-  extern __shared__ __align__(128) unsigned char sm[];
+// Deeper levels (3 and below) inside the same launch.  Every tile CTA also writes its 16x16 core of
+// level 3's image (its sources lie in the tile's level-2 region).  The launch's CTAs take work items
+// from an atomic queue: each camera's tiles, then (placed after the next camera's tiles, so that
+// their inputs are usually complete when they are taken) its deeper-level items:
+//   band items of phase d (d = level 3, then level 4 when needed): level d's gradients and level
+//     d+1's image for a band of rows, from level d's rows staged in shared memory;
+//   one rest item: the remaining levels from the first one that fits in shared memory, staged once,
+//     each further level computed there.
+// An item waits (bounded) until the items it reads from are counted complete: tiles for phase 3,
+// phase-3 bands for phase 4, the last banded phase (or the tiles) for the rest.  Items are taken in
+// queue order and only wait on earlier items, which are running or done, so the waits end.  Pixels
+// follow the reference's rules (25-tap decimation with mirror and corner skip, 7-tap derivatives),
+// so every level is bit-identical to the reference's.
+constexpr int kDeepFloats = (kOffBar / 4) & ~3;
+
+// Rows [lo, lo + rows) of level L into sm (row stride `stride` floats, a multiple of 4), through L2.
+__device__ __forceinline__ void stage_rows(const Level& L, int lo, int rows, int stride, float* sm) {
+  const int q4 = L.w >> 2, rem = L.w & 3;
+  for (int i = threadIdx.x; i < rows * q4; i += kThreads) {
+    const int r = i / q4, c = (i - r * q4) * 4;
+    const float* g = L.img + (size_t)(lo + r) * L.pitch + c;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sm + r * stride + c)), "l"(g) : "memory");
+  }
+  if (rem)
+    for (int i = threadIdx.x; i < rows * rem; i += kThreads) {
+      const int r = i / rem, c = (q4 << 2) + (i - r * rem);
+      sm[r * stride + c] = __ldcg(L.img + (size_t)(lo + r) * L.pitch + c);
+    }
+  cp_async_wait_all();
+  __syncthreads();
+}
+
+// Gradients of rows [y0, y1) of level D whose image rows [lo, ...) are in sm (row stride `stride`).
+__device__ __forceinline__ void smem_gradients(const Level& D, const float* a, int stride, int lo, int y0, int y1) {
+  const int w = D.w, h = D.h;
+  for (int i = threadIdx.x; i < (y1 - y0) * w; i += kThreads) {
+    const int y = y0 + i / w, x = i - (i / w) * w;
+    const float* p = a + (y - lo) * stride + x;
+    float gx = 0.f, gy = 0.f;
+    if (x > 2 && x < w - 3) {
+#pragma unroll
+      for (int j = 0; j < 7; ++j)
+        if (j != 3) gx = __fmaf_rn(dsp_tap(j), p[j - 3], gx);
+    }
+    if (y > 2 && y < h - 3) {
+#pragma unroll
+      for (int j = 0; j < 7; ++j)
+        if (j != 3) gy = __fmaf_rn(dsp_tap(j), p[(j - 3) * stride], gy);
+    }
+    D.gx[(size_t)y * D.pitch + x] = gx;
+    if (D.gy) D.gy[(size_t)y * D.pitch + x] = gy;
+  }
+}
+
+// Band item: level S's gradients on rows [2 r0, 2 r1) and level N's image on rows [r0, r1).
+__device__ void band_item(const Level& S, const Level& N, int r0, int nrows, float* sm) {
+  const int r1 = min(N.h, r0 + nrows);
+  const int ss = (S.w + 3) & ~3;
+  const int lo = max(0, 2 * r0 - 3), hi = min(S.h - 1, 2 * r1 + 2);
+  stage_rows(S, lo, hi - lo + 1, ss, sm);
+  smem_gradients(S, sm, ss, lo, min(S.h, 2 * r0), min(S.h, 2 * r1));
+  for (int i = threadIdx.x; i < (r1 - r0) * N.w; i += kThreads) {
+    const int y = r0 + i / N.w, x = i - (i / N.w) * N.w;
+    N.img[(size_t)y * N.pitch + x] = downscale_px(sm, ss, 0, lo, S.w, S.h, x, y);
+  }
+}
+
+// Rest item: levels tail[0..n): tail[0]'s image is complete; its gradients and every further level.
+__device__ void rest_item(const Level* tail, int n, float* sm) {
+  const int s0 = (tail[0].w + 3) & ~3;
+  stage_rows(tail[0], 0, tail[0].h, s0, sm);
+  const float* a = sm;
+  int as = s0;
+  float* b = sm + s0 * tail[0].h;
+  for (int t = 0; t < n; ++t) {
+    const Level& D = tail[t];
+    if (t > 0) {
+      const Level& S = tail[t - 1];
+      for (int i = threadIdx.x; i < D.w * D.h; i += kThreads) {
+        const int y = i / D.w, x = i - y * D.w;
+        const float v = downscale_px(a, as, 0, 0, S.w, S.h, x, y);
+        b[i] = v;
+        D.img[(size_t)y * D.pitch + x] = v;
+      }
+      __syncthreads();
+      a = b;
+      as = D.w;
+      b += D.w * D.h;
+    }
+    smem_gradients(D, a, as, 0, 0, D.h);
+  }
+}
+
+// Thread 0 waits (bounded) until *ctr >= target; false (and status bit 1) when the wait ran out.
+__device__ bool wait_count(const StageBatch& batch, int* ctr, int target) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    int ok = 0;
+    for (int i = 0; i < (1 << 22); ++i) {
+      if (*reinterpret_cast<volatile int*>(ctr) >= target) {
+        ok = 1;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!ok && batch.status) atomicOr(batch.status, 2);
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Deeper-level item idx of job J.  J.done: [0] tiles finished, [1] phase-3 bands, [2] phase-4
+// bands; the rest item, the job's last, returns them to zero for the next launch.
+__device__ void deep_item(const StageBatch& batch, const StageJob& J, int idx, float* sm) {
+  int* ctr = J.done;
+  const int ntiles = J.tiles_x * J.tiles_y;
+  const int nb0 = J.deep_bands[0], nb1 = J.deep_bands[1];
+  if (idx < nb0 + nb1) {
+    const int ph = idx < nb0 ? 0 : 1, b = ph ? idx - nb0 : idx;
+    if (wait_count(batch, ph ? ctr + 1 : ctr, ph ? nb0 : ntiles))
+      band_item(J.tail[ph], J.tail[ph + 1], b * J.deep_band_rows[ph], J.deep_band_rows[ph], sm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(ctr + 1 + ph, 1);
+    }
+  } else {
+    const int r = J.deep_rest;
+    if (wait_count(batch, r == 0 ? ctr : ctr + r, r == 0 ? ntiles : J.deep_bands[r - 1]))
+      rest_item(J.tail + r, J.tail_levels - r, sm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ctr[0] = 0;
+      ctr[1] = 0;
+      ctr[2] = 0;
+    }
+  }
+}
+
+// Tile t of job: levels 0-2, and when the launch computes the deeper levels, level 3's image core
+// (after which the tile counts itself complete in job.done[0]).
+__device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJob& job, int t, unsigned char* sm) {
   uint8_t* B0 = sm;
   float* B1 = reinterpret_cast<float*>(sm + kOffB1);
   float* B2 = reinterpret_cast<float*>(sm + kOffB2);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kOffBar);
   const int tid = threadIdx.x;
-
-  int lo = 0, hi = batch.njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (batch.job[mid].tile_begin <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
-  }
-  const StageJob& job = batch.job[lo];
-  const int t = (int)blockIdx.x - job.tile_begin;
   const int X2 = (t % job.tiles_x) * kT2, Y2 = (t / job.tiles_x) * kT2;
   const Level& L0 = job.out[0];
   const Level& L1 = job.out[1];
@@ -359,6 +491,7 @@ __global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __gr
       if (tid == 0 && batch.status) atomicOr(batch.status, 1);
       // the copy may still land: wait once more (bounded) so no write targets a retired CTA
       mbar_wait(bar, 0);
+      if (job.tail_levels > 0 && tid == 0) atomicAdd(job.done, 1);  // still counted (its level 3 is not written)
       return;
     }
   } else {
@@ -449,6 +582,23 @@ __global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __gr
       B2[(y2 - a2y) * kS2S + (x2 - a2x)] = downscale_px(B1, kS1S, a1x, a1y, w1, h1, x2, y2);
   }
   __syncthreads();
+  // level 3's image on this tile's 16x16 core (its sources [X2-2, X2+34) lie in the level-2 region),
+  // when the job's last CTA computes the deeper levels
+  if (job.tail_levels > 0) {
+    if (tid < 256) {
+      const Level& L3 = job.tail[0];
+      const int x3 = (X2 >> 1) + (tid & 15), y3 = (Y2 >> 1) + (tid >> 4);
+      if (x3 < L3.w && y3 < L3.h)
+        L3.img[(size_t)y3 * L3.pitch + x3] = downscale_px(B2, kS2S, a2x, a2y, w2, h2, x3, y3);
+    }
+    // the deeper-level items read only level 3's image: count the tile now, while its level 0-2
+    // stores (issued below) are not yet outstanding, so the fence has only these writes to wait for
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(job.done, 1);
+    }
+  }
 
   // 4. core outputs, four pixels per thread and store
   // level 0: 128x128 from the uint8 tile.  Bytes become floats exactly as (2^23 + b) - 2^23 (a byte
@@ -568,6 +718,47 @@ __global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __gr
   }
 }
 
+// MINB: CTAs resident per SM the registers are budgeted for (2, or 3 with fewer registers).
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __grid_constant__ StageBatch batch) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ int s_q;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_q = batch.queue ? atomicAdd(batch.queue, 1) : (int)blockIdx.x;
+  __syncthreads();
+  const int q = s_q;
+  int j = 0, idx = 0;
+  bool deep = false;
+  for (; j < batch.njobs; ++j) {
+    const StageJob& J = batch.job[j];
+    if (q >= J.tile_begin && q < J.tile_begin + J.tiles_x * J.tiles_y) {
+      idx = q - J.tile_begin;
+      break;
+    }
+    if (J.tail_levels > 0 && q >= J.q_deep && q < J.q_deep + J.deep_items) {
+      idx = q - J.q_deep;
+      deep = true;
+      break;
+    }
+  }
+  if (j < batch.njobs) {
+    const StageJob& job = batch.job[j];
+    if (!deep) {
+      l012_tile(batch, job, idx, sm);
+    } else {
+      deep_item(batch, job, idx, reinterpret_cast<float*>(sm));
+    }
+  }
+  if (batch.queue) {
+    // the last CTA to finish returns the queue to zero for the next launch
+    __syncthreads();
+    if (tid == 0 && atomicAdd(batch.queue + 1, 1) == (int)gridDim.x - 1) {
+      batch.queue[0] = 0;
+      batch.queue[1] = 0;
+    }
+  }
+}
+
 }  // namespace l012
 
 constexpr size_t stage_smem(int kt, int nl, bool tail = true) {
@@ -601,6 +792,8 @@ cudaError_t set_stage_attrs() {
 }
 
 }  // namespace
+
+int l012_deep_floats() { return l012::kDeepFloats; }
 
 int stage_tile(bool u8, int nl, int kt) { return (u8 && nl == 2) ? l012::kT2 : ((kt & 31) == 16 ? 16 : 8); }
 

@@ -121,7 +121,9 @@ FE_API int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int he
  *   cast_image (image_cast.cu:24-36) + GaussianGPUImagePyramid::build (image_pyramid.h:81-98,
  *   gaussian_scaling_kernel image_pyramid.cu:56-102) + GPUGradientPyramid::set
  *   (gradient_pyramid.cpp:83-118, conv_grad_x/y convolutions.cu:74-139).
- * `pyr` must describe width x height at level 0.  box3 must be 0 (box prefilter not built). */
+ * `pyr` must describe width x height at level 0.  box3 must be 0 (box prefilter not built).
+ * One launch builds every level (the last CTA of the levels 0-2 pass computes the deeper ones, with
+ * one of the context's 64 completion counters, used in turn: at most 64 builds in flight per context). */
 FE_API int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
                      int box3, const fe_pyramid* pyr, fe_stream stream);
 /* Same from an FP32 level-0 image (rows pitch_bytes apart). */

@@ -27,8 +27,11 @@ def test_matches_reference_hashes(ctx, golden, name):
 
 
 @pytest.mark.parametrize("shape", [(15, 15), (16, 17), (61, 97), (240, 376), (376, 1241), (480, 640), (33, 1000),
-                                   (1000, 33), (720, 1280)])
+                                   (1000, 33), (720, 1280), (1200, 1920), (1920, 2560), (3000, 4000)])
 def test_matches_oracle_random_sizes(ctx, oracle, shape):
+    """Every level bit-identical to the oracle.  The sizes cover the deeper levels computed inside the
+    levels 0-2 launch with no banded phase, one (1920x1200) and two (2560x1920), and a frame too
+    large for that (4000x3000, generic stages)."""
     rng = np.random.default_rng(shape[0] * 7919 + shape[1])
     img = rng.integers(0, 256, shape, dtype=np.uint8)
     got = gpu_pyramid(ctx, img).to_numpy()
