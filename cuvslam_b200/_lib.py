@@ -122,6 +122,7 @@ _SIGS = {
     "fe_pyramid_init": (_I, [_P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid)]),
     "fe_build_pyramid": (_I, [_P, _P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid), _P]),
     "fe_build_pyramid_f32": (_I, [_P, _P, _I64, _I, _I, ctypes.POINTER(FePyramid), _P]),
+    "fe_build_pyramid_rgb": (_I, [_P, _P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid), _P]),
     "fe_select": (_I, [_P, ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
     "fe_select_noalloc": (_I, [ctypes.POINTER(FePyramid), _I, _I, _I, _I, _P, _I64, _P, _I, _I, _P, _P, _P]),
     "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),

@@ -135,7 +135,7 @@ using StagePlan = std::vector<std::vector<StageGroup>>;  // [stage index][group]
 // launch fewer per remaining stage).
 int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& p, StagePlan& plan,
                  float scale = 1.f, int kt = 8, int* counters = nullptr, int* ncounters = nullptr,
-                 int counter_cap = 0) {
+                 int counter_cap = 0, bool box3 = false) {
   const fe::Pyr pyr = to_pyr(p);
   int s = 0;
   for (int stage = 0;; ++stage) {
@@ -146,6 +146,7 @@ int plan_pyramid(const void* src, int64_t src_pitch, bool u8, const fe_pyramid& 
     job.src = stage == 0 ? src : (const void*)pyr.lv[s].img;
     job.src_pitch_bytes = stage == 0 ? src_pitch : (int64_t)pyr.lv[s].pitch * 4;
     job.write_level0 = stage == 0 ? 1 : 0;
+    job.box3 = stage == 0 && u8 && box3 ? 1 : 0;
     job.scale = stage == 0 && !u8 ? scale : 1.f;
     job.src_w = pyr.lv[s].w;
     job.src_h = pyr.lv[s].h;
@@ -468,19 +469,46 @@ int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int height, i
   return FE_OK;
 }
 
+// The pyramid of a level 0 already in pyr->image[0] (the input stage wrote it): the FP32 plan, whose
+// first stage rewrites level 0 with the same values while it computes the gradients.
+int build_from_level0(fe_context* ctx, const fe_pyramid* pyr, cudaStream_t s) {
+  StagePlan plan;
+  int rc = plan_pyramid(pyr->image[0], pyr->pitch_bytes[0], false, *pyr, plan);
+  if (rc) return rc;
+  (void)ctx;
+  return run_plan(plan, s);
+}
+
 int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
                      int box3, const fe_pyramid* pyr, fe_stream stream) {
-  if (!ctx || !image || !valid_pyramid(pyr) || box3 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (!ctx || !image || !valid_pyramid(pyr) || (box3 != 0 && box3 != 1)) return FE_ERR_INVALID_ARGUMENT;
   if (pyr->width[0] != width || pyr->height[0] != height || image_pitch_bytes < width) return FE_ERR_INVALID_ARGUMENT;
   if (!pyr->grad_y[0]) return FE_ERR_INVALID_ARGUMENT;
+  if (box3 && pyr->levels < 3) {
+    // frames too small for the levels 0-2 kernel: the prefilter as its own input stage
+    FE_CUDA(fe::launch_input_stage(image, image_pitch_bytes, 1, 1, width, height, pyr->image[0],
+                                   pyr->pitch_bytes[0] / 4, (cudaStream_t)stream));
+    return build_from_level0(ctx, pyr, (cudaStream_t)stream);
+  }
   StagePlan plan;
   // one of the context's 64 counter sets per call, in turn (at most 64 builds in flight per context)
   int used = 0, nq = 0;
   int* done = ctx->stage_done + 8 * (ctx->stage_slot++ & 63);
-  int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan, 1.f, 8, done, &used, 4);
+  int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan, 1.f, 8, done, &used, 4, box3 != 0);
   if (!rc) rc = finish_l012_plan(plan, done + 4, &nq, 2);
   if (rc) return rc;
   return run_plan(plan, (cudaStream_t)stream);
+}
+
+int fe_build_pyramid_rgb(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
+                         int box3, const fe_pyramid* pyr, fe_stream stream) {
+  if (!ctx || !image || !valid_pyramid(pyr) || (box3 != 0 && box3 != 1)) return FE_ERR_INVALID_ARGUMENT;
+  if (pyr->width[0] != width || pyr->height[0] != height || image_pitch_bytes < 3 * (int64_t)width)
+    return FE_ERR_INVALID_ARGUMENT;
+  if (!pyr->grad_y[0]) return FE_ERR_INVALID_ARGUMENT;
+  FE_CUDA(fe::launch_input_stage(image, image_pitch_bytes, 3, box3, width, height, pyr->image[0],
+                                 pyr->pitch_bytes[0] / 4, (cudaStream_t)stream));
+  return build_from_level0(ctx, pyr, (cudaStream_t)stream);
 }
 
 int fe_build_pyramid_f32(fe_context* ctx, const float* image, int64_t image_pitch_bytes, int width, int height,

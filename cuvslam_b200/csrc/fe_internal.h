@@ -18,6 +18,7 @@ struct alignas(64) StageJob {
   int write_level0;         // also write level s (image cast + gradients): the uint8 stage
   int use_tma;              // frame meets TMA alignment (16-byte base and pitch)
   float scale;              // factor on the staged source (FP32 first stage; 1 otherwise)
+  int box3;                 // levels 0-2 kernel: apply the box prefilter to the uint8 frame
   int tiles_x, tiles_y;
   int tile_begin;           // first CTA (queue position, when the launch has a queue) of this job's tiles
   Level out[3];             // out[k] = level s + k; out[0] describes level s
@@ -57,6 +58,10 @@ int l012_deep_floats();  // shared-memory floats a deeper-level item of the leve
 bool encode_frame_tmap(StageJob& job);
 cudaError_t pyramid_init();  // kernel attributes; call once per device before capture
 cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, bool tail, cudaStream_t s);
+// Level 0 of a pyramid from a uint8 mono (channels 1) or RGB8 (channels 3) frame: the reference's cast
+// (gray = 0.299 r + 0.587 g + 0.114 b for RGB) and, with box3, its box prefilter; FP32 into dst.
+cudaError_t launch_input_stage(const uint8_t* src, int64_t src_pitch, int channels, int box3, int w, int h,
+                               float* dst, int64_t dst_pitch_floats, cudaStream_t s);
 
 // ---------------------------------------------------------------- selection
 struct SelectCam {

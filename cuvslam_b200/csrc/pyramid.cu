@@ -251,8 +251,9 @@ __global__ void __launch_bounds__(kThreads) pyramid_stage_kernel(const __grid_co
 //
 // The first stage dominates the pyramid's HBM traffic (it writes ~98% of the bytes), so it has its
 // own kernel.  A CTA owns a 32x32 level-2 core tile (128x128 at level 0) and
-//   1. stages its 176x161 uint8 tile with one TMA copy (zero fill outside the frame), or with plain
-//      loads when the frame's base/pitch are not 16-byte aligned;
+//   1. stages its 176x163 uint8 tile with one TMA copy (zero fill outside the frame), or with plain
+//      loads when the frame's base/pitch are not 16-byte aligned, and applies the optional box
+//      prefilter to it (integer arithmetic, exact);
 //   2. computes level 1 on its 79x79 region as column strips with a sliding 5-row window of
 //      horizontal 5-tap sums, in integers;
 //   3. computes level 2 on its 38x38 region the same way from level 1, in FP32;
@@ -265,7 +266,7 @@ namespace l012 {
 
 constexpr int kT2 = 32;
 constexpr int kThreads = 512;
-constexpr int kS0W = 176, kS0H = 161;  // uint8 tile: cols [4X2-32, 4X2+144), rows [4Y2-18, 4Y2+143)
+constexpr int kS0W = 176, kS0H = 163;  // uint8 tile: cols [4X2-32, 4X2+144), rows [4Y2-19, 4Y2+144)
 constexpr int kS1 = 79, kS1S = 80;     // level 1: [2X2-8, 2X2+71) in x and y
 constexpr int kS2 = 38, kS2S = 40;     // level 2: rows [Y2-3, Y2+35); columns stored from X2-4
 constexpr int kB0Bytes = kS0W * kS0H;
@@ -273,6 +274,9 @@ constexpr int kOffB1 = (kB0Bytes + 127) / 128 * 128;
 constexpr int kOffB2 = kOffB1 + kS1 * kS1S * 4;
 constexpr int kOffBar = kOffB2 + kS2 * kS2S * 4;
 constexpr int kSmem = kOffBar + 64;
+// with the box prefilter: the prefiltered tile after the rest
+constexpr int kOffBox = (kSmem + 127) / 128 * 128;
+constexpr int kSmemBox = kOffBox + kB0Bytes;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -453,6 +457,67 @@ __device__ void deep_item(const StageBatch& batch, const StageJob& J, int idx, f
   }
 }
 
+// The box prefilter of the reference (CudaBoxPrefilter::prefilter, box_prefilter.cpp:31-38: a
+// [1 2 1]/4 pass along x, then along y truncated to an integer, then the frame's one-pixel border ring
+// copied from the input) on the staged uint8 tile: on integer input every partial sum is exact, so
+// an interior pixel is (sum of [1 2 1] x [1 2 1] weighted bytes) >> 4.  Four columns per thread
+// item, as packed 16-bit lanes (sums stay below 2^12); rows 1..kS0H-2 and every column are written
+// (the tile's outermost rows and columns, never read, keep their input bytes).  Pixels on the
+// frame's border ring take the input byte.
+__device__ void box3_tile(const uint8_t* raw, uint8_t* out, int a0x, int a0y, int w0, int h0) {
+  constexpr int kWords = kS0W / 4;            // 44 four-column groups per row
+  constexpr int kBand = 15;                   // rows per thread item
+  constexpr int kBands = (kS0H - 2 + kBand - 1) / kBand;
+  const uint32_t* rw = reinterpret_cast<const uint32_t*>(raw);
+  for (int it = threadIdx.x; it < kWords * kBands; it += kThreads) {
+    const int c4 = it % kWords, band = it / kWords;
+    const int r0 = 1 + band * kBand, r1 = min(kS0H - 1, r0 + kBand);
+    // horizontal [1 2 1] of four columns as two words of 16-bit lanes (columns c, c+1 | c+2, c+3)
+    auto hsum = [&](int r, uint32_t& lo, uint32_t& hi) {
+      const uint32_t w = rw[r * kWords + c4];
+      const uint32_t wl = c4 > 0 ? rw[r * kWords + c4 - 1] : 0u;
+      const uint32_t wr = c4 + 1 < kWords ? rw[r * kWords + c4 + 1] : 0u;
+      // zero-extended byte pairs (selector nibbles 4-7 pick the second operand; masks clear the rest)
+      const uint32_t cl = __byte_perm(w, 0u, 0x4140), ch = __byte_perm(w, 0u, 0x4342);  // c, c+1 | c+2, c+3
+      const uint32_t mid = __byte_perm(w, 0u, 0x4241);                                   // c+1, c+2
+      const uint32_t left = __byte_perm(wl, w, 0x4443) & 0x00ff00ffu;                    // c-1, c
+      const uint32_t right = __byte_perm(w, wr, 0x4443) & 0x00ff00ffu;                   // c+3, c+4
+      lo = left + 2u * cl + mid;
+      hi = mid + 2u * ch + right;
+    };
+    uint32_t a_lo, a_hi, b_lo, b_hi, c_lo, c_hi;
+    hsum(r0 - 1, a_lo, a_hi);
+    hsum(r0, b_lo, b_hi);
+    for (int r = r0; r < r1; ++r) {
+      hsum(r + 1, c_lo, c_hi);
+      const uint32_t vlo = ((a_lo + 2u * b_lo + c_lo) >> 4) & 0x0fff0fffu;
+      const uint32_t vhi = ((a_hi + 2u * b_hi + c_hi) >> 4) & 0x0fff0fffu;
+      reinterpret_cast<uint32_t*>(out)[r * kWords + c4] = __byte_perm(vlo, vhi, 0x6420);
+      a_lo = b_lo; a_hi = b_hi;
+      b_lo = c_lo; b_hi = c_hi;
+    }
+  }
+  // rows 0 and kS0H-1 of the tile: input bytes
+  for (int i = threadIdx.x; i < 2 * kS0W; i += kThreads) {
+    const int r = i < kS0W ? 0 : kS0H - 1, c = i < kS0W ? i : i - kS0W;
+    out[r * kS0W + c] = raw[r * kS0W + c];
+  }
+  __syncthreads();
+  // the frame's border ring: input bytes (rows 0 and h0-1, columns 0 and w0-1 inside the tile)
+  for (int i = threadIdx.x; i < 2 * (kS0W + kS0H); i += kThreads) {
+    int r, c;
+    if (i < 2 * kS0W) {
+      r = (i < kS0W ? 0 : h0 - 1) - a0y;
+      c = i % kS0W;
+    } else {
+      const int k = i - 2 * kS0W;
+      c = (k < kS0H ? 0 : w0 - 1) - a0x;
+      r = k % kS0H;
+    }
+    if (r >= 0 && r < kS0H && c >= 0 && c < kS0W) out[r * kS0W + c] = raw[r * kS0W + c];
+  }
+}
+
 // Tile t of job: levels 0-2, and when the launch computes the deeper levels, level 3's image core
 // (after which the tile counts itself complete in job.done[0]).
 __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJob& job, int t, unsigned char* sm) {
@@ -466,7 +531,7 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
   const Level& L1 = job.out[1];
   const Level& L2 = job.out[2];
   const int w0 = L0.w, h0 = L0.h, w1 = L1.w, h1 = L1.h, w2 = L2.w, h2 = L2.h;
-  const int a0x = 4 * X2 - 32, a0y = 4 * Y2 - 18;
+  const int a0x = 4 * X2 - 32, a0y = 4 * Y2 - 19;
   const int a1x = 2 * X2 - 8, a1y = 2 * Y2 - 8;
   const int a2x = X2 - 4, a2y = Y2 - 3;  // level-2 storage origin (column X2-4 is never computed)
 
@@ -503,6 +568,12 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
     }
   }
   __syncthreads();
+  if (job.box3) {
+    uint8_t* F = sm + kOffBox;
+    box3_tile(B0, F, a0x, a0y, w0, h0);
+    B0 = F;
+    __syncthreads();
+  }
 
   // 2. level 1: column strips of 14 rows, sliding window of horizontal sums
   if (tid < kS1 * 6) {
@@ -791,6 +862,42 @@ cudaError_t set_stage_attrs() {
   return set_stage_attr<float, 2, KT>();
 }
 
+// ---------------------------------------------------------------- input stage
+// Level 0 from an RGB8 frame, or from a small mono frame with the box prefilter (larger mono frames
+// get the prefilter inside the levels 0-2 kernel).  One thread per pixel.
+template <int CH>
+__device__ __forceinline__ float input_gray(const uint8_t* src, int64_t pitch, int x, int y) {
+  const uint8_t* p = src + (int64_t)y * pitch + (int64_t)x * CH;
+  if (CH == 1) return (float)p[0];
+  const float red = p[0], green = p[1], blue = p[2];
+  // the expression of cast_image_kernel_rgb (image_cast.cu:60-66), contracted by nvcc the same way
+  return 0.299f * red + 0.587f * green + 0.114f * blue;
+}
+
+template <int CH>
+__global__ void input_stage_kernel(const uint8_t* src, int64_t pitch, int box3, int w, int h, float* dst,
+                                   int64_t dp) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  float v = input_gray<CH>(src, pitch, x, y);
+  if (box3 && x > 0 && x < w - 1 && y > 0 && y < h - 1) {
+    // box_blur_x / box_blur_y (convolutions.cu:141-205): [1 2 1]/4 along x, then along y, truncated
+    float col[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int yy = y - 1 + k;
+      float s = __fmul_rn(0.25f, input_gray<CH>(src, pitch, x - 1, yy));
+      s = __fmaf_rn(0.5f, input_gray<CH>(src, pitch, x, yy), s);
+      col[k] = __fmaf_rn(0.25f, input_gray<CH>(src, pitch, x + 1, yy), s);
+    }
+    float t = __fmul_rn(0.25f, col[0]);
+    t = __fmaf_rn(0.5f, col[1], t);
+    t = __fmaf_rn(0.25f, col[2], t);
+    v = (float)(__float2uint_rz(t) & 0xffu);
+  }
+  dst[(int64_t)y * dp + x] = v;
+}
+
 }  // namespace
 
 int l012_deep_floats() { return l012::kDeepFloats; }
@@ -831,13 +938,23 @@ bool encode_frame_tmap(StageJob& job) {
 cudaError_t pyramid_init() {
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                l012::kSmem)) != cudaSuccess)
+                                l012::kSmemBox)) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(l012::pyramid_l012_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                l012::kSmem)) != cudaSuccess)
+                                l012::kSmemBox)) != cudaSuccess)
     return e;
   if ((e = set_stage_attrs<8>()) != cudaSuccess) return e;
   return set_stage_attrs<16>();
+}
+
+cudaError_t launch_input_stage(const uint8_t* src, int64_t src_pitch, int channels, int box3, int w, int h,
+                               float* dst, int64_t dst_pitch_floats, cudaStream_t s) {
+  const dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
+  if (channels == 3)
+    input_stage_kernel<3><<<grid, block, 0, s>>>(src, src_pitch, box3, w, h, dst, dst_pitch_floats);
+  else
+    input_stage_kernel<1><<<grid, block, 0, s>>>(src, src_pitch, box3, w, h, dst, dst_pitch_floats);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, bool tail, cudaStream_t s) {
@@ -847,10 +964,13 @@ cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl
       case 0: return launch_stage<uint8_t, 0>(b, tiles, kt, tail, s);
       case 1: return launch_stage<uint8_t, 1>(b, tiles, kt, tail, s);
       default:
+        bool box = false;
+        for (int j = 0; j < b.njobs; ++j) box = box || b.job[j].box3;
+        const int smem = box ? l012::kSmemBox : l012::kSmem;
         if (kt & kL012Three)
-          l012::pyramid_l012_kernel<3><<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
+          l012::pyramid_l012_kernel<3><<<tiles, l012::kThreads, smem, s>>>(b);
         else
-          l012::pyramid_l012_kernel<2><<<tiles, l012::kThreads, l012::kSmem, s>>>(b);
+          l012::pyramid_l012_kernel<2><<<tiles, l012::kThreads, smem, s>>>(b);
         return cudaGetLastError();
     }
   }

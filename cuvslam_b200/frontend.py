@@ -88,17 +88,26 @@ class ImagePyramid:
         return self._plane(self.desc.grad_y[l], l)
 
     def build(self, ctx, image_u8, blur_filter=False, stream=None):
-        """Builds all levels and gradients from a (height, width) uint8 CUDA tensor."""
-        if blur_filter:
-            raise NotImplementedError("box3 prefilter is not part of this build")
+        """Builds all levels and gradients from a (height, width) uint8 mono or (height, width, 3)
+        uint8 RGB CUDA tensor; blur_filter applies the box prefilter first (the reference's
+        GaussianGPUImagePyramid::build(image, blur_filter))."""
         img = image_u8
-        if img.dtype != torch.uint8 or img.dim() != 2 or not img.is_cuda:
-            raise ValueError("image must be a 2-D uint8 CUDA tensor")
+        if img.dtype != torch.uint8 or img.dim() not in (2, 3) or not img.is_cuda or \
+                (img.dim() == 3 and img.shape[2] != 3):
+            raise ValueError("image must be a (h, w) or (h, w, 3) uint8 CUDA tensor")
+        if img.dim() == 3:
+            if img.stride(2) != 1 or img.stride(1) != 3:
+                img = img.contiguous()
+            h, w, _ = img.shape
+            _lib.check(ctx.lib.fe_build_pyramid_rgb(ctx.handle, _ptr(img), img.stride(0), w, h, int(bool(blur_filter)),
+                                                    ctypes.byref(self.desc), _stream_handle(stream)),
+                       "fe_build_pyramid_rgb")
+            return self
         if img.stride(1) != 1:
             img = img.contiguous()
         h, w = img.shape
-        _lib.check(ctx.lib.fe_build_pyramid(ctx.handle, _ptr(img), img.stride(0), w, h, 0, ctypes.byref(self.desc),
-                                            _stream_handle(stream)), "fe_build_pyramid")
+        _lib.check(ctx.lib.fe_build_pyramid(ctx.handle, _ptr(img), img.stride(0), w, h, int(bool(blur_filter)),
+                                            ctypes.byref(self.desc), _stream_handle(stream)), "fe_build_pyramid")
         return self
 
     def build_f32(self, ctx, image_f32, stream=None):

@@ -121,11 +121,19 @@ FE_API int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int he
  *   cast_image (image_cast.cu:24-36) + GaussianGPUImagePyramid::build (image_pyramid.h:81-98,
  *   gaussian_scaling_kernel image_pyramid.cu:56-102) + GPUGradientPyramid::set
  *   (gradient_pyramid.cpp:83-118, conv_grad_x/y convolutions.cu:74-139).
- * `pyr` must describe width x height at level 0.  box3 must be 0 (box prefilter not built).
+ * `pyr` must describe width x height at level 0.  box3 = 1 applies the reference's box prefilter
+ * first (GaussianGPUImagePyramid::build with blur_filter, CudaBoxPrefilter::prefilter,
+ * box_prefilter.cpp:31-38): done on each tile inside the same kernel.
  * One launch builds every level (the last CTA of the levels 0-2 pass computes the deeper ones, with
  * one of the context's 64 completion counters, used in turn: at most 64 builds in flight per context). */
 FE_API int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width, int height,
                      int box3, const fe_pyramid* pyr, fe_stream stream);
+/* Same from an RGB8 frame (3 bytes per pixel, rows image_pitch_bytes apart): level 0 is the
+ * reference's gray conversion (cast_image_rgb, image_cast.cu:52-70, as ImageContext::
+ * build_gpu_image_pyramid does for RGB8 sources, image_context.cpp:215-240), box prefiltered when
+ * box3 = 1, computed by one input kernel straight into level 0; then the FP32 stages. */
+FE_API int fe_build_pyramid_rgb(fe_context* ctx, const uint8_t* image, int64_t image_pitch_bytes, int width,
+                                int height, int box3, const fe_pyramid* pyr, fe_stream stream);
 /* Same from an FP32 level-0 image (rows pitch_bytes apart). */
 FE_API int fe_build_pyramid_f32(fe_context* ctx, const float* image, int64_t image_pitch_bytes, int width, int height,
                          const fe_pyramid* pyr, fe_stream stream);

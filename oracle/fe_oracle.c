@@ -39,6 +39,68 @@ void or_cast_u8(const uint8_t* src, int w, int h, float* dst) {
   for (size_t i = 0; i < (size_t)w * h; ++i) dst[i] = (float)src[i];
 }
 
+/* cast_image_kernel_rgb (cuda_kernels/image_cast.cu:52-70): gray = 0.299 r + 0.587 g + 0.114 b in
+ * FP32.  nvcc contracts the expression into fused multiply-adds; `variant` names the contraction:
+ *   0: no fusion   ((0.299 r + 0.587 g) + 0.114 b), each product and sum rounded
+ *   1: fma(0.114, b, fma(0.587, g, 0.299 r))
+ *   2: fma(0.114, b, fma(0.299, r, 0.587 g))
+ *   3: fma(0.587, g, 0.299 r) + 0.114 b
+ *   4: fma(0.299, r, 0.587 g) + 0.114 b
+ * (the tests pin which one the reference kernel computes against its own outputs). */
+void or_rgb_to_gray(const uint8_t* rgb, int w, int h, int64_t pitch, float* dst, int variant) {
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const uint8_t* p = rgb + (size_t)y * pitch + 3 * (size_t)x;
+      const float r = (float)p[0], g = (float)p[1], b = (float)p[2];
+      const float pr = 0.299f * r, pg = 0.587f * g, pb = 0.114f * b;
+      float v;
+      switch (variant) {
+        case 1: v = fmaf(0.114f, b, fmaf(0.587f, g, pr)); break;
+        case 2: v = fmaf(0.114f, b, fmaf(0.299f, r, pg)); break;
+        case 3: v = fmaf(0.587f, g, pr) + pb; break;
+        case 4: v = fmaf(0.299f, r, pg) + pb; break;
+        default: v = (pr + pg) + pb; break;
+      }
+      dst[(size_t)y * w + x] = v;
+    }
+}
+
+/* CudaBoxPrefilter::prefilter (cuda_modules/box_prefilter.cpp:31-38): box_blur_x_kernel, then
+ * box_blur_y_kernel on its output, then copy_border_kernel with border 1 (convolutions.cu:141-220).
+ * x pass: 0.25 v[x-1] + 0.5 v[x] + 0.25 v[x+1], 0 in columns 0 and w-1; y pass: the same down the
+ * x pass's columns, 0 in rows 0 and h-1, then truncated to an integer (the kernel stores
+ * (uint8_t)v); finally the one-pixel border ring is the input itself.  The weights are powers of
+ * two, so each product is exact and each sum rounds once whether or not it is fused. */
+void or_box3(const float* src, int w, int h, float* dst) {
+  float* xb = (float*)malloc(sizeof(float) * (size_t)w * h);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      float v = 0.f;
+      if (x > 0 && x < w - 1) {
+        const float* r = src + (size_t)y * w + x;
+        v = 0.25f * r[-1];
+        v = fmaf(0.5f, r[0], v);
+        v = fmaf(0.25f, r[1], v);
+      }
+      xb[(size_t)y * w + x] = v;
+    }
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      float v;
+      if (x == 0 || x == w - 1 || y == 0 || y == h - 1) {
+        v = src[(size_t)y * w + x];
+      } else {
+        const float* c = xb + (size_t)y * w + x;
+        float s = 0.25f * c[-w];
+        s = fmaf(0.5f, c[0], s);
+        s = fmaf(0.25f, c[w], s);
+        v = (float)(uint8_t)s;
+      }
+      dst[(size_t)y * w + x] = v;
+    }
+  free(xb);
+}
+
 /* gaussian_scaling_kernel (cuda_kernels/image_pyramid.cu:56-102): 5x5 [1 4 6 4 1]^T[1 4 6 4 1]/256
  * evaluated at even source coordinates, taps visited row-major and accumulated with FMA, mirror
  * addressing -x-1 / 2n-x-1, and the taps whose row AND column both fall outside are skipped. */

@@ -47,6 +47,8 @@ enum { OR_SAMPLE_TEXTURE = 0, /* emulation of cudaFilterModeLinear (8-bit-fracti
 
 int or_level_sizes(int w, int h, int max_levels, int* ws, int* hs);
 void or_cast_u8(const uint8_t* src, int w, int h, float* dst);
+void or_rgb_to_gray(const uint8_t* rgb, int w, int h, int64_t pitch, float* dst, int variant);
+void or_box3(const float* src, int w, int h, float* dst);
 void or_gauss_downscale(const float* src, int sw, int sh, float* dst, int dw, int dh);
 void or_gradients(const float* in, int w, int h, float* gx, float* gy);
 void or_gftt_response(const float* gx, const float* gy, int w, int h, float* resp);

@@ -36,6 +36,8 @@ def lib():
         L.or_level_sizes.argtypes = [I, I, I, P, P]
         L.or_cast_u8.argtypes = [P, I, I, P]
         L.or_gauss_downscale.argtypes = [P, I, I, P, I, I]
+        L.or_rgb_to_gray.argtypes = [P, I, I, ctypes.c_int64, P, I]
+        L.or_box3.argtypes = [P, I, I, P]
         L.or_gradients.argtypes = [P, I, I, P, P]
         L.or_gftt_response.argtypes = [P, P, I, I, P]
         L.or_bins.argtypes = [P, I, I, P]
@@ -119,6 +121,35 @@ def pyramid_f32(img_f32, max_levels=10):
         L.or_gradients(_p(prev), lw, lh, _p(gx), _p(gy))
         out.append((prev, gx, gy))
     return out
+
+
+RGB_VARIANT = 2  # the reference kernel computes fma(0.114, b, fma(0.299, r, 0.587 g)) (pinned by the tests)
+
+
+def rgb_to_gray(rgb, variant=None):
+    """(h, w, 3) uint8 -> (h, w) float32 as cast_image_kernel_rgb computes it."""
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    h, w, _ = rgb.shape
+    out = np.zeros((h, w), np.float32)
+    lib().or_rgb_to_gray(_p(rgb), w, h, w * 3, _p(out), RGB_VARIANT if variant is None else variant)
+    return out
+
+
+def box3(img_f32):
+    """The reference's box prefilter of a float32 level 0."""
+    img = np.ascontiguousarray(img_f32, np.float32)
+    h, w = img.shape
+    out = np.zeros_like(img)
+    lib().or_box3(_p(img), w, h, _p(out))
+    return out
+
+
+def level0(img, box=False):
+    """The pyramid's level 0 from a (h, w) uint8 mono or (h, w, 3) uint8 RGB frame, optionally box
+    prefiltered (ImageContext::build_gpu_image_pyramid + GaussianGPUImagePyramid::build)."""
+    img = np.asarray(img)
+    base = rgb_to_gray(img) if img.ndim == 3 else img.astype(np.float32)
+    return box3(base) if box else base
 
 
 def gftt(gx, gy):

@@ -10,6 +10,8 @@
 //   - GPUImage<float> pitched storage + point/linear texture objects   (cuda_helper.h:297-300,402-431)
 //   - ImageCast::cast (u8 upload + cast_image)                          (image_cast.cpp:33-47)
 //   - GaussianGPUImagePyramid::build / prepare_levels                   (image_pyramid.h:81-98,136-151)
+//   - cast_image_rgb + CudaBoxPrefilter::prefilter (RGB8 input, box3)   (image_context.cpp:215-240,
+//                                                                        box_prefilter.cpp:31-38)
 //   - GPUGradientPyramid::set                                           (gradient_pyramid.cpp:83-118)
 //   - GPUSelection::computeGFTTAndSelectFeatures incl. host quota loop  (selection_v2.cpp:27-184)
 //   - GPULKFeatureTracker::track_points                                 (cuda_modules/lk_tracker.cpp:24-73)
@@ -111,6 +113,61 @@ int init_tables() {
 }
 
 // ImageCast::cast + GaussianGPUImagePyramid::build + GPUGradientPyramid::set.
+int build(const uint8_t* host_u8, int w, int h, int max_levels, Pyr& p, cudaStream_t s);
+
+// The same with the input options of ImageContext::build_gpu_image_pyramid (image_context.cpp:215-240):
+// an RGB8 frame (cast_image_rgb) and the box prefilter of GaussianGPUImagePyramid::build
+// (CudaBoxPrefilter::prefilter: box_blur_x, box_blur_y, copy_border with border 1).
+int build_ex(const uint8_t* host, int w, int h, int rgb, int box3, int max_levels, Pyr& p, cudaStream_t s) {
+  p.n = level_count(w, h, max_levels);
+  int lw = w, lh = h;
+  for (int l = 0; l < p.n; ++l) {
+    p.img[l].reset(new DevImage);
+    p.gx[l].reset(new DevImage);
+    p.gy[l].reset(new DevImage);
+    HCHECK(p.img[l]->alloc(lw, lh));
+    HCHECK(p.gx[l]->alloc(lw, lh));
+    HCHECK(p.gy[l]->alloc(lw, lh));
+    lw = (lw + 1) / 2;
+    lh = (lh + 1) / 2;
+  }
+  const int bpp = rgb ? 3 : 1;
+  uint8_t* d_u8 = nullptr;
+  size_t u8_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&d_u8, &u8_pitch, (size_t)w * bpp, h));
+  HCHECK(cudaMemcpy2D(d_u8, u8_pitch, host, (size_t)w * bpp, (size_t)w * bpp, h, cudaMemcpyHostToDevice));
+  DevImage cast, buffer;
+  HCHECK(cast.alloc(w, h));
+  if (rgb)
+    HCHECK(cast_image_rgb(d_u8, u8_pitch, cast.ptr, cast.pitch, {(unsigned)w, (unsigned)h}, s));
+  else
+    HCHECK(cast_image(d_u8, u8_pitch, cast.ptr, cast.pitch, {(unsigned)w, (unsigned)h}, s));
+  if (box3) {
+    HCHECK(init_box_prefilter_kernels());
+    HCHECK(buffer.alloc(w, h));
+    HCHECK(box_blur_x(cast.tex_point, {(unsigned)w, (unsigned)h}, buffer.ptr, buffer.pitch, s));
+    HCHECK(box_blur_y(buffer.tex_point, {(unsigned)w, (unsigned)h}, p.img[0]->ptr, p.img[0]->pitch, s));
+    HCHECK(copy_border(cast.tex_point, {(unsigned)w, (unsigned)h}, p.img[0]->ptr, p.img[0]->pitch, 1, s));
+  } else {
+    HCHECK(cudaMemcpy2DAsync(p.img[0]->ptr, p.img[0]->pitch, cast.ptr, cast.pitch, (size_t)w * 4, h,
+                             cudaMemcpyDeviceToDevice, s));
+  }
+  for (int l = 0; l + 1 < p.n; ++l) {
+    const DevImage& a = *p.img[l];
+    DevImage& b = *p.img[l + 1];
+    HCHECK(gaussian_scaling(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, b.ptr, b.pitch,
+                            {(unsigned)b.w, (unsigned)b.h}, s));
+  }
+  for (int l = 0; l < p.n; ++l) {
+    const DevImage& a = *p.img[l];
+    HCHECK(conv_grad_x(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, p.gx[l]->ptr, p.gx[l]->pitch, s));
+    HCHECK(conv_grad_y(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, p.gy[l]->ptr, p.gy[l]->pitch, s));
+  }
+  HCHECK(cudaStreamSynchronize(s));
+  cudaFree(d_u8);
+  return 0;
+}
+
 int build(const uint8_t* host_u8, int w, int h, int max_levels, Pyr& p, cudaStream_t s) {
   p.n = level_count(w, h, max_levels);
   int lw = w, lh = h;
@@ -305,6 +362,26 @@ int ref_select(const uint8_t* img, int w, int h, const float* alive_xy, int n_al
   cudaFree(kp);
   cudaFree(bins);
   cudaFree(tmp);
+  return 0;
+}
+
+// Pyramid of a mono or RGB8 frame with or without the box prefilter (build_ex), all levels to host
+// buffers laid out level after level (as ref_pyramid).
+int ref_pyramid_ex(const uint8_t* img, int w, int h, int rgb, int box3, int max_levels, int* nlev, float* levels,
+                   float* gx, float* gy) {
+  int rc = init_tables();
+  if (rc) return rc;
+  Pyr p;
+  rc = build_ex(img, w, h, rgb, box3, max_levels, p, 0);
+  if (rc) return rc;
+  size_t off = 0;
+  for (int l = 0; l < p.n; ++l) {
+    HCHECK(p.img[l]->download(levels + off));
+    HCHECK(p.gx[l]->download(gx + off));
+    HCHECK(p.gy[l]->download(gy + off));
+    off += (size_t)p.img[l]->w * p.img[l]->h;
+  }
+  *nlev = p.n;
   return 0;
 }
 

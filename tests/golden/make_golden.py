@@ -11,6 +11,8 @@ Step 2 (a B200, after oracle/build_ref.sh built oracle/_ref/libcuvslam_ref.so):
     the sorted keypoints, the selected features, the LK results and a texture-sampling probe) and
     DIR/reference_full.npz (every intermediate array, for debugging; not committed).
 The committed tests/golden/reference.npz is the step-2 output.
+`input-reference --out DIR` runs the reference's cast_image_rgb and box prefilter ahead of its pyramid
+(oracle/ref_harness.cu ref_pyramid_ex) and writes DIR/input_reference.npz.
 `stereo-reference --out DIR` runs the reference's multi-launch left-to-right scan
 (lk_track_horizontal per candidate round, oracle/ref_harness.cu) on stereo_inputs.npz and writes
 DIR/stereo_reference.npz.
@@ -271,9 +273,50 @@ def make_stereo_reference(out_dir):
     np.savez_compressed(os.path.join(out_dir, "stereo_reference.npz"), **compact)
 
 
+# Input-stage fixtures: the pyramid from an RGB8 frame (cast_image_rgb) and with the box prefilter,
+# by the reference's kernels (oracle/ref_harness.cu ref_pyramid_ex), on frames built from inputs.npz.
+INPUT_CASES = ("c1", "odd", "tiny")
+INPUT_MODES = {"mono_box3": (0, 1), "rgb": (1, 0), "rgb_box3": (1, 1)}
+
+
+def input_frame(inp, name, rgb):
+    prev = inp[f"{name}/prev"]
+    if not rgb:
+        return np.ascontiguousarray(prev)
+    return np.ascontiguousarray(np.stack([prev, inp[f"{name}/next"], np.roll(prev, 7, axis=1)], -1))
+
+
+def make_input_reference(out_dir):
+    lib = _lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.ref_pyramid_ex.argtypes = [P, I, I, I, I, I, P, P, P, P]
+    inp = np.load(os.path.join(HERE, "inputs.npz"))
+    compact = {}
+    for name in INPUT_CASES:
+        for mode, (rgb, box) in INPUT_MODES.items():
+            img = input_frame(inp, name, rgb)
+            h, w = img.shape[:2]
+            sizes = level_sizes(w, h, 10)
+            total = sum(a * b for a, b in sizes)
+            lv, gx, gy = (np.zeros(total, np.float32) for _ in range(3))
+            n = ctypes.c_int(0)
+            rc = lib.ref_pyramid_ex(_ptr(img), w, h, rgb, box, 10, ctypes.byref(n), _ptr(lv), _ptr(gx), _ptr(gy))
+            assert rc == 0 and n.value == len(sizes), (rc, n.value)
+            off = 0
+            for l, (a, b) in enumerate(sizes):
+                for q, arr in (("img", lv), ("gx", gx), ("gy", gy)):
+                    compact[f"{name}/{mode}/L{l}/{q}/sha"] = np.array(_sha(arr[off:off + a * b].reshape(b, a)))
+                if l == 0 and name != "c1":
+                    compact[f"{name}/{mode}/level0"] = lv[:a * b].reshape(b, a).copy()
+                off += a * b
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "input_reference.npz"), **compact)
+    print("wrote input_reference.npz")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference"])
+    ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference", "input-reference"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if a.step == "inputs":
@@ -282,5 +325,7 @@ if __name__ == "__main__":
         make_stereo_inputs(os.path.join(HERE, "stereo_inputs.npz"))
     elif a.step == "stereo-reference":
         make_stereo_reference(a.out)
+    elif a.step == "input-reference":
+        make_input_reference(a.out)
     else:
         make_reference(a.out)

@@ -1,12 +1,17 @@
 """Pyramid + gradient kernels on the GPU: bit-identical to the oracle (and so to the reference)."""
 
 import hashlib
+import os
+import sys
 
 import numpy as np
 import pytest
 import torch
 
-from conftest import gpu_pyramid
+from conftest import ROOT, gpu_pyramid
+from cuvslam_b200.frontend import ImagePyramid
+
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 
 pytestmark = pytest.mark.gpu
 
@@ -77,3 +82,60 @@ def test_full_size_properties(ctx):
     assert np.all(gx[:, :3] == 0) and np.all(gx[:, -3:] == 0)
     gy = p.grad_y(0).cpu().numpy()
     assert np.abs(gy).max() < 1e-4
+
+
+def _rgb_variant(oracle, golden):
+    from test_oracle_input import matching_rgb_variant
+
+    path = os.path.join(ROOT, "tests", "golden", "input_reference.npz")
+    if not os.path.exists(path):
+        pytest.skip("input_reference.npz not generated")
+    v = matching_rgb_variant(oracle, golden, np.load(path))
+    assert v is not None, "no oracle variant reproduces the reference's RGB conversion"
+    return v
+
+
+@pytest.mark.parametrize("shape", [(17, 31), (40, 50), (61, 97), (162, 176), (163, 200), (480, 752), (1200, 1920)])
+@pytest.mark.parametrize("mode", ["mono_box3", "rgb", "rgb_box3"])
+def test_input_stage_matches_oracle(ctx, oracle, golden, shape, mode):
+    """RGB8 input (gray conversion) and the box prefilter: every level bit-identical to the oracle.
+    Mono frames of three or more levels take the prefilter inside the levels 0-2 kernel, smaller ones
+    and every RGB frame the input kernel."""
+    rgb, box = mode.startswith("rgb"), mode.endswith("box3")
+    rng = np.random.default_rng(shape[0] * 31 + shape[1] + (7 if rgb else 0))
+    img = rng.integers(0, 256, shape + ((3,) if rgb else ()), dtype=np.uint8)
+    if rgb:
+        oracle_img = oracle.rgb_to_gray(img, _rgb_variant(oracle, golden))
+        base = oracle.box3(oracle_img) if box else oracle_img
+    else:
+        base = oracle.level0(img, box=True)
+    want = oracle.pyramid_f32(base)
+    h, w = shape
+    p = ImagePyramid(w, h).build(ctx, torch.from_numpy(img).cuda(), blur_filter=box)
+    torch.cuda.synchronize()
+    got = p.to_numpy()
+    assert len(got) == len(want)
+    for l, (g, wv) in enumerate(zip(got, want)):
+        for q in range(3):
+            np.testing.assert_array_equal(g[q], wv[q], err_msg=f"level {l} plane {q}")
+
+
+@pytest.mark.parametrize("name", ["c1", "odd", "tiny"])
+@pytest.mark.parametrize("mode", ["mono_box3", "rgb", "rgb_box3"])
+def test_input_stage_matches_reference_hashes(ctx, golden, name, mode):
+    path = os.path.join(ROOT, "tests", "golden", "input_reference.npz")
+    if not os.path.exists(path):
+        pytest.skip("input_reference.npz not generated")
+    from make_golden import INPUT_MODES, input_frame
+
+    ref = np.load(path)
+    inp, _ = golden
+    rgb, box = INPUT_MODES[mode]
+    img = input_frame(inp, name, rgb)
+    h, w = img.shape[:2]
+    p = ImagePyramid(w, h).build(ctx, torch.from_numpy(img).cuda(), blur_filter=bool(box))
+    torch.cuda.synchronize()
+    for l, (a, gx, gy) in enumerate(p.to_numpy()):
+        assert _sha(a) == str(ref[f"{name}/{mode}/L{l}/img/sha"]), (l, "img")
+        assert _sha(gx) == str(ref[f"{name}/{mode}/L{l}/gx/sha"]), (l, "gx")
+        assert _sha(gy) == str(ref[f"{name}/{mode}/L{l}/gy/sha"]), (l, "gy")
