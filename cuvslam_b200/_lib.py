@@ -29,6 +29,29 @@ class FePyramid(ctypes.Structure):
     ]
 
 
+class FeTrackFinish(ctypes.Structure):
+    _fields_ = [
+        ("retrack_ncc", ctypes.c_float),
+        ("age", ctypes.c_void_p),
+        ("predicted", ctypes.c_void_p),
+        ("mask", ctypes.c_void_p),
+        ("mask_pitch_bytes", ctypes.c_int64),
+        ("collapse", ctypes.c_int32),
+        ("alive_count", ctypes.c_void_p),
+    ]
+
+
+class FeFinishCamera(ctypes.Structure):
+    _fields_ = [
+        ("tracks", ctypes.c_void_p),
+        ("n", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("border", ctypes.c_int32 * 4),
+        ("opts", FeTrackFinish),
+    ]
+
+
 class FeCameraFrame(ctypes.Structure):
     _fields_ = [
         ("image", ctypes.c_void_p),
@@ -43,6 +66,7 @@ class FeCameraFrame(ctypes.Structure):
         ("new_xy", ctypes.c_void_p),
         ("new_count", ctypes.c_void_p),
         ("border", ctypes.c_int32 * 4),
+        ("finish", ctypes.POINTER(FeTrackFinish)),
     ]
 
 
@@ -128,6 +152,8 @@ _SIGS = {
     "fe_select_debug": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     "fe_track": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _P]),
     "fe_track_stereo": (_I, [_P, ctypes.POINTER(FeStereoPair), _I, ctypes.c_float, _I, _I, _P]),
+    "fe_track_mono": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, ctypes.c_float, _I, _P]),
+    "fe_finish_tracks": (_I, [_P, ctypes.POINTER(FeFinishCamera), _I, _P]),
     "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),
     "fe_batch_run": (_I, [_P, _P]),
     "fe_batch_run_plain": (_I, [_P, _P]),

@@ -22,6 +22,15 @@ namespace {
 
 thread_local int g_last_cuda_error = 0;
 
+// cudaMalloc that leaves no error state behind when it succeeds: the runtime has been seen to return
+// success from cudaMalloc while recording cudaErrorInvalidValue as the thread's last error, which the
+// next kernel launch's cudaGetLastError() check would then report as its own failure.
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) (void)cudaGetLastError();
+  return e;
+}
+
 int cuda_fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
   return e == cudaErrorMemoryAllocation ? FE_ERR_OUT_OF_MEMORY : FE_ERR_CUDA;
@@ -267,6 +276,8 @@ struct fe_context {
   int* stage_done = nullptr;  // fe_build_pyramid's CTA counters (the levels 0-2 kernel's last CTA per
                               // frame computes the deeper levels): 64, used in turn
   unsigned stage_slot = 0;
+  unsigned long long* finish_cells = nullptr;  // fe_finish_tracks' collapse cells (zero between calls)
+  size_t finish_cap = 0;
   void* stereo_mem = nullptr;  // left-to-right matching scratch (grown on demand)
   size_t stereo_bytes = 0;
   bool debug = false;
@@ -331,7 +342,7 @@ int ensure_select_scratch(fe_context* ctx, int w, int h, int n_alive_cap, int q_
   ScratchLayout L = scratch_layout(w, h, na, qc);
   if (s.mem) cudaFree(s.mem);
   s.mem = nullptr;
-  FE_CUDA(cudaMalloc(&s.mem, L.total));
+  FE_CUDA(dev_alloc((void**)&s.mem, L.total));
   char* base = (char*)s.mem;
   s.w = w;
   s.h = h;
@@ -408,8 +419,8 @@ int fe_create(int device, fe_context** out) {
   if (!c) return FE_ERR_OUT_OF_MEMORY;
   c->device = device;
   c->debug = getenv("CUVSLAM_FE_DEBUG_MAPS") != nullptr;
-  cudaError_t e = cudaMalloc((void**)&c->lk_counter, 256);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->stage_done, 64 * 8 * sizeof(int));
+  cudaError_t e = dev_alloc((void**)&c->lk_counter, 256);
+  if (e == cudaSuccess) e = dev_alloc((void**)&c->stage_done, 64 * 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->stage_done, 0, 64 * 8 * sizeof(int));
   if (e != cudaSuccess) {
     if (c->lk_counter) cudaFree(c->lk_counter);
@@ -427,6 +438,7 @@ int fe_destroy(fe_context* ctx) {
   if (ctx->lk_counter) cudaFree(ctx->lk_counter);
   if (ctx->stage_done) cudaFree(ctx->stage_done);
   if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
+  if (ctx->finish_cells) cudaFree(ctx->finish_cells);
   if (ctx->sel.resp) cudaFree(ctx->sel.resp);
   if (ctx->sel.nms) cudaFree(ctx->sel.nms);
   delete ctx;
@@ -539,8 +551,8 @@ int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int border
   if (rc) return rc;
   SelectScratch& s = ctx->sel;
   if (ctx->debug && !s.resp) {
-    FE_CUDA(cudaMalloc((void**)&s.resp, (size_t)w * h * 4));
-    FE_CUDA(cudaMalloc((void**)&s.nms, (size_t)w * h * 4));
+    FE_CUDA(dev_alloc((void**)&s.resp, (size_t)w * h * 4));
+    FE_CUDA(dev_alloc((void**)&s.nms, (size_t)w * h * 4));
   }
   cudaStream_t st = (cudaStream_t)stream;
   FE_CUDA(cudaMemsetAsync(s.mem, 0, s.zero_bytes, st));
@@ -600,6 +612,78 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
   return FE_OK;
 }
 
+int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks, int n,
+                  float retrack_ncc, int sampling, fe_stream stream) {
+  if (!(retrack_ncc == retrack_ncc)) return FE_ERR_INVALID_ARGUMENT;
+  if (!ctx || !valid_pyramid(prev) || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
+  if (cur->levels < prev->levels) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  for (int l = 0; l < prev->levels; ++l)
+    if (!prev->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
+  if ((uintptr_t)tracks % 16 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FE_OK;
+  fe::LkLaunch p;
+  memset(&p, 0, sizeof(p));
+  p.counter = ctx->lk_counter;
+  p.ncams = 1;
+  p.total = n;
+  p.sampling = sampling;
+  p.single.prev = to_pyr(*prev);
+  p.single.cur = to_pyr(*cur);
+  p.single.tracks = tracks;
+  p.single.n = n;
+  p.single.retrack_ncc = retrack_ncc > 0.f ? retrack_ncc : 0.f;
+  FE_CUDA(fe::launch_lk(p, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_finish_tracks(fe_context* ctx, const fe_finish_camera* cams, int ncams, fe_stream stream) {
+  if (!ctx || !cams || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
+  if (ncams > fe::kMaxCams) return FE_ERR_CAPACITY;
+  fe::FinishBatch fb;
+  memset(&fb, 0, sizeof(fb));
+  size_t ncells = 0;
+  for (int i = 0; i < ncams; ++i) {
+    const fe_finish_camera& c = cams[i];
+    if (c.n < 0 || (c.n > 0 && (!c.tracks || !c.opts.age)) || c.width <= 0 || c.height <= 0)
+      return FE_ERR_INVALID_ARGUMENT;
+    if ((uintptr_t)c.tracks % 16 != 0 || (uintptr_t)c.opts.predicted % 8 != 0) return FE_ERR_INVALID_ARGUMENT;
+    if (c.opts.mask && c.opts.mask_pitch_bytes < c.width) return FE_ERR_INVALID_ARGUMENT;
+    if (c.opts.collapse) ncells += (size_t)((c.width + 2) / 3) * ((c.height + 2) / 3);
+  }
+  if (ncells > ctx->finish_cap) {
+    if (ctx->finish_cells) cudaFree(ctx->finish_cells);
+    ctx->finish_cells = nullptr;
+    ctx->finish_cap = 0;
+    FE_CUDA(dev_alloc((void**)&ctx->finish_cells, ncells * sizeof(unsigned long long)));
+    FE_CUDA(cudaMemset(ctx->finish_cells, 0, ncells * sizeof(unsigned long long)));
+    ctx->finish_cap = ncells;
+  }
+  size_t o = 0;
+  for (int i = 0; i < ncams; ++i) {
+    const fe_finish_camera& c = cams[i];
+    fe::FinishCam& f = fb.cam[fb.ncams++];
+    f.tracks = c.tracks;
+    f.age = c.opts.age;
+    f.n = c.n;
+    f.pred = c.opts.predicted;
+    f.w = c.width;
+    f.h = c.height;
+    for (int k = 0; k < 4; ++k) f.border[k] = c.border[k];
+    f.mask = c.opts.mask;
+    f.mask_pitch = c.opts.mask_pitch_bytes;
+    f.alive_count = c.opts.alive_count;
+    if (c.opts.collapse) {
+      f.cw = (c.width + 2) / 3;
+      f.ch = (c.height + 2) / 3;
+      f.cells = ctx->finish_cells + o;
+      o += (size_t)f.cw * f.ch;
+    }
+  }
+  FE_CUDA(fe::launch_finish(fb, (cudaStream_t)stream));
+  return FE_OK;
+}
+
 int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, float early_exit_fraction,
                     int horizontal, int sampling, fe_stream stream) {
   if (!ctx || !pairs || npairs <= 0) return FE_ERR_INVALID_ARGUMENT;
@@ -649,9 +733,10 @@ int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, fl
   const int64_t need = zero_bytes + ones_bytes + pos_elems * 8;
   if ((size_t)need > ctx->stereo_bytes) {
     if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
+  if (ctx->finish_cells) cudaFree(ctx->finish_cells);
     ctx->stereo_mem = nullptr;
     ctx->stereo_bytes = 0;
-    FE_CUDA(cudaMalloc(&ctx->stereo_mem, (size_t)need));
+    FE_CUDA(dev_alloc((void**)&ctx->stereo_mem, (size_t)need));
     ctx->stereo_bytes = (size_t)need;
   }
   char* base = (char*)ctx->stereo_mem;
@@ -741,6 +826,8 @@ struct fe_batch {
   int lk_shape = 0;      // LK block shape (fe::kLkShapes)
   int overlap = 1;       // response tiles on a second stream beside LK
   int stage_tile = 8;    // deepest-level tile of the generic pyramid stages
+  fe::FinishBatch* finish = nullptr;      // cameras with finish filters (heap), or nullptr
+  unsigned long long* finish_cells = nullptr;
 };
 
 namespace {
@@ -766,6 +853,7 @@ int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap =
   rc = run_stages(b->plan, split, b->plan.size(), st);
   if (rc) return rc;
   if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
+  if (b->finish) FE_CUDA(fe::launch_finish(*b->finish, st));
   if (fork) {
     FE_CUDA(cudaEventRecord(b->join_ev, side));
     FE_CUDA(cudaStreamWaitEvent(st, b->join_ev, 0));
@@ -826,7 +914,7 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
   for (int i = 0; i < b->ncams; ++i)
     if (b->has_prev[i]) bytes += (size_t)b->cams[i].n_tracks * sizeof(fe_track_data);
   void* saved = nullptr;
-  if (bytes) FE_CUDA(cudaMalloc(&saved, bytes));
+  if (bytes) FE_CUDA(dev_alloc((void**)&saved, bytes));
   auto copy_tracks = [&](bool save) -> cudaError_t {
     size_t o = 0;
     for (int i = 0; i < b->ncams; ++i) {
@@ -973,17 +1061,18 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
       lc.tracks = c.tracks;
       lc.n = c.n_tracks;
       lc.begin = total;
+      lc.retrack_ncc = c.finish ? c.finish->retrack_ncc : 0.f;
       total += c.n_tracks;
       lk.push_back(lc);
     }
   }
   memset(&b->lk, 0, sizeof(b->lk));
   if (!lk.empty()) {
-    cudaError_t e = cudaMalloc((void**)&b->d_lk, sizeof(fe::LkCam) * lk.size());
+    cudaError_t e = dev_alloc((void**)&b->d_lk, sizeof(fe::LkCam) * lk.size());
     if (e != cudaSuccess) return fail(cuda_fail(e));
     e = cudaMemcpy(b->d_lk, lk.data(), sizeof(fe::LkCam) * lk.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_fail(e));
-    e = cudaMalloc((void**)&b->lk_counter, 256);
+    e = dev_alloc((void**)&b->lk_counter, 256);
     if (e != cudaSuccess) return fail(cuda_fail(e));
     b->lk.cams = b->d_lk;
     b->lk.counter = b->lk_counter;
@@ -991,6 +1080,48 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     b->lk.total = total;
     b->lk.horizontal = 0;
     b->lk.sampling = sampling;
+  }
+  // finish filters (cameras with tracks and options): one CTA per camera, collapse cells zeroed once
+  {
+    fe::FinishBatch fb;
+    memset(&fb, 0, sizeof(fb));
+    size_t ncells = 0;
+    for (int i = 0; i < ncams; ++i) {
+      const fe_camera_frame& c = cams[i];
+      if (!c.finish || !b->has_prev[i]) continue;
+      if (!c.finish->age) return fail(FE_ERR_INVALID_ARGUMENT);
+      fe::FinishCam& f = fb.cam[fb.ncams++];
+      f.tracks = c.tracks;
+      f.age = c.finish->age;
+      f.n = c.n_tracks;
+      f.pred = c.finish->predicted;
+      f.w = c.width;
+      f.h = c.height;
+      for (int k = 0; k < 4; ++k) f.border[k] = c.border[k];
+      f.mask = c.finish->mask;
+      f.mask_pitch = c.finish->mask_pitch_bytes;
+      f.alive_count = c.finish->alive_count;
+      if (c.finish->collapse) {
+        f.cw = (c.width + 2) / 3;
+        f.ch = (c.height + 2) / 3;
+        ncells += (size_t)f.cw * f.ch;
+      }
+    }
+    if (fb.ncams > 0) {
+      if (ncells) {
+        cudaError_t e = dev_alloc((void**)&b->finish_cells, ncells * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemset(b->finish_cells, 0, ncells * sizeof(unsigned long long));
+        if (e != cudaSuccess) return fail(cuda_fail(e));
+      }
+      size_t o = 0;
+      for (int k = 0; k < fb.ncams; ++k)
+        if (fb.cam[k].cw) {
+          fb.cam[k].cells = b->finish_cells + o;
+          o += (size_t)fb.cam[k].cw * fb.cam[k].ch;
+        }
+      b->finish = new (std::nothrow) fe::FinishBatch(fb);
+      if (!b->finish) return fail(FE_ERR_OUT_OF_MEMORY);
+    }
   }
   // selection scratch: every camera's [stats | burn | touched] first (one memset per step), then
   // each camera's cells, sub-tile sums, quotas, kept keys and response/NMS maps
@@ -1041,7 +1172,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     b->any_select = true;
   }
   if (b->any_select) {
-    cudaError_t e = cudaMalloc(&b->sel_mem, zero + rest);
+    cudaError_t e = dev_alloc((void**)&b->sel_mem, zero + rest);
     if (e != cudaSuccess) return fail(cuda_fail(e));
     b->zero_bytes = zero;
     char* zp = (char*)b->sel_mem;
@@ -1089,7 +1220,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(cuda_fail(e));
   // pyramid stages with tails: the deep levels' counters, then the final plan
-  e = cudaMalloc((void**)&b->stage_done, sizeof(int) * (4 * ncams + 8));
+  e = dev_alloc((void**)&b->stage_done, sizeof(int) * (4 * ncams + 8));
   if (e == cudaSuccess) e = cudaMemset(b->stage_done, 0, sizeof(int) * (4 * ncams + 8));
   if (e != cudaSuccess) return fail(cuda_fail(e));
   int rc = replan_pyramids(b, b->stage_tile);
@@ -1149,7 +1280,22 @@ int fe_batch_run_plain(fe_batch* b, fe_stream stream) {
     int rc = fe_build_pyramid(ctx, c.image, c.image_pitch_bytes, c.width, c.height, 0, &b->cur[i], stream);
     if (rc) return rc;
     if (b->has_prev[i]) {
-      rc = fe_track(ctx, &b->prev[i], &b->cur[i], c.tracks, c.n_tracks, 0, b->sampling, stream);
+      if (c.finish) {
+        rc = fe_track_mono(ctx, &b->prev[i], &b->cur[i], c.tracks, c.n_tracks, c.finish->retrack_ncc, b->sampling,
+                           stream);
+        if (rc) return rc;
+        fe_finish_camera fc;
+        memset(&fc, 0, sizeof(fc));
+        fc.tracks = c.tracks;
+        fc.n = c.n_tracks;
+        fc.width = c.width;
+        fc.height = c.height;
+        for (int k = 0; k < 4; ++k) fc.border[k] = c.border[k];
+        fc.opts = *c.finish;
+        rc = fe_finish_tracks(ctx, &fc, 1, stream);
+      } else {
+        rc = fe_track(ctx, &b->prev[i], &b->cur[i], c.tracks, c.n_tracks, 0, b->sampling, stream);
+      }
       if (rc) return rc;
     }
     if (c.num_desired > 0) {
@@ -1192,6 +1338,8 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->lk_counter) cudaFree(b->lk_counter);
   if (b->sel_mem) cudaFree(b->sel_mem);
   if (b->stage_done) cudaFree(b->stage_done);
+  if (b->finish_cells) cudaFree(b->finish_cells);
+  delete b->finish;
   delete b->sel;
   delete b;
   return FE_OK;
@@ -1344,7 +1492,7 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
   const size_t o_recs = take(mode == FE_ADJOINT_UNROLLED ? std::max(total, 1) * fe::lk_record_bytes() : 0);
   const size_t o_done = take(sizeof(int) * 2 * njobs);
   const size_t o_ctr = take(256);
-  cudaError_t e = cudaMalloc(&a->mem, o);
+  cudaError_t e = dev_alloc((void**)&a->mem, o);
   if (e != cudaSuccess) return fail(cuda_fail(e));
   char* base = (char*)a->mem;
   a->counters = (int*)(base + o_ctr);

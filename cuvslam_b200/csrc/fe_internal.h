@@ -125,6 +125,7 @@ struct LkCam {
   const fe_track_data* tracks_in;  // out-of-place input records, or nullptr (tracks in place)
   int n;
   int begin;                    // first track of this camera in the flattened list
+  float retrack_ncc;            // > 0: tracks the first pass lost run again with this NCC threshold
 };
 
 // Iteration rule of a launch: the reference tracker, or the differentiable tracker (exact
@@ -152,6 +153,28 @@ struct LkLaunch {
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
 constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2
+
+// ---------------------------------------------------------------- track filters after LK
+struct FinishCam {
+  fe_track_data* tracks;        // records after LK (status in, status 0 out for dead tracks)
+  uint32_t* age;                // in/out, 0 = dead
+  int n;
+  const float* pred;            // n x 2 or nullptr; NaN x = no prediction
+  int w, h;
+  int border[4];                // top, bottom, left, right
+  const uint8_t* mask;          // or nullptr
+  int64_t mask_pitch;
+  unsigned long long* cells;    // collapse: ceil(w/3) x ceil(h/3) keys, zero between launches; or nullptr
+  int cw, ch;
+  int* alive_count;             // optional
+};
+
+struct FinishBatch {
+  int ncams;
+  FinishCam cam[kMaxCams];
+};
+
+cudaError_t launch_finish(const FinishBatch& b, cudaStream_t s);
 
 // ---------------------------------------------------------------- left-to-right matching
 constexpr int kMaxStereoPairs = 16;

@@ -128,6 +128,13 @@ class ImagePyramid:
                 for l in range(self.levels)]
 
 
+def track_mono(ctx, prev, cur, tracks, retrack_ncc=0.85, sampling=_lib.FE_SAMPLE_TEXTURE, stream=None):
+    """MonoSOFGPU::launch's track + retrack passes as collect merges them (fe_track_mono)."""
+    _lib.check(ctx.lib.fe_track_mono(ctx.handle, ctypes.byref(prev.desc), ctypes.byref(cur.desc), _ptr(tracks),
+                                     tracks.shape[0], ctypes.c_float(retrack_ncc), int(sampling),
+                                     _stream_handle(stream)), "fe_track_mono")
+
+
 def tracks_to_device(tracks, device="cuda"):
     """TRACK_DTYPE records -> (n, 80) uint8 CUDA tensor (the TrackData array the kernels update)."""
     arr = np.ascontiguousarray(tracks, dtype=TRACK_DTYPE)
@@ -214,16 +221,54 @@ class _DeviceArray:
                                          "version": 2, "strides": None}
 
 
-class CameraFrame:
-    """One camera of a batched frame step (fe_camera_frame)."""
+class TrackFinish:
+    """MonoSOFGPU's retrack pass and finish filters for one camera (fe_track_finish).  age: (n,)
+    int32/uint32 CUDA tensor of track ages (0 = dead), updated in place; predicted: optional (n, 2)
+    float32 CUDA tensor (NaN = no prediction); mask: optional (h, w) uint8 CUDA tensor."""
 
-    def __init__(self, image_u8, cur, prev=None, tracks=None, num_desired=0, border=(0, 0, 0, 0)):
+    def __init__(self, age, retrack_ncc=0.85, predicted=None, mask=None, collapse=True):
+        self.age = age
+        self.retrack_ncc = float(retrack_ncc)
+        self.predicted = predicted.contiguous() if predicted is not None else None
+        self.mask = mask.contiguous() if mask is not None else None
+        self.collapse = bool(collapse)
+        self.alive_count = torch.zeros(1, dtype=torch.int32, device=age.device)
+
+    def desc(self):
+        d = _lib.FeTrackFinish()
+        d.retrack_ncc = self.retrack_ncc
+        d.age = self.age.data_ptr()
+        d.predicted = self.predicted.data_ptr() if self.predicted is not None else None
+        d.mask = self.mask.data_ptr() if self.mask is not None else None
+        d.mask_pitch_bytes = self.mask.stride(0) if self.mask is not None else 0
+        d.collapse = int(self.collapse)
+        d.alive_count = self.alive_count.data_ptr()
+        return d
+
+
+def finish_tracks(ctx, tracks, finish, width, height, border=(0, 0, 0, 0), stream=None):
+    """fe_finish_tracks for one camera: tracks is the (n, 80) uint8 TrackData tensor after LK."""
+    c = (_lib.FeFinishCamera * 1)()
+    c[0].tracks = tracks.data_ptr()
+    c[0].n = tracks.shape[0]
+    c[0].width, c[0].height = int(width), int(height)
+    for k in range(4):
+        c[0].border[k] = int(border[k])
+    c[0].opts = finish.desc()
+    _lib.check(ctx.lib.fe_finish_tracks(ctx.handle, c, 1, _stream_handle(stream)), "fe_finish_tracks")
+
+
+class CameraFrame:
+    """One camera of a batched frame step (fe_camera_frame); finish: optional TrackFinish."""
+
+    def __init__(self, image_u8, cur, prev=None, tracks=None, num_desired=0, border=(0, 0, 0, 0), finish=None):
         self.image = image_u8.contiguous()
         self.cur = cur
         self.prev = prev
         self.tracks = tracks
         self.num_desired = int(num_desired)
         self.border = tuple(int(b) for b in border)
+        self.finish = finish
         dev = image_u8.device
         self.new_xy = torch.zeros((max(self.num_desired, 1), 2), dtype=torch.float32, device=dev)
         self.new_count = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -236,6 +281,7 @@ class Batch:
         self.ctx = ctx
         self.frames = list(frames)
         arr = (_lib.FeCameraFrame * len(self.frames))()
+        self._finish_descs = []
         for i, f in enumerate(self.frames):
             a = arr[i]
             a.image = f.image.data_ptr()
@@ -250,6 +296,10 @@ class Batch:
             a.new_count = f.new_count.data_ptr()
             for k in range(4):
                 a.border[k] = f.border[k]
+            if f.finish is not None:
+                d = f.finish.desc()
+                self._finish_descs.append(d)
+                a.finish = ctypes.pointer(d)
         h = ctypes.c_void_p()
         _lib.check(ctx.lib.fe_batch_create(ctx.handle, arr, len(self.frames), int(sampling), ctypes.byref(h)),
                    "fe_batch_create")

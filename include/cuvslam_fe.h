@@ -190,6 +190,49 @@ FE_API int fe_select_debug(fe_context* ctx, const float** response, const float*
 FE_API int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks, int n,
              int horizontal, int sampling, fe_stream stream);
 
+/* MonoSOFGPU::launch's two LK passes as MonoSOFGPU::collect merges them (sof_mono_gpu.cpp:34-104):
+ * each track with its record's ncc_threshold (0.8 in the reference), and the tracks that pass lost
+ * again from the same inputs with retrack_ncc (0.85); a record ends with the first pass's result if
+ * it tracked, else the retrack's.  The records keep their own ncc_threshold. */
+FE_API int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks,
+                         int n, float retrack_ncc, int sampling, fe_stream stream);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Track filters after LK (MonoSOFGPU::finish, on the device)                                */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Options of the filters MonoSOFGPU::finish applies after tracking (sof_mono_gpu.cpp:144-170).
+ * Device pointers. */
+typedef struct {
+  float retrack_ncc;          /* batched step: > 0 runs the retrack pass of fe_track_mono */
+  uint32_t* age;              /* n track ages (in/out; 0 = dead): required */
+  const float* predicted;     /* n x 2 predicted positions (NaN x = none), or NULL (no predictor) */
+  const uint8_t* mask;        /* nonzero = masked pixel, or NULL */
+  int64_t mask_pitch_bytes;
+  int32_t collapse;           /* 1: collapseTracks (the reference always applies it) */
+  int32_t* alive_count;       /* out: tracks alive after the filters, or NULL */
+} fe_track_finish;
+
+/* One camera's tracks after LK. */
+typedef struct {
+  fe_track_data* tracks;      /* n records (in/out): dead tracks get track_status = 0 */
+  int32_t n;
+  int32_t width, height;      /* level-0 size */
+  int32_t border[4];          /* top, bottom, left, right */
+  fe_track_finish opts;       /* retrack_ncc is ignored here */
+} fe_finish_camera;
+
+/* The filters of MonoSOFGPU::finish for ncams (<= 64) cameras in one launch, in its order: collect
+ * and age (an alive track whose record tracked ages by one, else dies; sof_mono_gpu.cpp:80-104,
+ * sof_mono_base.cpp:111-118), the prediction-error filter (sof_mono_base.cpp:51-109: with at least 3
+ * alive predicted tracks, those farther from their prediction than max(3, 2 x the median distance)
+ * die), KillTracksOnBorder (selector_stereo.cpp:109-125), KillTracksWithinMask
+ * (sof_mono_base.cpp:121-133) and collapseTracks (sof_mono_gpu.cpp:249-280: per 3x3-pixel cell the
+ * first track with the cell's largest age survives).  Not on the device: the RANSAC filter (off by
+ * default), keyframe selection and the track list's compaction.  Collapse scratch lives in the
+ * context (grown on demand: make the first call at the largest size before capturing). */
+FE_API int fe_finish_tracks(fe_context* ctx, const fe_finish_camera* cams, int ncams, fe_stream stream);
+
 /* ---------------------------------------------------------------------------------------- */
 /* Left-to-right (primary -> secondary camera) matching                                      */
 /* ---------------------------------------------------------------------------------------- */
@@ -271,6 +314,9 @@ typedef struct {
   float* new_xy;          /* out: selected features, capacity num_desired */
   int32_t* new_count;     /* out */
   int32_t border[4];      /* top, bottom, left, right */
+  const fe_track_finish* finish; /* host pointer, or NULL: MonoSOFGPU's retrack pass and finish
+                                    filters between LK and selection (selection then keeps the
+                                    survivors alive) */
 } fe_camera_frame;
 
 /* Plans a batched frame step over ncams cameras: the pyramids of all cameras, LK of all tracks,

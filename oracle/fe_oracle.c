@@ -834,6 +834,111 @@ void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const
   stats[3] = 0;
 }
 
+/* MonoSOFGPU::finish's track filters (libs/sof/sof_mono_gpu.cpp:80-104 collect, :144-170 finish;
+ * sof_mono_base.cpp:51-109 filterByPredictionError and IncrementTracksAge, :121-133
+ * KillTracksWithinMask; selector_stereo.cpp:109-125 KillTracksOnBorder; sof_mono_gpu.cpp:249-280
+ * collapseTracks), over the n tracks of one camera after LK, in the reference's order:
+ *   collect:    an alive track (age > 0) whose LK record has track_status keeps the record's track
+ *               as its position, else it dies (age 0; records merge the track and retrack passes);
+ *   age:        every alive track's age + 1;
+ *   prediction: with pred (x, y per track, NaN x = no prediction) and at least 3 alive predicted
+ *               tracks, d = |pred - position| (sqrt of dx*dx + dy*dy), m = the (count/2)-th smallest
+ *               d (nth_element), and tracks with d > max(3, 2 m) die;
+ *   border:     a track dies unless bl <= x <= w-1-br and bt <= y <= h-1-bb (integer bounds computed
+ *               as size_t, then compared as float);
+ *   mask:       a track on a nonzero mask pixel (row (size_t)y, column (size_t)x) dies;
+ *   collapse:   per 3x3-pixel cell ((size_t)(x / 3), (size_t)(y / 3)) only the first track (in index
+ *               order) with the cell's largest age survives.
+ * Dead tracks get track_status 0 in their record.  Returns the number of tracks alive. */
+int or_finish_tracks(or_track_data* td, uint32_t* age, int n, const float* pred, int w, int h, const int* border,
+                     const uint8_t* mask, int64_t mask_pitch, int collapse) {
+  for (int i = 0; i < n; ++i) {
+    if (age[i] == 0) {
+      td[i].track_status = 0;
+      continue;
+    }
+    if (td[i].track_status)
+      age[i] += 1;
+    else
+      age[i] = 0;
+  }
+  if (pred) {
+    float* d = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* sorted = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+      if (age[i] == 0 || pred[2 * i] != pred[2 * i]) continue;
+      const float dx = pred[2 * i] - td[i].track[0], dy = pred[2 * i + 1] - td[i].track[1];
+      d[i] = sqrtf(dx * dx + dy * dy);
+      sorted[m++] = d[i];
+    }
+    if (m >= 3) {
+      /* the (m/2)-th smallest: insertion-free selection by counting (m is small) */
+      float kth = 0.f;
+      for (int a = 0; a < m; ++a) {
+        int below = 0, equal = 0;
+        for (int b = 0; b < m; ++b) {
+          below += sorted[b] < sorted[a];
+          equal += sorted[b] == sorted[a];
+        }
+        if (below <= m / 2 && m / 2 < below + equal) {
+          kth = sorted[a];
+          break;
+        }
+      }
+      const float thr = 2.f * kth > 3.f ? 2.f * kth : 3.f;
+      for (int i = 0; i < n; ++i) {
+        if (age[i] == 0 || pred[2 * i] != pred[2 * i]) continue;
+        if (d[i] > thr) age[i] = 0;
+      }
+    }
+    free(d);
+    free(sorted);
+  }
+  const uint64_t W = (uint64_t)w, H = (uint64_t)h;
+  const uint64_t bt = (uint64_t)border[0], bb = (uint64_t)border[1], bl = (uint64_t)border[2],
+                 br = (uint64_t)border[3];
+  for (int i = 0; i < n; ++i) {
+    if (age[i] == 0) continue;
+    const float x = td[i].track[0], y = td[i].track[1];
+    if (!((float)bl <= x && x <= (float)(W - 1 - br) && (float)bt <= y && y <= (float)(H - 1 - bb))) age[i] = 0;
+  }
+  if (mask)
+    for (int i = 0; i < n; ++i) {
+      if (age[i] == 0) continue;
+      const float x = td[i].track[0], y = td[i].track[1];
+      if (x >= 0.f && y >= 0.f && x < (float)w && y < (float)h && mask[(size_t)y * mask_pitch + (size_t)x]) age[i] = 0;
+    }
+  if (collapse) {
+    const int cw = (w + 2) / 3, ch = (h + 2) / 3;
+    uint32_t* best = (uint32_t*)calloc((size_t)cw * ch, sizeof(uint32_t));
+    for (int i = 0; i < n; ++i) {
+      if (age[i] == 0) continue;
+      const int cx = (int)(td[i].track[0] / 3.f), cy = (int)(td[i].track[1] / 3.f);
+      if (cx < 0 || cy < 0 || cx >= cw || cy >= ch) continue;
+      uint32_t* p = &best[(size_t)cy * cw + cx];
+      if (*p < age[i]) *p = age[i];
+    }
+    for (int i = 0; i < n; ++i) {
+      if (age[i] == 0) continue;
+      const int cx = (int)(td[i].track[0] / 3.f), cy = (int)(td[i].track[1] / 3.f);
+      if (cx < 0 || cy < 0 || cx >= cw || cy >= ch) continue;
+      uint32_t* p = &best[(size_t)cy * cw + cx];
+      if (age[i] == *p)
+        *p = 0;
+      else
+        age[i] = 0;
+    }
+    free(best);
+  }
+  int alive = 0;
+  for (int i = 0; i < n; ++i) {
+    if (age[i] == 0) td[i].track_status = 0;
+    alive += age[i] != 0;
+  }
+  return alive;
+}
+
 /* FP64 restatement of the same LK (exact bilinear weights, double arithmetic, plain summation
  * order).  Used only to state per-track error of the FP32 paths. */
 static double samp64(const float* img, int w, int h, double x, double y) {

@@ -66,6 +66,9 @@ void or_lk_track_f64(int levels, const int* ws, const int* hs, const float* cons
                      const float* const* prev_gy, const float* const* prev_img, const float* const* cur_img,
                      or_track_data* td, int n);
 
+/* MonoSOFGPU::finish's track filters after LK (see fe_oracle.c); returns the tracks alive. */
+int or_finish_tracks(or_track_data* td, uint32_t* age, int n, const float* pred, int w, int h, const int* border,
+                     const uint8_t* mask, int64_t mask_pitch, int collapse);
 /* Candidates of a primary base-level point (u, v) from an epipolar table of cw x ch corner curves
  * in CSR form (offsets[cw * ch + 1], xy pairs): EpipolarCurves::Candidates
  * (libs/sof/epipolar_curves.cpp:64-101).  Writes up to `cap` x, y pairs, returns the count. */

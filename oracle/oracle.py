@@ -37,6 +37,8 @@ def lib():
         L.or_cast_u8.argtypes = [P, I, I, P]
         L.or_gauss_downscale.argtypes = [P, I, I, P, I, I]
         L.or_rgb_to_gray.argtypes = [P, I, I, ctypes.c_int64, P, I]
+        L.or_finish_tracks.argtypes = [P, P, I, P, I, I, P, P, ctypes.c_int64, I]
+        L.or_finish_tracks.restype = I
         L.or_box3.argtypes = [P, I, I, P]
         L.or_gradients.argtypes = [P, I, I, P, P]
         L.or_gftt_response.argtypes = [P, P, I, I, P]
@@ -246,6 +248,38 @@ def epipolar_candidates(cw, ch, inv_scale, offsets, xy, uv, valid=None):
         out_off.append(out_off[-1] + n)
     xy_all = np.concatenate(out_xy) if out_off[-1] else np.zeros((0, 2), np.float32)
     return np.array(out_off, np.int32), xy_all.astype(np.float32)
+
+
+def lk_retrack(prev_pyr, cur_pyr, tracks, retrack_ncc=0.85, mode=TEXTURE):
+    """MonoSOFGPU::launch's two passes merged as collect reads them: LK with each record's threshold,
+    then the tracks it lost again from their inputs with retrack_ncc (the threshold field is kept)."""
+    first = lk(prev_pyr, cur_pyr, tracks, mode)
+    lost = first["track_status"] == 0
+    if lost.any():
+        again = tracks[lost].copy()
+        again["ncc_threshold"] = retrack_ncc
+        again = lk(prev_pyr, cur_pyr, again, mode)
+        again["ncc_threshold"] = tracks[lost]["ncc_threshold"]
+        first[lost] = again
+    return first
+
+
+def finish_tracks(tracks, age, width, height, border=(0, 0, 0, 0), pred=None, mask=None, collapse=True):
+    """The finish filters (or_finish_tracks) on copies: returns (records, ages, alive count)."""
+    t = np.ascontiguousarray(tracks.copy())
+    a = np.ascontiguousarray(np.asarray(age, np.uint32).copy())
+    pp = None
+    if pred is not None:
+        pred = np.ascontiguousarray(pred, np.float32).reshape(-1, 2)
+        pp = _p(pred)
+    mp, mpitch = None, 0
+    if mask is not None:
+        mask = np.ascontiguousarray(mask, np.uint8)
+        mp, mpitch = _p(mask), mask.shape[1]
+    b = np.ascontiguousarray(border, np.int32)
+    alive = lib().or_finish_tracks(_p(t), _p(a), len(t), pp, int(width), int(height), _p(b), mp, mpitch,
+                                   int(bool(collapse)))
+    return t, a, alive
 
 
 def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_radius=48.0, ncc_threshold=0.8,

@@ -1,0 +1,109 @@
+"""MonoSOFGPU's retrack pass and finish filters on the device: fe_track_mono and fe_finish_tracks
+bit-identical to the oracle's restatement, and the batched frame step with the filters between LK
+and selection equal to the plain per-camera sequence."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import assert_tracks_equal, gpu_pyramid
+from cuvslam_b200 import synthetic
+from cuvslam_b200.frontend import (Batch, CameraFrame, ImagePyramid, Selection, TrackFinish, finish_tracks,
+                                   track_mono, tracks_from_device, tracks_to_device)
+from cuvslam_b200.types import make_tracks
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["c1", "half", "odd"])
+def test_retrack_matches_oracle(ctx, oracle, golden, name):
+    inp, ref = golden
+    tin = ref[f"{name}/lk_pred/in"]
+    pp, cp = gpu_pyramid(ctx, inp[f"{name}/prev"]), gpu_pyramid(ctx, inp[f"{name}/next"])
+    d = tracks_to_device(tin)
+    track_mono(ctx, pp, cp, d, 0.85)
+    got = tracks_from_device(d)
+    want = oracle.lk_retrack(oracle.pyramid(inp[f"{name}/prev"]), oracle.pyramid(inp[f"{name}/next"]), tin, 0.85)
+    assert_tracks_equal(got, want)
+    # the retrack pass can only add tracks to the first pass's
+    first = oracle.lk(oracle.pyramid(inp[f"{name}/prev"]), oracle.pyramid(inp[f"{name}/next"]), tin)
+    assert np.all(got["track_status"] >= first["track_status"])
+
+
+def _finish_case(seed, n, w, h, clustered=True):
+    rng = np.random.default_rng(seed)
+    xy = np.stack([rng.uniform(-3, w + 3, n), rng.uniform(-3, h + 3, n)], 1).astype(np.float32)
+    if clustered:  # many tracks in few 3x3 cells, to exercise collapse's age and index rules
+        k = n // 3
+        xy[:k] = (np.floor(xy[:k] / 3) * 3 + rng.uniform(0, 2.9, (k, 2))).astype(np.float32)
+        xy[k:2 * k] = xy[:k] + rng.uniform(-1, 1, (k, 2)).astype(np.float32)
+    t = make_tracks(xy, None, float(w), 0.8)
+    t["track_status"] = (rng.uniform(size=n) < 0.85).astype(np.uint8)
+    age = rng.integers(0, 6, n).astype(np.uint32)
+    pred = (xy + rng.normal(0, 2.0, xy.shape) * rng.choice([1.0, 4.0], (n, 1))).astype(np.float32)
+    pred[rng.uniform(size=n) < 0.2] = np.nan
+    mask = (rng.uniform(size=(h, w)) < 0.02).astype(np.uint8)
+    return t, age, pred, mask
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(pred=True), dict(mask=True), dict(pred=True, mask=True, border=(3, 4, 5, 6)),
+                                  dict(collapse=False, pred=True), dict(border=(0, 0, 2000, 0))])
+def test_finish_matches_oracle(ctx, oracle, opts):
+    w, h, n = 640, 480, 3000
+    t, age, pred, mask = _finish_case(17 + len(opts), n, w, h)
+    border = opts.get("border", (0, 0, 0, 0))
+    collapse = opts.get("collapse", True)
+    d = tracks_to_device(t)
+    age_d = torch.from_numpy(age.astype(np.int32)).cuda()
+    fin = TrackFinish(age_d, predicted=torch.from_numpy(pred).cuda() if opts.get("pred") else None,
+                      mask=torch.from_numpy(mask).cuda() if opts.get("mask") else None, collapse=collapse)
+    finish_tracks(ctx, d, fin, w, h, border)
+    torch.cuda.synchronize()
+    want, wage, walive = oracle.finish_tracks(t, age, w, h, border, pred if opts.get("pred") else None,
+                                              mask if opts.get("mask") else None, collapse)
+    assert_tracks_equal(tracks_from_device(d), want)
+    np.testing.assert_array_equal(age_d.cpu().numpy().astype(np.uint32), wage)
+    assert int(fin.alive_count.item()) == walive
+    # the collapse cells are cleared: a second identical call gives the same result
+    d2 = tracks_to_device(t)
+    age2 = torch.from_numpy(age.astype(np.int32)).cuda()
+    fin2 = TrackFinish(age2, predicted=fin.predicted, mask=fin.mask, collapse=collapse)
+    finish_tracks(ctx, d2, fin2, w, h, border)
+    torch.cuda.synchronize()
+    assert_tracks_equal(tracks_from_device(d2), want)
+
+
+def test_batched_step_with_finish_equals_plain_and_oracle(ctx, oracle):
+    shapes = [(640, 480), (1280, 720), (97, 61)]
+    frames, hosts, ages, prevs, nexts = [], [], [], [], []
+    for i, (w, h) in enumerate(shapes):
+        p, nx, _ = synthetic.frame_pair(i + 70, w, h)
+        pp = ImagePyramid(w, h).build(ctx, torch.from_numpy(p).cuda())
+        xy = Selection(ctx).compute_gftt_and_select_features(pp, 0, 0, 0, 0, None, None, 400).cpu().numpy()
+        t = make_tracks(xy, None, float(w), 0.8)
+        age = np.random.default_rng(i).integers(1, 9, len(t)).astype(np.uint32)
+        hosts.append(t)
+        ages.append(age)
+        prevs.append(p)
+        nexts.append(nx)
+        fin = TrackFinish(torch.from_numpy(age.astype(np.int32)).cuda(), 0.85)
+        frames.append(CameraFrame(torch.from_numpy(nx).cuda(), ImagePyramid(w, h), pp, tracks_to_device(t), 450,
+                                  (2, 2, 2, 2), finish=fin))
+    b = Batch(ctx, frames)
+    b.run()
+    torch.cuda.synchronize()
+    batched = [(tracks_from_device(f.tracks), f.finish.age.cpu().numpy().copy(),
+                f.new_xy[:int(f.new_count.item())].cpu().numpy().copy()) for f in frames]
+    for f, t, a in zip(frames, hosts, ages):
+        f.tracks.copy_(tracks_to_device(t))
+        f.finish.age.copy_(torch.from_numpy(a.astype(np.int32)))
+    b.run_plain()
+    torch.cuda.synchronize()
+    for f, (tb, ab, nb), t, a, p, nx, (w, h) in zip(frames, batched, hosts, ages, prevs, nexts, shapes):
+        assert_tracks_equal(tracks_from_device(f.tracks), tb)
+        np.testing.assert_array_equal(f.finish.age.cpu().numpy(), ab)
+        np.testing.assert_array_equal(f.new_xy[:int(f.new_count.item())].cpu().numpy(), nb)
+        lk = oracle.lk_retrack(oracle.pyramid(p), oracle.pyramid(nx), t, 0.85)
+        want, wage, _ = oracle.finish_tracks(lk, a, w, h, (2, 2, 2, 2))
+        assert_tracks_equal(tb, want)
+        np.testing.assert_array_equal(ab.astype(np.uint32), wage)
