@@ -810,6 +810,28 @@ def main():
     total_units = reduce_sum(attempted, dist, dev)
     value = throughput(total_units, args.steps, ms)
 
+    # ---- the whole MonoSOFGPU frame: the same step plus the retrack pass and the finish filters
+    #      (collect, ages, border kill, collapse) between LK and selection
+    from cuvslam_b200.frontend import TrackFinish
+    fin_frames, fin_ages = [], []
+    for f, p in zip(frames, pristine):
+        age = torch.ones(p.shape[0], dtype=torch.int32, device=dev)
+        fin_ages.append(age)
+        fin_frames.append(CameraFrame(f.image, ImagePyramid(f.image.shape[1], f.image.shape[0], device=dev), f.prev,
+                                      p.clone(), f.num_desired, f.border, finish=TrackFinish(age.clone(), 0.85)))
+    batch_f = Batch(ctx, fin_frames, _lib.FE_SAMPLE_TEXTURE)
+    batch_f.set_tuning(**tuning)
+
+    def step_finish():
+        for f, p, a in zip(fin_frames, pristine, fin_ages):
+            f.tracks.copy_(p, non_blocking=True)
+            f.finish.age.copy_(a, non_blocking=True)
+        batch_f.run(stream)
+
+    ms_fin = timed(step_finish, max(3, args.steps // 2), 2)
+    fin_value = throughput(total_units, max(3, args.steps // 2), ms_fin)
+    fin_alive = sum(int(f.finish.alive_count.item()) for f in fin_frames)
+
     # ---- plain per-camera launch sequence (same work)
     ms_plain = timed(step_plain, max(3, args.steps // 2), 2)
     plain_value = throughput(total_units, max(3, args.steps // 2), ms_plain)
@@ -935,6 +957,9 @@ def main():
                        "tuning": tuning},
             "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain / max(3, args.steps // 2)},
             "batched_over_plain": value / plain_value,
+            "frame_with_finish": {"value": fin_value, "unit": UNIT, "ms_per_step": ms_fin / max(3, args.steps // 2),
+                                  "kernels_per_step": batch_f.kernel_count(), "tracks_alive": fin_alive,
+                                  "what": "the step plus the retrack pass (NCC 0.85) and the finish filters"},
             "parts_ms": part_ms,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "pipeline": "two batches in ping-pong, uploads and downloads on their own streams"},
@@ -950,6 +975,7 @@ def main():
         print(json.dumps(line), flush=True)
     batch.close()
     batch_b.close()
+    batch_f.close()
     ctx.close()
     if dist:
         dist.barrier()
