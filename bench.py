@@ -545,6 +545,70 @@ def config_l2r(ctx, dev, stream, npairs=8):
             "cpu_oracle_ms_one_pair": cpu_ms, "cpu_cores": 1}
 
 
+def config_affine(ctx, dev, stream, n_tracks=8192):
+    """Affine (Shi-Tomasi) tracker: one 1920x1200 frame pair (seeded scene, similarity warp), n_tracks
+    Shi-Tomasi features, 0 shift + 20 full-map steps (GPUSTFeatureTracker(0, 20)).  Times fe_track_affine,
+    fe_affine_build_cache and fe_track_affine_cached on the device (CUDA events, records reset before
+    each call), and the oracle's CPU restatement on a bounded sample (1 core)."""
+    import torch
+
+    from cuvslam_b200 import synthetic
+    from cuvslam_b200.frontend import (ImagePyramid, Selection, STFeatureTracker, STFeatureTrackerWithCache,
+                                       tracks_from_device)
+    from cuvslam_b200.types import make_tracks
+    from oracle import oracle as O
+
+    W, H = 1920, 1200
+    prev, nxt, warp = synthetic.frame_pair(5, W, H)
+    pp = ImagePyramid(W, H, 10, device=dev).build(ctx, torch.from_numpy(prev).to(dev))
+    cp = ImagePyramid(W, H, 10, device=dev).build(ctx, torch.from_numpy(nxt).to(dev))
+    uv = Selection(ctx).compute_gftt_and_select_features(pp, 0, 0, 0, 0, None, None, n_tracks, stream)
+    torch.cuda.synchronize()
+    pts = uv.cpu().numpy().astype(np.float32)
+    gt = synthetic.flow_texture(warp, pts.astype(np.float64)).astype(np.float32)
+    rec = make_tracks(pts, (gt - pts) + np.float32(0.5), 64.0, 0.8)
+    src = torch.from_numpy(rec.view(np.uint8).reshape(len(rec), 80).copy()).to(dev)
+    d = src.clone()
+    st = STFeatureTracker(ctx, 0, 20)
+    stc = STFeatureTrackerWithCache(ctx, 0, 20)
+    cache = stc.build_points_cache(pp, d, stream=stream)
+
+    def dev_ms(fn, reps=20):
+        for _ in range(3):
+            d.copy_(src)
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            d.copy_(src)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            torch.cuda.synchronize()
+            tot += s.elapsed_time(e)
+        return tot / reps
+
+    with torch.cuda.stream(stream):
+        track_ms = dev_ms(lambda: st.track_points(pp, cp, d, stream=stream))
+        out = tracks_from_device(d)
+        build_ms = dev_ms(lambda: stc.build_points_cache(pp, d, cache, stream=stream))
+        cached_ms = dev_ms(lambda: stc.track_points(cp, cache, d, stream=stream))
+    ok = out["track_status"] == 1
+    err = np.linalg.norm(out["track"][ok] - gt[ok], axis=1)
+    opp, ocp = O.pyramid(prev), O.pyramid(nxt)
+    ns = min(512, len(rec))
+    t0 = time.perf_counter()
+    O.st_track(opp, ocp, rec[:ns], 0, 20)
+    cpu_s = time.perf_counter() - t0
+    n = len(rec)
+    return {"workload": f"{W}x{H} frame pair, {n} Shi-Tomasi features, affine tracker 0 shift + 20 full-map steps",
+            "tracks": n, "tracked": int(ok.sum()), "median_err_px_vs_truth": float(np.median(err)) if ok.any() else None,
+            "track_ms": track_ms, "build_cache_ms": build_ms, "track_cached_ms": cached_ms,
+            "tracks_per_s": n / (track_ms / 1e3), "tracks_per_s_cached": n / (cached_ms / 1e3),
+            "cpu_oracle_tracks_per_s": ns / cpu_s, "cpu_sample": f"{ns} tracks, 1 core"}
+
+
 STREAM_CAMS, STREAM_W, STREAM_H, STREAM_TRACKS, STREAM_FRAMES = 32, 1920, 1200, 8192, 30
 
 
@@ -940,6 +1004,7 @@ def main():
         for name, fn in (("1_stereo_plain", lambda: config_stereo_plain(ctx, dev, stream)),
                          ("2_sequence", lambda: config_sequence(ctx, dev, stream, seq_frames)),
                          ("l2r_stereo", lambda: config_l2r(ctx, dev, stream)),
+                         ("affine_st", lambda: config_affine(ctx, dev, stream)),
                          ("5_stream_fwd_bwd", lambda: config_stream(ctx, dev, stream, bases))):
             try:
                 configs[name] = fn()

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libcuvslam_fe.so")
 MAX_LEVELS = 10
 
 FE_OK = 0
+FE_ERR_INVALID_ARGUMENT = 1
 FE_SAMPLE_TEXTURE = 0
 FE_SAMPLE_EXACT = 1
 FE_SAMPLE_TEXTURE_WIDE = 2
@@ -154,6 +155,9 @@ _SIGS = {
     "fe_track_stereo": (_I, [_P, ctypes.POINTER(FeStereoPair), _I, ctypes.c_float, _I, _I, _P]),
     "fe_track_mono": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, ctypes.c_float, _I, _P]),
     "fe_finish_tracks": (_I, [_P, ctypes.POINTER(FeFinishCamera), _I, _P]),
+    "fe_track_affine": (_I, [_P, ctypes.POINTER(FePyramid), ctypes.POINTER(FePyramid), _P, _I, _I, _I, _I, _P]),
+    "fe_affine_build_cache": (_I, [_P, ctypes.POINTER(FePyramid), _P, _I, _P, _I, _P]),
+    "fe_track_affine_cached": (_I, [_P, ctypes.POINTER(FePyramid), _P, _I, _P, _I, _I, _I, _I, _P]),
     "fe_batch_create": (_I, [_P, ctypes.POINTER(FeCameraFrame), _I, _I, ctypes.POINTER(_P)]),
     "fe_batch_run": (_I, [_P, _P]),
     "fe_batch_run_plain": (_I, [_P, _P]),

@@ -637,6 +637,80 @@ int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur
   return FE_OK;
 }
 
+namespace {
+
+int affine_args(fe_context* ctx, const fe_pyramid* cur, fe_track_data* tracks, int n, int n_shift, int n_full,
+                int sampling) {
+  if (!ctx || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
+  if (n_shift < 0 || n_full < 0 || n_shift > 1000 || n_full > 1000) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  for (int l = 0; l < cur->levels; ++l)
+    if (!cur->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
+  if ((uintptr_t)tracks % 16 != 0) return FE_ERR_INVALID_ARGUMENT;
+  return FE_OK;
+}
+
+}  // namespace
+
+int fe_track_affine(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks, int n,
+                    int n_shift_iterations, int n_full_iterations, int sampling, fe_stream stream) {
+  const int rc = affine_args(ctx, cur, tracks, n, n_shift_iterations, n_full_iterations, sampling);
+  if (rc) return rc;
+  if (!valid_pyramid(prev) || prev->levels < cur->levels) return FE_ERR_INVALID_ARGUMENT;
+  for (int l = 0; l < cur->levels; ++l)
+    if (prev->width[l] != cur->width[l] || prev->height[l] != cur->height[l]) return FE_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FE_OK;
+  fe::StLaunch p;
+  memset(&p, 0, sizeof(p));
+  p.prev = to_pyr(*prev);
+  p.cur = to_pyr(*cur);
+  p.tracks = tracks;
+  p.n = n;
+  p.n_shift = n_shift_iterations;
+  p.n_full = n_full_iterations;
+  p.sampling = sampling;
+  FE_CUDA(fe::launch_st(p, 0, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_affine_build_cache(fe_context* ctx, const fe_pyramid* prev, fe_track_data* tracks, int n,
+                          fe_affine_cache* cache, int sampling, fe_stream stream) {
+  if (!ctx || !valid_pyramid(prev) || n < 0 || (n > 0 && (!tracks || !cache))) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  if ((uintptr_t)tracks % 16 != 0 || (uintptr_t)cache % 4 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FE_OK;
+  fe::StLaunch p;
+  memset(&p, 0, sizeof(p));
+  p.prev = to_pyr(*prev);
+  p.tracks = tracks;
+  p.n = n;
+  p.sampling = sampling;
+  p.cache_out = cache;
+  FE_CUDA(fe::launch_st(p, 2, (cudaStream_t)stream));
+  return FE_OK;
+}
+
+int fe_track_affine_cached(fe_context* ctx, const fe_pyramid* cur, const fe_affine_cache* cache, int n_cache,
+                           fe_track_data* tracks, int n, int n_shift_iterations, int n_full_iterations, int sampling,
+                           fe_stream stream) {
+  const int rc = affine_args(ctx, cur, tracks, n, n_shift_iterations, n_full_iterations, sampling);
+  if (rc) return rc;
+  if (n_cache < 0 || (n_cache > 0 && !cache) || (uintptr_t)cache % 4 != 0) return FE_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FE_OK;
+  fe::StLaunch p;
+  memset(&p, 0, sizeof(p));
+  p.cur = to_pyr(*cur);
+  p.tracks = tracks;
+  p.n = n;
+  p.n_shift = n_shift_iterations;
+  p.n_full = n_full_iterations;
+  p.sampling = sampling;
+  p.cache = cache;
+  p.n_cache = n_cache;
+  FE_CUDA(fe::launch_st(p, 1, (cudaStream_t)stream));
+  return FE_OK;
+}
+
 int fe_finish_tracks(fe_context* ctx, const fe_finish_camera* cams, int ncams, fe_stream stream) {
   if (!ctx || !cams || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
   if (ncams > fe::kMaxCams) return FE_ERR_CAPACITY;

@@ -176,6 +176,22 @@ struct FinishBatch {
 
 cudaError_t launch_finish(const FinishBatch& b, cudaStream_t s);
 
+// ---------------------------------------------------------------- affine (Shi-Tomasi) tracker
+struct StLaunch {
+  Pyr prev;                     // image (track, build cache)
+  Pyr cur;                      // image + gradients (track)
+  fe_track_data* tracks;
+  int n;
+  int n_shift, n_full;          // translation-only, then full-map Gauss-Newton steps per level
+  int sampling;
+  const fe_affine_cache* cache; // cached tracking: entries indexed by cache_index
+  int n_cache;
+  fe_affine_cache* cache_out;   // build: n entries
+};
+
+// kind 0: st_track, 1: st_track_with_cache, 2: st_build_cache
+cudaError_t launch_st(const StLaunch& p, int kind, cudaStream_t s);
+
 // ---------------------------------------------------------------- left-to-right matching
 constexpr int kMaxStereoPairs = 16;
 

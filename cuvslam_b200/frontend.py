@@ -168,6 +168,74 @@ class LKFeatureTracker:
         return True
 
 
+AFFINE_CACHE_BYTES = 81 * 10 * 4 + 10 * 4 + 4  # fe_affine_cache (PointCacheData<float, 9>)
+
+
+def _check_tracks(track_data):
+    if track_data.dtype != torch.uint8 or track_data.dim() != 2 or track_data.shape[1] != 80:
+        raise ValueError("track_data must be an (n, 80) uint8 tensor of TrackData records")
+
+
+class STFeatureTracker:
+    """GPUSTFeatureTracker (cuda_modules/st_tracker.cpp:22-78): affine tracking, previous patches
+    sampled from the previous pyramid.  The reference tracker is built with (0, 20)."""
+
+    def __init__(self, ctx, n_shift_only_iterations=0, n_full_mapping_iterations=20,
+                 sampling=_lib.FE_SAMPLE_TEXTURE):
+        self.ctx = ctx
+        self.n_shift = int(n_shift_only_iterations)
+        self.n_full = int(n_full_mapping_iterations)
+        self.sampling = sampling
+
+    def track_points(self, previous_image_pyramid, current_image_pyramid, track_data, num_tracks=None,
+                     stream=None):
+        """Advances `track_data` ((n, 80) uint8 CUDA tensor) in place; asynchronous.  The current
+        pyramid supplies the image and both gradients."""
+        n = track_data.shape[0] if num_tracks is None else int(num_tracks)
+        if n == 0:
+            return True
+        _check_tracks(track_data)
+        _lib.check(self.ctx.lib.fe_track_affine(self.ctx.handle, ctypes.byref(previous_image_pyramid.desc),
+                                                ctypes.byref(current_image_pyramid.desc), _ptr(track_data), n,
+                                                self.n_shift, self.n_full, int(self.sampling),
+                                                _stream_handle(stream)), "fe_track_affine")
+        return True
+
+
+class STFeatureTrackerWithCache(STFeatureTracker):
+    """GPUSTFeatureTrackerWithCache (cuda_modules/st_tracker.cpp:80-160): previous patches built
+    once into a cache ((n, AFFINE_CACHE_BYTES) uint8 tensor), then tracked against it."""
+
+    def build_points_cache(self, previous_image_pyramid, track_data, cache_data=None, num_tracks=None, stream=None):
+        """Fills cache_data[i] from track i and sets its cache_index = i; returns the cache."""
+        n = track_data.shape[0] if num_tracks is None else int(num_tracks)
+        if cache_data is None:
+            cache_data = torch.zeros((max(n, 1), AFFINE_CACHE_BYTES), dtype=torch.uint8, device=track_data.device)
+        if n == 0:
+            return cache_data
+        _check_tracks(track_data)
+        if cache_data.dtype != torch.uint8 or cache_data.dim() != 2 or cache_data.shape[1] != AFFINE_CACHE_BYTES \
+                or cache_data.shape[0] < n:
+            raise ValueError(f"cache_data must be an (>= n, {AFFINE_CACHE_BYTES}) uint8 tensor")
+        _lib.check(self.ctx.lib.fe_affine_build_cache(self.ctx.handle, ctypes.byref(previous_image_pyramid.desc),
+                                                      _ptr(track_data), n, _ptr(cache_data), int(self.sampling),
+                                                      _stream_handle(stream)), "fe_affine_build_cache")
+        return cache_data
+
+    def track_points(self, current_image_pyramid, cache_data, track_data, num_tracks=None, stream=None):
+        n = track_data.shape[0] if num_tracks is None else int(num_tracks)
+        if n == 0:
+            return True
+        _check_tracks(track_data)
+        if cache_data.dtype != torch.uint8 or cache_data.dim() != 2 or cache_data.shape[1] != AFFINE_CACHE_BYTES:
+            raise ValueError(f"cache_data must be an (m, {AFFINE_CACHE_BYTES}) uint8 tensor")
+        _lib.check(self.ctx.lib.fe_track_affine_cached(self.ctx.handle, ctypes.byref(current_image_pyramid.desc),
+                                                       _ptr(cache_data), cache_data.shape[0], _ptr(track_data), n,
+                                                       self.n_shift, self.n_full, int(self.sampling),
+                                                       _stream_handle(stream)), "fe_track_affine_cached")
+        return True
+
+
 class Selection:
     """GPUSelection: Shi-Tomasi response + deterministic feature selection on pyramid level 0."""
 

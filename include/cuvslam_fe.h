@@ -198,6 +198,41 @@ FE_API int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyram
                          int n, float retrack_ncc, int sampling, fe_stream stream);
 
 /* ---------------------------------------------------------------------------------------- */
+/* Affine (Shi-Tomasi) tracker                                                               */
+/* ---------------------------------------------------------------------------------------- */
+
+/* cuvslam::cuda::PointCacheData<float, 9> (cuda_kernels.h:68-74), byte-for-byte: a track's
+ * previous-frame 9x9 patches on up to FE_MAX_LEVELS levels (81 floats per level, row-major), their
+ * sums, and the mask of the levels whose patch lies inside the image. */
+typedef struct {
+  float patch[81 * FE_MAX_LEVELS];
+  float patch_sums[FE_MAX_LEVELS];
+  uint32_t level_mask;
+} fe_affine_cache;
+
+/* st_track (st_tracker.cu:1397-1409, kernel st_track_kernel st_tracker.cu:320-814; host wrapper
+ * GPUSTFeatureTracker::track_points, cuda_modules/st_tracker.cpp:24-78): affine tracking of n
+ * tracks from `prev` (image) to `cur` (image + gradients), in place.  n_shift_iterations
+ * translation-only Gauss-Newton steps, then n_full_iterations steps of the full 2x2 map + shift
+ * (the reference's GPUSTFeatureTracker runs 0 and 20).  Uses the records' offset (predicted
+ * motion), initial_guess_map (row-major 2x2; identity for a plain track), search_radius_px and
+ * ncc_threshold; writes track, track_status, info and, when tracked, ncc.  One warp per track. */
+FE_API int fe_track_affine(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks,
+                           int n, int n_shift_iterations, int n_full_iterations, int sampling, fe_stream stream);
+
+/* st_build_cache (st_tracker.cu:1386-1395, kernel st_tracker.cu:1298-1371): each track's
+ * previous-frame patches from `prev` into cache[i] and cache_index = i.  cache holds n entries. */
+FE_API int fe_affine_build_cache(fe_context* ctx, const fe_pyramid* prev, fe_track_data* tracks, int n,
+                                 fe_affine_cache* cache, int sampling, fe_stream stream);
+
+/* st_track_with_cache (st_tracker.cu:1373-1384, kernel st_tracker.cu:816-1296): as fe_track_affine
+ * with the previous patches read from cache[tracks[i].cache_index] (-1: not tracked).  `cache`
+ * holds n_cache entries; a track whose cache_index is outside [0, n_cache) is not tracked. */
+FE_API int fe_track_affine_cached(fe_context* ctx, const fe_pyramid* cur, const fe_affine_cache* cache, int n_cache,
+                                  fe_track_data* tracks, int n, int n_shift_iterations, int n_full_iterations,
+                                  int sampling, fe_stream stream);
+
+/* ---------------------------------------------------------------------------------------- */
 /* Track filters after LK (MonoSOFGPU::finish, on the device)                                */
 /* ---------------------------------------------------------------------------------------- */
 

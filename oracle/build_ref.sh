@@ -15,12 +15,12 @@ if [ ! -d "$K" ]; then
 fi
 mkdir -p "$HERE/_ref"
 OUT="$HERE/_ref/libcuvslam_ref.so"
-if [ -f "$OUT" ] && [ "$OUT" -nt "$HERE/ref_harness.cu" ] && [ "$OUT" -nt "$K/lk_tracker.cu" ]; then
+if [ -f "$OUT" ] && [ "$OUT" -nt "$HERE/ref_harness.cu" ] && [ "$OUT" -nt "$K/lk_tracker.cu" ] && [ "$OUT" -nt "$HERE/build_ref.sh" ]; then
   exit 0
 fi
 nvcc -gencode arch=compute_100a,code=sm_100a -O3 -DNDEBUG -std=c++17 -lineinfo \
   -Xcompiler -fPIC -shared -I "$REF/libs" \
   "$K/image_cast.cu" "$K/image_pyramid.cu" "$K/convolutions.cu" "$K/gftt.cu" \
-  "$K/selection_v2.cu" "$K/sort.cu" "$K/lk_tracker.cu" \
+  "$K/selection_v2.cu" "$K/sort.cu" "$K/lk_tracker.cu" "$K/st_tracker.cu" \
   "$HERE/ref_harness.cu" -o "$HERE/_ref/libcuvslam_ref.so"
 echo "built $HERE/_ref/libcuvslam_ref.so"

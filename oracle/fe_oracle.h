@@ -86,6 +86,24 @@ void or_stereo_scan(int levels, const int* ws, const int* hs, const float* const
                     float search_radius, float ncc_threshold, float early_exit_fraction, int horizontal, int mode,
                     or_track_data* out, int32_t* winner, int32_t* stats);
 
+/* Affine (Shi-Tomasi) tracker (st_oracle.c): st_track_kernel, st_build_cache_kernel and
+ * st_track_with_cache_kernel (libs/cuda_modules/cuda_kernels/st_tracker.cu).  The cache entry is
+ * PointCacheData<float, 9> (cuda_kernels.h:68-74). */
+typedef struct {
+  float patch[81 * 10];
+  float patch_sums[10];
+  uint32_t level_mask;
+} or_st_cache;
+int or_st_qr_solve(int D, const float* a, const float* b, float* x);
+void or_st_track(int levels, const int* ws, const int* hs, const float* const* prev_img, const float* const* cur_img,
+                 const float* const* cur_gx, const float* const* cur_gy, or_track_data* td, int n, int n_shift,
+                 int n_full, int mode);
+void or_st_track_cached(int levels, const int* ws, const int* hs, const float* const* cur_img,
+                        const float* const* cur_gx, const float* const* cur_gy, const or_st_cache* cache,
+                        or_track_data* td, int n, int n_shift, int n_full, int mode);
+void or_st_build_cache(int levels, const int* ws, const int* hs, const float* const* prev_img, or_track_data* td, int n,
+                       or_st_cache* cache, int mode);
+
 /* FP64 differentiable LK tracker and its adjoint (lk_adjoint64.c). */
 enum { OR64_IMPLICIT = 0, OR64_UNROLLED = 1 };
 typedef struct or64_cam or64_cam;

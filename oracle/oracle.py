@@ -38,6 +38,11 @@ def lib():
         L.or_gauss_downscale.argtypes = [P, I, I, P, I, I]
         L.or_rgb_to_gray.argtypes = [P, I, I, ctypes.c_int64, P, I]
         L.or_finish_tracks.argtypes = [P, P, I, P, I, I, P, P, ctypes.c_int64, I]
+        L.or_st_qr_solve.argtypes = [I, P, P, P]
+        L.or_st_qr_solve.restype = I
+        L.or_st_track.argtypes = [I, P, P, P, P, P, P, P, I, I, I, I]
+        L.or_st_track_cached.argtypes = [I, P, P, P, P, P, P, P, I, I, I, I]
+        L.or_st_build_cache.argtypes = [I, P, P, P, P, I, P, I]
         L.or_finish_tracks.restype = I
         L.or_box3.argtypes = [P, I, I, P]
         L.or_gradients.argtypes = [P, I, I, P, P]
@@ -280,6 +285,62 @@ def finish_tracks(tracks, age, width, height, border=(0, 0, 0, 0), pred=None, ma
     alive = lib().or_finish_tracks(_p(t), _p(a), len(t), pp, int(width), int(height), _p(b), mp, mpitch,
                                    int(bool(collapse)))
     return t, a, alive
+
+
+ST_CACHE_DTYPE = np.dtype([("patch", np.float32, (810,)), ("patch_sums", np.float32, (10,)),
+                           ("level_mask", np.uint32)])
+
+
+def _sizes(pyr):
+    levels = len(pyr)
+    ws = np.array([p[0].shape[1] for p in pyr] + [0] * (10 - levels), np.int32)
+    hs = np.array([p[0].shape[0] for p in pyr] + [0] * (10 - levels), np.int32)
+    return levels, ws, hs
+
+
+def st_track(prev_pyr, cur_pyr, tracks, n_shift=0, n_full=20, mode=TEXTURE):
+    """The affine tracker (or_st_track): previous patches from prev_pyr's images, current image and
+    gradients from cur_pyr.  Returns updated copies of the TRACK_DTYPE records."""
+    t = np.ascontiguousarray(tracks.copy())
+    levels, ws, hs = _sizes(prev_pyr)
+    k1, pim = _level_ptrs([p[0] for p in prev_pyr])
+    k2, cim = _level_ptrs([p[0] for p in cur_pyr[:levels]])
+    k3, cgx = _level_ptrs([p[1] for p in cur_pyr[:levels]])
+    k4, cgy = _level_ptrs([p[2] for p in cur_pyr[:levels]])
+    lib().or_st_track(levels, _p(ws), _p(hs), pim, cim, cgx, cgy, _p(t), len(t), n_shift, n_full, mode)
+    del k1, k2, k3, k4
+    return t
+
+
+def st_build_cache(prev_pyr, tracks, mode=TEXTURE):
+    """(tracks with cache_index set, cache entries) as st_build_cache_kernel makes them."""
+    t = np.ascontiguousarray(tracks.copy())
+    levels, ws, hs = _sizes(prev_pyr)
+    k1, pim = _level_ptrs([p[0] for p in prev_pyr])
+    cache = np.zeros(max(len(t), 1), ST_CACHE_DTYPE)
+    lib().or_st_build_cache(levels, _p(ws), _p(hs), pim, _p(t), len(t), _p(cache), mode)
+    del k1
+    return t, cache[:len(t)]
+
+
+def st_track_cached(cur_pyr, cache, tracks, n_shift=0, n_full=20, mode=TEXTURE):
+    t = np.ascontiguousarray(tracks.copy())
+    levels, ws, hs = _sizes(cur_pyr)
+    k2, cim = _level_ptrs([p[0] for p in cur_pyr])
+    k3, cgx = _level_ptrs([p[1] for p in cur_pyr])
+    k4, cgy = _level_ptrs([p[2] for p in cur_pyr])
+    cache = np.ascontiguousarray(cache, ST_CACHE_DTYPE)
+    lib().or_st_track_cached(levels, _p(ws), _p(hs), cim, cgx, cgy, _p(cache), _p(t), len(t), n_shift, n_full, mode)
+    del k2, k3, k4
+    return t
+
+
+def st_qr_solve(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    x = np.zeros(len(b), np.float32)
+    ok = lib().or_st_qr_solve(len(b), _p(a), _p(b), _p(x))
+    return bool(ok), x
 
 
 def stereo_scan(prim_pyr, sec_pyr, uv, cand_off, cand_xy, valid=None, search_radius=48.0, ncc_threshold=0.8,

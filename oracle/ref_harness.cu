@@ -413,6 +413,45 @@ int ref_lk(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int ma
   return 0;
 }
 
+// GPUSTFeatureTracker::track_points (cached = 0) or GPUSTFeatureTrackerWithCache's
+// build_points_cache + track_points (cached = 1) between the pyramids of two u8 images
+// (cuda_modules/st_tracker.cpp:27-160): the current pyramid's image and gradients, the previous
+// pyramid's image.  `tracks` (n TrackData records) is updated in place; with cached = 1 and
+// cache_out != null the n PointCacheData entries (3284 bytes each) are copied out as well.
+int ref_st_track(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int max_levels, void* tracks, int n,
+                 int n_shift, int n_full, int cached, void* cache_out) {
+  int rc = init_tables();
+  if (rc) return rc;
+  HCHECK(init_st_tracker());
+  if (sizeof(TrackData) != 80 || sizeof(PointCacheDataT) != 3284) return -1;
+  Pyr pp, cp;
+  rc = build(prev_img, w, h, max_levels, pp, 0);
+  if (rc) return rc;
+  rc = build(cur_img, w, h, max_levels, cp, 0);
+  if (rc) return rc;
+  TrackData* d = nullptr;
+  PointCacheDataT* c = nullptr;
+  HCHECK(cudaMalloc((void**)&d, sizeof(TrackData) * (size_t)(n > 0 ? n : 1)));
+  HCHECK(cudaMalloc((void**)&c, sizeof(PointCacheDataT) * (size_t)(n > 0 ? n : 1)));
+  HCHECK(cudaMemset(c, 0, sizeof(PointCacheDataT) * (size_t)(n > 0 ? n : 1)));
+  HCHECK(cudaMemcpy(d, tracks, sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
+  Pyramid cgx = make_pyr(cp, cp.gx), cgy = make_pyr(cp, cp.gy), pi = make_pyr(pp, pp.img), ci = make_pyr(cp, cp.img);
+  if (n > 0) {
+    if (cached) {
+      HCHECK(st_build_cache(pi, d, c, (size_t)n, 0));
+      HCHECK(st_track_with_cache(cgx, cgy, ci, c, d, n, (unsigned)n_shift, (unsigned)n_full, 0));
+    } else {
+      HCHECK(st_track(cgx, cgy, pi, ci, d, n, (unsigned)n_shift, (unsigned)n_full, 0));
+    }
+  }
+  HCHECK(cudaDeviceSynchronize());
+  HCHECK(cudaMemcpy(tracks, d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToHost));
+  if (cached && cache_out) HCHECK(cudaMemcpy(cache_out, c, sizeof(PointCacheDataT) * (size_t)n, cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  cudaFree(c);
+  return 0;
+}
+
 // MultiSOFGPU::LaunchTrackingPrimaryToSecondary's scan between the pyramids of a primary and a
 // secondary u8 image: one lk_track_horizontal (or lk_track) launch per candidate index k over all n points, a copy
 // back and a synchronisation, first success wins, early exit once matched >= frac * n.  Candidates

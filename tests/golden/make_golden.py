@@ -16,6 +16,8 @@ The committed tests/golden/reference.npz is the step-2 output.
 `stereo-reference --out DIR` runs the reference's multi-launch left-to-right scan
 (lk_track_horizontal per candidate round, oracle/ref_harness.cu) on stereo_inputs.npz and writes
 DIR/stereo_reference.npz.
+`st-reference --out DIR` runs the reference's affine tracker (st_track, st_build_cache +
+st_track_with_cache; oracle/ref_harness.cu ref_st_track) and writes DIR/st_reference.npz.
 """
 
 import argparse
@@ -314,9 +316,95 @@ def make_input_reference(out_dir):
     print("wrote input_reference.npz")
 
 
+# Affine (Shi-Tomasi) tracker fixtures: the reference's st_track / st_build_cache +
+# st_track_with_cache (oracle/ref_harness.cu ref_st_track) on the inputs.npz pairs, from the
+# selected points of reference.npz, and on one strongly rotated and scaled pair drawn here
+# (st_frames, "rot").
+ST_CASES = ("c1", "half", "odd")
+ST_ROT_WARP = (0.12, 1.08, 3.0, -2.0)  # theta, scale, tx, ty about the frame centre
+ST_CACHE_KEEP = 8  # cache entries stored whole per case
+
+
+def st_frames(name, inp=None):
+    """(prev, next, Similarity) of an affine-tracker case."""
+    if name == "rot":
+        w, h = 376, 240
+        scene = synthetic.Scene.draw(1101, w, h)
+        warp = synthetic.Similarity(*ST_ROT_WARP, cx=(w - 1) / 2.0, cy=(h - 1) / 2.0)
+        prev = synthetic.quantise(scene.render())
+        nxt = synthetic.quantise(scene.render(warp), np.random.default_rng(3101), 2.0)
+        return prev, nxt, warp
+    wp = inp[f"{name}/warp"]
+    return inp[f"{name}/prev"], inp[f"{name}/next"], synthetic.Similarity(*[float(v) for v in wp])
+
+
+def st_points(name, ref, prev):
+    if name == "rot":
+        h, w = prev.shape
+        rng = np.random.default_rng(44)
+        return np.stack([rng.uniform(12, w - 12, 300), rng.uniform(12, h - 12, 300)], 1).astype(np.float32)
+    return ref[f"{name}/sel0/sel"].astype(np.float32)
+
+
+def st_runs(name, prev, warp, pts):
+    """name -> (records, n_shift, n_full, cached)."""
+    h, w = prev.shape
+    gt = synthetic.flow_texture(warp, pts.astype(np.float64)).astype(np.float32)
+    rng = np.random.default_rng(6)
+    pred = gt + rng.normal(0.0, 0.7, gt.shape).astype(np.float32)
+    lin = warp._mat().astype(np.float32).reshape(-1)
+    mapped = make_tracks(pts, pred - pts, float(w), 0.8)
+    mapped["initial_guess_map"] = lin
+    runs = {
+        "st_pred": (make_tracks(pts, pred - pts, float(w), 0.8), 0, 20, 0),
+        "st_map": (mapped, 0, 20, 0),
+        "st_cached": (make_tracks(pts, pred - pts, float(w), 0.8), 0, 20, 1),
+    }
+    if name != "rot":
+        runs["st_zero"] = (make_tracks(pts, None, float(w), 0.8), 0, 20, 0)
+        runs["st_mixed"] = (make_tracks(pts, pred - pts, 7.0, 0.8), 10, 10, 0)
+    return runs, gt
+
+
+def make_st_reference(out_dir):
+    lib = _lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.ref_st_track.argtypes = [P, P, I, I, I, P, I, I, I, I, P]
+    inp = np.load(os.path.join(HERE, "inputs.npz"))
+    ref = np.load(os.path.join(HERE, "reference.npz"))
+    compact = {}
+    for name in ST_CASES + ("rot",):
+        prev, nxt, warp = st_frames(name, inp)
+        h, w = prev.shape
+        pts = st_points(name, ref, prev)
+        runs, gt = st_runs(name, prev, warp, pts)
+        compact[f"{name}/gt"] = gt
+        for tag, (t, ns, nf, cached) in runs.items():
+            out = np.ascontiguousarray(t.copy())
+            cache = np.zeros((max(len(t), 1), 3284), np.uint8)
+            rc = lib.ref_st_track(_ptr(np.ascontiguousarray(prev)), _ptr(np.ascontiguousarray(nxt)), w, h, 10,
+                                  _ptr(out), len(out), ns, nf, cached, _ptr(cache))
+            assert rc == 0, rc
+            compact[f"{name}/{tag}/in"] = t
+            compact[f"{name}/{tag}/out"] = out
+            if cached:
+                c = cache[:len(t)]
+                compact[f"{name}/{tag}/cache_head"] = c[:ST_CACHE_KEEP].copy()
+                compact[f"{name}/{tag}/patch_sums"] = c[:, 3240:3280].copy().view(np.float32)
+                compact[f"{name}/{tag}/level_mask"] = c[:, 3280:3284].copy().view(np.uint32).reshape(-1)
+        if name == "rot":
+            compact["rot/prev"] = prev
+            compact["rot/next"] = nxt
+        print(name, {k: int((v[0]["track_status"] != 0).sum()) for k, v in runs.items()})
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "st_reference.npz"), **compact)
+    print("wrote st_reference.npz")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference", "input-reference"])
+    ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference", "input-reference",
+                                        "st-reference"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if a.step == "inputs":
@@ -327,5 +415,7 @@ if __name__ == "__main__":
         make_stereo_reference(a.out)
     elif a.step == "input-reference":
         make_input_reference(a.out)
+    elif a.step == "st-reference":
+        make_st_reference(a.out)
     else:
         make_reference(a.out)
