@@ -669,6 +669,7 @@ int fe_track_affine(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* c
   p.n_shift = n_shift_iterations;
   p.n_full = n_full_iterations;
   p.sampling = sampling;
+  p.counter = ctx->lk_counter + 32;
   FE_CUDA(fe::launch_st(p, 0, (cudaStream_t)stream));
   return FE_OK;
 }
@@ -707,6 +708,7 @@ int fe_track_affine_cached(fe_context* ctx, const fe_pyramid* cur, const fe_affi
   p.sampling = sampling;
   p.cache = cache;
   p.n_cache = n_cache;
+  p.counter = ctx->lk_counter + 32;
   FE_CUDA(fe::launch_st(p, 1, (cudaStream_t)stream));
   return FE_OK;
 }

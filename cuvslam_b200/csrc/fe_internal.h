@@ -187,6 +187,7 @@ struct StLaunch {
   const fe_affine_cache* cache; // cached tracking: entries indexed by cache_index
   int n_cache;
   fe_affine_cache* cache_out;   // build: n entries
+  int* counter;                 // tracking: persistent warps' track counter (zeroed by the launch)
 };
 
 // kind 0: st_track, 1: st_track_with_cache, 2: st_build_cache

@@ -81,7 +81,7 @@ int or_st_qr_solve(int D, const float* a, const float* b, float* x) {
         mc = c;
       }
     if (nzp == D && mn * mn < th * (float)(D - q)) nzp = q;
-    if (q != mc) {
+    if (mc >= 0 && q != mc) { /* mc < 0: no column norm above -1 (all NaN), nothing to swap */
       int t = perm[q];
       perm[q] = perm[mc];
       perm[mc] = t;
