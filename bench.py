@@ -49,10 +49,12 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other BASELINE configs (stereo plain, 100-frame sequence, fwd+bwd stream)")
-    ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled"], default=None,
+    ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled", "affine"],
+                    default=None,
                     help="for an ncu capture: run only this part of the step (inside NVTX ranges named "
                          "'part'), whole batched steps (ranges named 'step'), or the LK adjoint workload's "
-                         "forward and backward in one mode (ranges 'fwd', 'bwd'), warmup + steps times")
+                         "forward and backward in one mode (ranges 'fwd', 'bwd'), warmup + steps times, or "
+                         "the affine tracker's workload alone")
     return ap.parse_args()
 
 
@@ -768,6 +770,20 @@ def profile_adjoint(args, local):
     ctx.close()
 
 
+def profile_affine(args, local):
+    """The affine-tracker workload alone (2048 Shi-Tomasi features of one 1920x1200 pair), for an ncu
+    capture of st_track_kernel; prints the config's JSON."""
+    import torch
+
+    from cuvslam_b200.frontend import Context
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    r = config_affine(ctx, torch.device("cuda", local), torch.cuda.Stream(), n_tracks=2048)
+    print(json.dumps({"profile": "affine", **r}))
+    ctx.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -778,6 +794,8 @@ def main():
 
     if args.profile in ("implicit", "unrolled"):
         return profile_adjoint(args, local)
+    if args.profile == "affine":
+        return profile_affine(args, local)
     shapes, counts, prevs, nexts = workload(seed_offset=rank)
     want_configs = rank == 0 and world == 1 and not args.no_configs
     seq_frames = sequence_frames() if want_configs else None

@@ -216,7 +216,9 @@ typedef struct {
  * translation-only Gauss-Newton steps, then n_full_iterations steps of the full 2x2 map + shift
  * (the reference's GPUSTFeatureTracker runs 0 and 20).  Uses the records' offset (predicted
  * motion), initial_guess_map (row-major 2x2; identity for a plain track), search_radius_px and
- * ncc_threshold; writes track, track_status, info and, when tracked, ncc.  One warp per track. */
+ * ncc_threshold; writes track, track_status, info and, when tracked, ncc.  Persistent warps take
+ * tracks from a counter the context owns: affine tracking calls on one context must not overlap on
+ * the GPU (use one stream per context). */
 FE_API int fe_track_affine(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_track_data* tracks,
                            int n, int n_shift_iterations, int n_full_iterations, int sampling, fe_stream stream);
 
