@@ -3,7 +3,7 @@
  * The library replaces the hot path that cuVSLAM's MonoSOFGPU drives through four host wrappers
  * and the C-style kernel launchers of libs/cuda_modules:
  *   Gaussian image pyramid + gradient pyramid, Shi-Tomasi (GFTT) response and feature selection,
- *   and pyramidal Lucas-Kanade tracking,
+ *   pyramidal Lucas-Kanade tracking, and the affine (Shi-Tomasi) tracker,
  * with results equal to the reference GPU path (see each entry point).  All entry points:
  *   - take device pointers, sizes in elements/pixels and pitches in BYTES;
  *   - enqueue work on the caller's stream and return without synchronising, unless stated;
