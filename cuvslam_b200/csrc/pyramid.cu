@@ -680,13 +680,6 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
     const int y = 4 * Y2 + (q >> 5), x = 4 * X2 + (q & 31) * 4;
     if (y >= h0 || x >= w0) continue;
     const int r = y - a0y, c = x - a0x;
-    float2 v[6];  // horizontal neighbours x-4 .. x+7 as pairs
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c - 4 + 4 * k);
-      v[2 * k] = bytes_to_float2(wd, 0);
-      v[2 * k + 1] = bytes_to_float2(wd, 2);
-    }
     float2 col[7][2];  // rows y-3 .. y+3, pixel pairs (x, x+1) and (x+2, x+3)
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
@@ -694,6 +687,11 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
       col[k][0] = bytes_to_float2(wd, 0);
       col[k][1] = bytes_to_float2(wd, 2);
     }
+    // horizontal neighbours x-4 .. x+7 as pairs; the middle word is row y of the column window
+    const uint32_t wl = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c - 4);
+    const uint32_t wr = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c + 4);
+    const float2 v[6] = {bytes_to_float2(wl, 0), bytes_to_float2(wl, 2), col[3][0],
+                         col[3][1],              bytes_to_float2(wr, 0), bytes_to_float2(wr, 2)};
     // pixel x+i needs v at flat indices 1+i+j (j = 0..6); pairs (i, i+1) for i = 0, 2
     auto hv = [&](int f) { return (f & 1) ? make_float2(v[f >> 1].y, v[(f >> 1) + 1].x) : v[f >> 1]; };
     float2 gx2[2], gy2[2];
