@@ -452,6 +452,92 @@ int ref_st_track(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, 
   return 0;
 }
 
+// Device time (CUDA events, mean over `reps` after 3 warm-up runs) of one reference GPU stage on
+// the pyramids of two u8 images: which = 0 the current frame's pyramid (cast_image, gaussian_scaling
+// per level, conv_grad_x/y per level, as build() enqueues them; allocations excluded); 1 lk_track;
+// 2 st_track (n_shift, n_full); 3 st_track_with_cache after st_build_cache.  Tracks are reset from
+// the caller's n records before every run (the copy is outside the timed interval).
+int ref_time_stage(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int max_levels, const void* tracks,
+                   int n, int which, int n_shift, int n_full, int reps, float* ms_out) {
+  int rc = init_tables();
+  if (rc) return rc;
+  HCHECK(init_st_tracker());
+  Pyr pp, cp;
+  rc = build(prev_img, w, h, max_levels, pp, 0);
+  if (rc) return rc;
+  rc = build(cur_img, w, h, max_levels, cp, 0);
+  if (rc) return rc;
+  TrackData *d = nullptr, *d0 = nullptr;
+  PointCacheDataT* c = nullptr;
+  const size_t nb = sizeof(TrackData) * (size_t)(n > 0 ? n : 1);
+  HCHECK(cudaMalloc((void**)&d, nb));
+  HCHECK(cudaMalloc((void**)&d0, nb));
+  HCHECK(cudaMalloc((void**)&c, sizeof(PointCacheDataT) * (size_t)(n > 0 ? n : 1)));
+  if (n > 0) HCHECK(cudaMemcpy(d0, tracks, sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
+  uint8_t* d_u8 = nullptr;
+  size_t u8_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&d_u8, &u8_pitch, w, h));
+  HCHECK(cudaMemcpy2D(d_u8, u8_pitch, cur_img, w, w, h, cudaMemcpyHostToDevice));
+  DevImage cast;
+  HCHECK(cast.alloc(w, h));
+  Pyramid pgx = make_pyr(pp, pp.gx), pgy = make_pyr(pp, pp.gy), pi = make_pyr(pp, pp.img);
+  Pyramid cgx = make_pyr(cp, cp.gx), cgy = make_pyr(cp, cp.gy), ci = make_pyr(cp, cp.img);
+  cudaStream_t s = 0;
+  if (which == 3 && n > 0) {
+    HCHECK(cudaMemcpy(d, d0, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToDevice));
+    HCHECK(st_build_cache(pi, d, c, (size_t)n, s));
+    HCHECK(cudaMemcpy(d0, d, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToDevice));  // cache_index set
+  }
+  auto run = [&]() -> int {
+    if (which == 0) {
+      HCHECK(cast_image(d_u8, u8_pitch, cast.ptr, cast.pitch, {(unsigned)w, (unsigned)h}, s));
+      HCHECK(cudaMemcpy2DAsync(cp.img[0]->ptr, cp.img[0]->pitch, cast.ptr, cast.pitch, (size_t)w * 4, h,
+                               cudaMemcpyDeviceToDevice, s));
+      for (int l = 0; l + 1 < cp.n; ++l) {
+        const DevImage& a = *cp.img[l];
+        DevImage& b = *cp.img[l + 1];
+        HCHECK(gaussian_scaling(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, b.ptr, b.pitch,
+                                {(unsigned)b.w, (unsigned)b.h}, s));
+      }
+      for (int l = 0; l < cp.n; ++l) {
+        const DevImage& a = *cp.img[l];
+        HCHECK(conv_grad_x(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, cp.gx[l]->ptr, cp.gx[l]->pitch, s));
+        HCHECK(conv_grad_y(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, cp.gy[l]->ptr, cp.gy[l]->pitch, s));
+      }
+    } else if (which == 1) {
+      HCHECK(lk_track(pgx, pgy, pi, ci, d, n, s));
+    } else if (which == 2) {
+      HCHECK(st_track(cgx, cgy, pi, ci, d, n, (unsigned)n_shift, (unsigned)n_full, s));
+    } else {
+      HCHECK(st_track_with_cache(cgx, cgy, ci, c, d, n, (unsigned)n_shift, (unsigned)n_full, s));
+    }
+    return 0;
+  };
+  cudaEvent_t e0, e1;
+  HCHECK(cudaEventCreate(&e0));
+  HCHECK(cudaEventCreate(&e1));
+  float total = 0.f;
+  for (int r = 0; r < reps + 3; ++r) {
+    if (n > 0 && which != 0) HCHECK(cudaMemcpyAsync(d, d0, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    HCHECK(cudaEventRecord(e0, s));
+    rc = run();
+    if (rc) return rc;
+    HCHECK(cudaEventRecord(e1, s));
+    HCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    HCHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (r >= 3) total += ms;
+  }
+  *ms_out = total / (float)(reps > 0 ? reps : 1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  cudaFree(d0);
+  cudaFree(c);
+  cudaFree(d_u8);
+  return 0;
+}
+
 // MultiSOFGPU::LaunchTrackingPrimaryToSecondary's scan between the pyramids of a primary and a
 // secondary u8 image: one lk_track_horizontal (or lk_track) launch per candidate index k over all n points, a copy
 // back and a synchronisation, first success wins, early exit once matched >= frac * n.  Candidates
