@@ -20,6 +20,7 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -535,6 +536,138 @@ int ref_time_stage(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h
   cudaFree(d0);
   cudaFree(c);
   cudaFree(d_u8);
+  return 0;
+}
+
+// Host wall-clock time (mean over `reps` after 2 warm-up runs) of one camera's frame through the
+// reference's GPU path on one stream, as MonoSOFGPU runs it: the current frame's pyramid and
+// gradients from a uint8 frame in device memory (cast_image, gaussian_scaling, conv_grad_x/y), LK of
+// n tracks from the previous pyramid (lk_track; records reset before each run, outside the timed
+// interval), then GPUSelection::computeGFTTAndSelectFeatures with the n track positions alive:
+// gftt_values, accumulateGFTT, non_max_suppression, filter_maximums, downsample_gftt_x8,
+// select_features, the count read back, sort_keypoints, the keypoints read back and the host quota
+// loop for num_desired features (selection_v2.cpp:27-184).  Allocations happen before timing.
+int ref_time_frame(const uint8_t* prev_img, const uint8_t* cur_img, int w, int h, int max_levels, const void* tracks,
+                   int n, int num_desired, int reps, float* ms_out) {
+  int rc = init_tables();
+  if (rc) return rc;
+  Pyr pp, cp;
+  rc = build(prev_img, w, h, max_levels, pp, 0);
+  if (rc) return rc;
+  rc = build(cur_img, w, h, max_levels, cp, 0);
+  if (rc) return rc;
+  cudaStream_t s = 0;
+  TrackData *d = nullptr, *d0 = nullptr;
+  const size_t nb = sizeof(TrackData) * (size_t)(n > 0 ? n : 1);
+  HCHECK(cudaMalloc((void**)&d, nb));
+  HCHECK(cudaMalloc((void**)&d0, nb));
+  if (n > 0) HCHECK(cudaMemcpy(d0, tracks, sizeof(TrackData) * (size_t)n, cudaMemcpyHostToDevice));
+  std::vector<TrackData> host_td((size_t)(n > 0 ? n : 1));
+  if (n > 0) memcpy(host_td.data(), tracks, sizeof(TrackData) * (size_t)n);
+  uint8_t* d_u8 = nullptr;
+  size_t u8_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&d_u8, &u8_pitch, w, h));
+  HCHECK(cudaMemcpy2D(d_u8, u8_pitch, cur_img, w, w, h, cudaMemcpyHostToDevice));
+  DevImage cast, val, maxim, dsm;
+  HCHECK(cast.alloc(w, h));
+  const uint2 size = {(unsigned)w, (unsigned)h};
+  const uint2 bin_size = {(unsigned)(w / 8), (unsigned)(h / 8)};
+  const uint2 num_bins = {8, 8};
+  const uint2 ds = {(unsigned)w / 8, (unsigned)h / 8};
+  const int max_tracks = (int)(ds.x * ds.y);
+  HCHECK(val.alloc(w, h));
+  HCHECK(maxim.alloc(w, h));
+  HCHECK(dsm.alloc((int)ds.x, (int)ds.y));
+  uint2* idx = nullptr;
+  size_t idx_pitch = 0;
+  HCHECK(cudaMallocPitch((void**)&idx, &idx_pitch, ds.x * sizeof(uint2), ds.y));
+  Keypoint* kp = nullptr;
+  HCHECK(cudaMalloc((void**)&kp, sizeof(Keypoint) * (size_t)(max_tracks > 0 ? max_tracks : 1)));
+  float* bins = nullptr;
+  HCHECK(cudaMalloc((void**)&bins, sizeof(float) * 66));
+  size_t tmp_bytes = sort_keypoints_get_temp_buffer_size((size_t)max_tracks);
+  void* tmp = nullptr;
+  HCHECK(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 1));
+  std::vector<Keypoint> alive((size_t)(max_tracks > 0 ? max_tracks : 1)), host_kp(alive.size());
+  const int n_old = n < max_tracks ? n : max_tracks;
+  for (int i = 0; i < n_old; ++i) alive[i] = {host_td[i].track.x, host_td[i].track.y, 0.f};
+  Pyramid pgx = make_pyr(pp, pp.gx), pgy = make_pyr(pp, pp.gy), pi = make_pyr(pp, pp.img), ci = make_pyr(cp, cp.img);
+  std::vector<float> sel((size_t)2 * (num_desired > 0 ? num_desired : 1));
+  double total = 0.0;
+  for (int r = 0; r < reps + 2; ++r) {
+    if (n > 0) HCHECK(cudaMemcpy(d, d0, sizeof(TrackData) * (size_t)n, cudaMemcpyDeviceToDevice));
+    HCHECK(cudaDeviceSynchronize());
+    const auto t0 = std::chrono::steady_clock::now();
+    // pyramid + gradients
+    HCHECK(cast_image(d_u8, u8_pitch, cast.ptr, cast.pitch, size, s));
+    HCHECK(cudaMemcpy2DAsync(cp.img[0]->ptr, cp.img[0]->pitch, cast.ptr, cast.pitch, (size_t)w * 4, h,
+                             cudaMemcpyDeviceToDevice, s));
+    for (int l = 0; l + 1 < cp.n; ++l) {
+      const DevImage& a = *cp.img[l];
+      DevImage& b = *cp.img[l + 1];
+      HCHECK(gaussian_scaling(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, b.ptr, b.pitch,
+                              {(unsigned)b.w, (unsigned)b.h}, s));
+    }
+    for (int l = 0; l < cp.n; ++l) {
+      const DevImage& a = *cp.img[l];
+      HCHECK(conv_grad_x(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, cp.gx[l]->ptr, cp.gx[l]->pitch, s));
+      HCHECK(conv_grad_y(a.tex_point, {(unsigned)a.w, (unsigned)a.h}, cp.gy[l]->ptr, cp.gy[l]->pitch, s));
+    }
+    // LK
+    if (n > 0) HCHECK(lk_track(pgx, pgy, pi, ci, d, n, s));
+    // selection on the current frame with the tracks alive
+    if (n_old > 0) HCHECK(cudaMemcpyAsync(kp, alive.data(), sizeof(Keypoint) * n_old, cudaMemcpyHostToDevice, s));
+    HCHECK(cudaMemsetAsync(bins, 0, sizeof(float) * 66, s));
+    HCHECK(gftt_values(cp.gx[0]->tex_point, cp.gy[0]->tex_point, val.ptr, val.pitch, size, s));
+    HCHECK(accumulateGFTT(val.tex_point, size, bin_size, num_bins, bins + 2, s));
+    HCHECK(non_max_suppression(val.tex_point, size, maxim.ptr, maxim.pitch, s));
+    if (n_old > 0) HCHECK(filter_maximums(maxim.ptr, size, maxim.pitch, kp, (size_t)n_old, s));
+    float hb[66];
+    int kp_count = 0;
+    if (max_tracks > 0) {
+      HCHECK(downsample_gftt_x8(maxim.ptr, maxim.pitch, dsm.ptr, ds, dsm.pitch, idx, idx_pitch, s));
+      HCHECK(select_features(val.ptr, size, val.pitch, dsm.ptr, ds, dsm.pitch, idx, idx_pitch, kp,
+                             (size_t)max_tracks, (int*)bins, (int*)bins + 1, s));
+    }
+    HCHECK(cudaMemcpyAsync(hb, bins, sizeof(float) * 66, cudaMemcpyDeviceToHost, s));
+    HCHECK(cudaStreamSynchronize(s));
+    memcpy(&kp_count, hb, sizeof(int));
+    if (kp_count > max_tracks) kp_count = max_tracks;
+    if (kp_count > 0) sort_keypoints(kp, (size_t)kp_count, tmp, tmp_bytes, s);
+    if (kp_count > 0) HCHECK(cudaMemcpyAsync(host_kp.data(), kp, sizeof(Keypoint) * kp_count, cudaMemcpyDeviceToHost, s));
+    HCHECK(cudaStreamSynchronize(s));
+    float sum = 0.f;
+    for (int i = 0; i < 64; ++i) sum += hb[i + 2];
+    size_t prev_cnt[64] = {0}, want[64] = {0}, added[64] = {0};
+    for (int i = 0; i < n_old; ++i) {
+      const unsigned bx = (unsigned)(alive[i].x / (float)bin_size.x), by = (unsigned)(alive[i].y / (float)bin_size.y);
+      if (bx < 8 && by < 8) prev_cnt[by * 8 + bx]++;
+    }
+    for (int i = 0; i < 64 && sum > 0.f; ++i) {
+      const size_t e = (size_t)std::round((float)((size_t)n + (size_t)num_desired) * hb[i + 2] / sum);
+      if (e > prev_cnt[i]) want[i] = e - prev_cnt[i];
+    }
+    int out_n = 0;
+    for (int i = 0; i < kp_count && out_n < num_desired; ++i) {
+      const unsigned bx = (unsigned)(host_kp[i].x / (float)bin_size.x), by = (unsigned)(host_kp[i].y / (float)bin_size.y);
+      if (bx < 8 && by < 8 && added[by * 8 + bx] < want[by * 8 + bx]) {
+        added[by * 8 + bx]++;
+        sel[2 * out_n] = host_kp[i].x;
+        sel[2 * out_n + 1] = host_kp[i].y;
+        ++out_n;
+      }
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (r >= 2) total += std::chrono::duration<double, std::milli>(t1 - t0).count();
+  }
+  *ms_out = (float)(total / (reps > 0 ? reps : 1));
+  cudaFree(d);
+  cudaFree(d0);
+  cudaFree(d_u8);
+  cudaFree(idx);
+  cudaFree(kp);
+  cudaFree(bins);
+  cudaFree(tmp);
   return 0;
 }
 

@@ -99,3 +99,59 @@ def test_stages_vs_reference_kernels(ctx):
     for k in ("pyramid", "affine", "affine_cached"):
         assert ours[k] <= ref[k], (k, ours[k], ref[k])
     assert all(v > 0 for v in ours.values()) and all(v > 0 for v in ref.values())
+
+
+def test_multicam_frame_vs_reference_path(ctx):
+    """The 32-camera frame step (bench.py's workload: 12 x 640x480, 12 x 1280x720, 8 x 1920x1200,
+    300-3000 features each) through the reference's GPU path, one camera after another on one stream
+    as MonoSOFGPU runs it (pyramid, lk_track, GPUSelection with its read-backs and host quota loop;
+    ref_time_frame, host clock), against this library's batched step (one CUDA graph, CUDA events).
+    Prints one JSON line; asserts the batched step is faster."""
+    if not os.path.exists(REF_LIB):
+        pytest.skip("oracle/_ref/libcuvslam_ref.so not built (needs the reference sources)")
+    import bench
+    from cuvslam_b200 import _lib
+    from cuvslam_b200.frontend import Batch, CameraFrame, ImagePyramid, Selection, tracks_to_device
+    from cuvslam_b200.types import make_tracks
+
+    lib = ctypes.CDLL(REF_LIB)
+    lib.ref_time_frame.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_float)]
+    shapes, counts, prevs, nexts = bench.workload()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sel = Selection(ctx)
+    frames, pristine, hosts = [], [], []
+    for (w, h), p, nx, n in zip(shapes, prevs, nexts, counts):
+        pp = ImagePyramid(w, h, device=dev).build(ctx, torch.from_numpy(p).to(dev))
+        xy = sel.compute_gftt_and_select_features(pp, 0, 0, 0, 0, None, None, n).cpu().numpy()
+        t = make_tracks(xy, None, float(w), 0.8)
+        hosts.append(t)
+        td = tracks_to_device(t, dev)
+        pristine.append(td.clone())
+        frames.append(CameraFrame(torch.from_numpy(nx).to(dev), ImagePyramid(w, h, device=dev), pp, td, n, (0, 0, 0, 0)))
+    batch = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)
+    batch.autotune(reps=10, stream=stream)
+
+    def restore():
+        for f, p0 in zip(frames, pristine):
+            f.tracks.copy_(p0)
+
+    ours_ms = _ours(lambda: batch.run(stream), restore)
+    batch.close()
+    ref_ms = []
+    for (w, h), p, nx, n, t in zip(shapes, prevs, nexts, counts, hosts):
+        ms = ctypes.c_float(0.0)
+        rc = lib.ref_time_frame(np.ascontiguousarray(p).ctypes.data_as(ctypes.c_void_p),
+                                np.ascontiguousarray(nx).ctypes.data_as(ctypes.c_void_p), w, h, 10,
+                                t.ctypes.data_as(ctypes.c_void_p), len(t), n, 5, ctypes.byref(ms))
+        assert rc == 0, rc
+        ref_ms.append(ms.value)
+    tracks = sum(len(t) for t in hosts)
+    line = {"workload": "multicam32 frame step", "tracks": tracks, "ours_batched_ms": ours_ms,
+            "reference_path_ms": float(sum(ref_ms)), "speedup": float(sum(ref_ms)) / ours_ms,
+            "reference_per_camera_ms": {"640x480": float(np.mean(ref_ms[:12])), "1280x720": float(np.mean(ref_ms[12:24])),
+                                        "1920x1200": float(np.mean(ref_ms[24:]))}}
+    print(json.dumps(line))
+    assert ours_ms < sum(ref_ms)
