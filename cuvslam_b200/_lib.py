@@ -16,6 +16,7 @@ FE_ERR_INVALID_ARGUMENT = 1
 FE_SAMPLE_TEXTURE = 0
 FE_SAMPLE_EXACT = 1
 FE_SAMPLE_TEXTURE_WIDE = 2
+FE_SAMPLE_HARDWARE = 3
 
 
 class FePyramid(ctypes.Structure):

@@ -43,6 +43,7 @@ int cuda_fail(cudaError_t e) {
   } while (0)
 
 constexpr int64_t kAlign = 256;
+constexpr int64_t kPlaneAlign = 512;  // pyramid planes: the texture base alignment (FE_SAMPLE_HARDWARE)
 int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 int next_pow2(int v) {
   int p = 1;
@@ -281,7 +282,73 @@ struct fe_context {
   void* stereo_mem = nullptr;  // left-to-right matching scratch (grown on demand)
   size_t stereo_bytes = 0;
   bool debug = false;
+  // FE_SAMPLE_HARDWARE: texture objects of the planes tracked on, created on first use
+  struct Tex {
+    const void* ptr;
+    int w, h;
+    int64_t pitch;
+    cudaTextureObject_t t;
+  };
+  std::vector<Tex> tex;
 };
+
+namespace {
+
+// The texture object (linear filtering, clamped, unnormalised coordinates: the reference's sampling
+// of its pyramid planes) of one plane, from the context's cache or created now.
+int plane_texture(fe_context* ctx, const float* ptr, int w, int h, int64_t pitch, unsigned long long* out) {
+  for (const auto& t : ctx->tex)
+    if (t.ptr == ptr && t.w == w && t.h == h && t.pitch == pitch) {
+      *out = (unsigned long long)t.t;
+      return FE_OK;
+    }
+  int base_align = 0, pitch_align = 0;
+  if (cudaDeviceGetAttribute(&base_align, cudaDevAttrTextureAlignment, ctx->device) != cudaSuccess || base_align <= 0)
+    base_align = 512;
+  if (cudaDeviceGetAttribute(&pitch_align, cudaDevAttrTexturePitchAlignment, ctx->device) != cudaSuccess ||
+      pitch_align <= 0)
+    pitch_align = 32;
+  if ((uintptr_t)ptr % (uintptr_t)base_align != 0 || pitch % pitch_align != 0) return FE_ERR_INVALID_ARGUMENT;
+  cudaResourceDesc rd;
+  memset(&rd, 0, sizeof(rd));
+  rd.resType = cudaResourceTypePitch2D;
+  rd.res.pitch2D.devPtr = const_cast<float*>(ptr);
+  rd.res.pitch2D.width = (size_t)w;
+  rd.res.pitch2D.height = (size_t)h;
+  rd.res.pitch2D.pitchInBytes = (size_t)pitch;
+  rd.res.pitch2D.desc = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+  cudaTextureDesc td;
+  memset(&td, 0, sizeof(td));
+  td.addressMode[0] = cudaAddressModeClamp;
+  td.addressMode[1] = cudaAddressModeClamp;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  cudaTextureObject_t t = 0;
+  if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    return FE_ERR_INVALID_ARGUMENT;
+  }
+  ctx->tex.push_back({ptr, w, h, pitch, t});
+  *out = (unsigned long long)t;
+  return FE_OK;
+}
+
+// The texture objects LK with FE_SAMPLE_HARDWARE reads: previous image and gradients, current image.
+int lk_textures(fe_context* ctx, const fe_pyramid& prev, const fe_pyramid& cur, bool horizontal, fe::LkTex& out) {
+  memset(&out, 0, sizeof(out));
+  for (int l = 0; l < prev.levels; ++l) {
+    int rc = plane_texture(ctx, prev.image[l], prev.width[l], prev.height[l], prev.pitch_bytes[l], &out.prev_img[l]);
+    if (!rc) rc = plane_texture(ctx, prev.grad_x[l], prev.width[l], prev.height[l], prev.pitch_bytes[l], &out.prev_gx[l]);
+    if (!rc && !horizontal)
+      rc = plane_texture(ctx, prev.grad_y[l], prev.width[l], prev.height[l], prev.pitch_bytes[l], &out.prev_gy[l]);
+    if (!rc) rc = plane_texture(ctx, cur.image[l], cur.width[l], cur.height[l], cur.pitch_bytes[l], &out.cur_img[l]);
+    if (rc) return rc;
+  }
+  return FE_OK;
+}
+
+}  // namespace
 
 namespace {
 
@@ -434,6 +501,7 @@ int fe_create(int device, fe_context** out) {
 
 int fe_destroy(fe_context* ctx) {
   if (!ctx) return FE_ERR_INVALID_ARGUMENT;
+  for (const auto& t : ctx->tex) cudaDestroyTextureObject(t.t);
   if (ctx->sel.mem) cudaFree(ctx->sel.mem);
   if (ctx->lk_counter) cudaFree(ctx->lk_counter);
   if (ctx->stage_done) cudaFree(ctx->stage_done);
@@ -454,7 +522,7 @@ int64_t fe_pyramid_bytes(int width, int height, int max_levels) {
   int ws[FE_MAX_LEVELS], hs[FE_MAX_LEVELS];
   const int n = level_sizes(width, height, max_levels, ws, hs);
   int64_t total = 0;
-  for (int l = 0; l < n; ++l) total += 3 * align_up(align_up((int64_t)ws[l] * 4, kAlign) * hs[l], kAlign);
+  for (int l = 0; l < n; ++l) total += 3 * align_up(align_up((int64_t)ws[l] * 4, kAlign) * hs[l], kPlaneAlign);
   return total;
 }
 
@@ -469,7 +537,7 @@ int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int height, i
   char* p = (char*)device_memory;
   for (int l = 0; l < n; ++l) {
     const int64_t pitch = align_up((int64_t)ws[l] * 4, kAlign);
-    const int64_t plane = align_up(pitch * hs[l], kAlign);
+    const int64_t plane = align_up(pitch * hs[l], kPlaneAlign);
     out->width[l] = ws[l];
     out->height[l] = hs[l];
     out->pitch_bytes[l] = pitch;
@@ -589,7 +657,7 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
              int horizontal, int sampling, fe_stream stream) {
   if (!ctx || !valid_pyramid(prev) || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
   if (cur->levels < prev->levels) return FE_ERR_INVALID_ARGUMENT;
-  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_HARDWARE) return FE_ERR_INVALID_ARGUMENT;
   if (!horizontal)
     for (int l = 0; l < prev->levels; ++l)
       if (!prev->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
@@ -608,6 +676,10 @@ int fe_track(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur, fe_
   p.single.tracks = tracks;
   p.single.n = n;
   p.single.begin = 0;
+  if (sampling == FE_SAMPLE_HARDWARE) {
+    const int rc = lk_textures(ctx, *prev, *cur, horizontal != 0, p.single_tex);
+    if (rc) return rc;
+  }
   FE_CUDA(fe::launch_lk(p, (cudaStream_t)stream));
   return FE_OK;
 }
@@ -617,7 +689,7 @@ int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur
   if (!(retrack_ncc == retrack_ncc)) return FE_ERR_INVALID_ARGUMENT;
   if (!ctx || !valid_pyramid(prev) || !valid_pyramid(cur) || n < 0 || (n > 0 && !tracks)) return FE_ERR_INVALID_ARGUMENT;
   if (cur->levels < prev->levels) return FE_ERR_INVALID_ARGUMENT;
-  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_HARDWARE) return FE_ERR_INVALID_ARGUMENT;
   for (int l = 0; l < prev->levels; ++l)
     if (!prev->grad_y[l]) return FE_ERR_INVALID_ARGUMENT;
   if ((uintptr_t)tracks % 16 != 0) return FE_ERR_INVALID_ARGUMENT;
@@ -633,6 +705,10 @@ int fe_track_mono(fe_context* ctx, const fe_pyramid* prev, const fe_pyramid* cur
   p.single.tracks = tracks;
   p.single.n = n;
   p.single.retrack_ncc = retrack_ncc > 0.f ? retrack_ncc : 0.f;
+  if (sampling == FE_SAMPLE_HARDWARE) {
+    const int rc = lk_textures(ctx, *prev, *cur, false, p.single_tex);
+    if (rc) return rc;
+  }
   FE_CUDA(fe::launch_lk(p, (cudaStream_t)stream));
   return FE_OK;
 }
@@ -885,6 +961,7 @@ struct fe_batch {
   std::vector<char> has_prev;
   StagePlan plan;
   fe::LkCam* d_lk = nullptr;
+  fe::LkTex* d_tex = nullptr;  // FE_SAMPLE_HARDWARE: texture objects per LK camera
   int* lk_counter = nullptr;
   fe::LkLaunch lk;
   fe::SelectBatch* sel = nullptr;  // heap: large
@@ -1093,7 +1170,7 @@ int fe_batch_tuning(const fe_batch* b, int32_t* lk_shape, int32_t* overlap, int3
 int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int sampling, fe_batch** out) {
   if (!ctx || !cams || !out || ncams <= 0) return FE_ERR_INVALID_ARGUMENT;
   if (ncams > fe::kMaxCams) return FE_ERR_CAPACITY;
-  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_TEXTURE_WIDE) return FE_ERR_INVALID_ARGUMENT;
+  if (sampling < FE_SAMPLE_TEXTURE || sampling > FE_SAMPLE_HARDWARE) return FE_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   fe_batch* b = new (std::nothrow) fe_batch;
   if (!b) return FE_ERR_OUT_OF_MEMORY;
@@ -1116,6 +1193,7 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
   };
   // validate and copy descriptors; plan the pyramid stages
   std::vector<fe::LkCam> lk;
+  std::vector<fe::LkTex> lk_tex;
   int total = 0;
   for (int i = 0; i < ncams; ++i) {
     const fe_camera_frame& c = cams[i];
@@ -1140,6 +1218,12 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
       lc.retrack_ncc = c.finish ? c.finish->retrack_ncc : 0.f;
       total += c.n_tracks;
       lk.push_back(lc);
+      if (sampling == FE_SAMPLE_HARDWARE) {
+        fe::LkTex t;
+        rc = lk_textures(ctx, b->prev[i], b->cur[i], false, t);
+        if (rc) return fail(rc);
+        lk_tex.push_back(t);
+      }
     }
   }
   memset(&b->lk, 0, sizeof(b->lk));
@@ -1156,6 +1240,13 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
     b->lk.total = total;
     b->lk.horizontal = 0;
     b->lk.sampling = sampling;
+    if (sampling == FE_SAMPLE_HARDWARE) {
+      e = dev_alloc((void**)&b->d_tex, sizeof(fe::LkTex) * lk_tex.size());
+      if (e != cudaSuccess) return fail(cuda_fail(e));
+      e = cudaMemcpy(b->d_tex, lk_tex.data(), sizeof(fe::LkTex) * lk_tex.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(cuda_fail(e));
+      b->lk.texs = b->d_tex;
+    }
   }
   // finish filters (cameras with tracks and options): one CTA per camera, collapse cells zeroed once
   {
@@ -1412,6 +1503,7 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->join_ev) cudaEventDestroy(b->join_ev);
   if (b->d_lk) cudaFree(b->d_lk);
   if (b->lk_counter) cudaFree(b->lk_counter);
+  if (b->d_tex) cudaFree(b->d_tex);
   if (b->sel_mem) cudaFree(b->sel_mem);
   if (b->stage_done) cudaFree(b->stage_done);
   if (b->finish_cells) cudaFree(b->finish_cells);

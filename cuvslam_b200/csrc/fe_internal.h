@@ -136,6 +136,11 @@ namespace lk {
 struct LkRecord;
 }
 
+// Texture objects of one camera's planes for FE_SAMPLE_HARDWARE (cudaTextureObject_t values).
+struct LkTex {
+  unsigned long long prev_img[kMaxLevels], prev_gx[kMaxLevels], prev_gy[kMaxLevels], cur_img[kMaxLevels];
+};
+
 struct LkLaunch {
   const LkCam* cams;            // device array (batched) or nullptr
   int* counter;                 // device track counter (persistent warps), or nullptr: one warp per track
@@ -149,9 +154,13 @@ struct LkLaunch {
   int shape;                    // reference rule: block shape (kLkShapes), chosen by the batch autotuner
   lk::LkRecord* recs;           // unrolled: per-track records for the adjoint (may be null)
   LkCam single;                 // used when cams == nullptr
+  const LkTex* texs;            // FE_SAMPLE_HARDWARE: device array parallel to cams, or nullptr
+  LkTex single_tex;             // FE_SAMPLE_HARDWARE with cams == nullptr
 };
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
+// The reference rule with the texture unit's filtering (lk_hw.cu).
+cudaError_t launch_lk_hw(const LkLaunch& p, cudaStream_t s);
 constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2
 
 // ---------------------------------------------------------------- track filters after LK

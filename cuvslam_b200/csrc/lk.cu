@@ -120,6 +120,7 @@ cudaError_t launch(const LkLaunch& p, cudaStream_t s) {
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s) {
   if (p.total <= 0) return cudaSuccess;
+  if (p.sampling == FE_SAMPLE_HARDWARE) return p.mode == kLkReference ? launch_lk_hw(p, s) : cudaErrorInvalidValue;
   if (p.counter) {
     cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;

@@ -85,6 +85,13 @@ typedef enum {
   FE_SAMPLE_TEXTURE_WIDE = 2, /* the texture weights with each 4-tap sum rounded to FP32 once (FP64
                                  arithmetic), as the texture unit does: equals the hardware's samples
                                  more often, so marginal accept/reject decisions follow the reference */
+  FE_SAMPLE_HARDWARE = 3,     /* the texture unit itself (linear filtering on texture objects the
+                                 library creates for the pyramid planes, as the reference samples):
+                                 LK only (fe_track, fe_track_mono, batches).  Planes must start on the
+                                 device's texture alignment (512 bytes) with pitches on its texture
+                                 pitch alignment (32 bytes), as fe_pyramid_init lays them out in
+                                 512-byte aligned memory.  Not bit-identical to an emulation: within
+                                 0.01 px of the wide mode's results on the test frames */
 } fe_sampling;
 
 /* ---------------------------------------------------------------------------------------- */
@@ -110,10 +117,11 @@ FE_API int fe_destroy(fe_context* ctx);
 /* Number of levels of a width x height pyramid capped at max_levels (0 on bad arguments). */
 FE_API int fe_pyramid_levels(int width, int height, int max_levels);
 /* Bytes of device memory one pyramid (image + grad_x + grad_y, all levels) needs in this
- * library's layout (each plane 256-byte aligned, rows padded to 256 bytes). */
+ * library's layout (planes at multiples of 512 bytes from the start, rows padded to 256 bytes). */
 FE_API int64_t fe_pyramid_bytes(int width, int height, int max_levels);
 /* Lays a pyramid out in caller-provided device memory of at least fe_pyramid_bytes() bytes
- * (256-byte aligned).  Host-only; allocates nothing. */
+ * (256-byte aligned; 512-byte aligned memory also suits FE_SAMPLE_HARDWARE's texture objects).
+ * Host-only; allocates nothing. */
 FE_API int fe_pyramid_init(void* device_memory, int64_t bytes, int width, int height, int max_levels, fe_pyramid* out);
 
 /* Builds every level and both gradient images of `pyr` from a uint8 grayscale image in device

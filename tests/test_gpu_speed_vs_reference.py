@@ -4,7 +4,8 @@ cuVSLAM sources for sm_100a into oracle/_ref by oracle/build_ref.sh) on the same
 offsets.  Stages: the current frame's pyramid + gradients (uint8 in device memory -> every level),
 pyramidal LK (texture-weight emulation), the affine tracker (0 shift + 20 full steps) and its cached
 variant.  Both sides are timed with CUDA events around the stage alone (records reset before each
-run, outside the timed interval), mean of 20 runs after 3 warm-up runs.  Prints one JSON line.
+run, outside the timed interval, and the host's enqueue time hidden behind a spin kernel), mean of 20 runs after 3 warm-up
+runs.  Prints one JSON line.
 Asserts that the pyramid and the affine tracker are faster than the reference's kernels.  LK is
 reported, not asserted: the reference's warp-per-track kernel samples with the texture unit, ours
 emulates that filtering exactly in FP32 (the price of bit-identical results with the oracle) and is
@@ -36,11 +37,14 @@ def _ref_stage(lib, prev, nxt, tracks, which):
 
 
 def _ours(fn, reset=None):
+    """Device time of fn: the stream is kept busy by a short spin kernel while the host enqueues fn
+    (so the Python call's host time is not counted, as the reference's C harness counts none)."""
     stream = torch.cuda.current_stream()
     tot = 0.0
     for r in range(REPS + 3):
         if reset is not None:
             reset()
+        torch.cuda._sleep(1_000_000)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
         fn()
