@@ -44,6 +44,7 @@ int cuda_fail(cudaError_t e) {
 
 constexpr int64_t kAlign = 256;
 constexpr int64_t kPlaneAlign = 512;  // pyramid planes: the texture base alignment (FE_SAMPLE_HARDWARE)
+constexpr int kMaxContextTextures = 4096;  // FE_SAMPLE_HARDWARE texture objects one context keeps
 int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 int next_pow2(int v) {
   int p = 1;
@@ -309,6 +310,8 @@ int plane_texture(fe_context* ctx, const float* ptr, int w, int h, int64_t pitch
       pitch_align <= 0)
     pitch_align = 32;
   if ((uintptr_t)ptr % (uintptr_t)base_align != 0 || pitch % pitch_align != 0) return FE_ERR_INVALID_ARGUMENT;
+  // kept until fe_destroy (a kernel in flight may still read one): a bounded number per context
+  if (ctx->tex.size() >= (size_t)kMaxContextTextures) return FE_ERR_CAPACITY;
   cudaResourceDesc rd;
   memset(&rd, 0, sizeof(rd));
   rd.resType = cudaResourceTypePitch2D;

@@ -90,8 +90,11 @@ typedef enum {
                                  LK only (fe_track, fe_track_mono, batches).  Planes must start on the
                                  device's texture alignment (512 bytes) with pitches on its texture
                                  pitch alignment (32 bytes), as fe_pyramid_init lays them out in
-                                 512-byte aligned memory.  Not bit-identical to an emulation: within
-                                 0.01 px of the wide mode's results on the test frames */
+                                 512-byte aligned memory.  The context keeps a texture object per
+                                 plane it tracked on until fe_destroy, at most 4096 (then
+                                 FE_ERR_CAPACITY): reuse pyramids.  Not bit-identical to an
+                                 emulation: within 0.01 px of the wide mode's results on the test
+                                 frames */
 } fe_sampling;
 
 /* ---------------------------------------------------------------------------------------- */
