@@ -1,6 +1,6 @@
 """Benchmark: batched multi-camera tracking front-end on B200.
 
-Workload (BASELINE config "batched multicamera"): 32 cameras of uneven resolution (12 x 640x480,
+Workload ("batched multicamera"): 32 cameras of uneven resolution (12 x 640x480,
 12 x 1280x720, 8 x 1920x1200, uint8), each with its own seeded synthetic scene and similarity warp,
 and 300..3000 features per camera (seeded).  One step is one frame of all 32 cameras: build the
 current pyramids and gradient pyramids, track every feature from the previous frame (pyramidal LK),
@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the other BASELINE configs (stereo plain, 100-frame sequence, fwd+bwd stream)")
+                    help="skip the other workloads (stereo plain, 100-frame sequence, fwd+bwd stream, L2R, affine)")
     ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled", "affine"],
                     default=None,
                     help="for an ncu capture: run only this part of the step (inside NVTX ranges named "
@@ -264,7 +264,7 @@ def adjoint_bench(ctx, dev, stream, timed, reps=20):
     return out
 
 
-# ---------------------------------------------------------------- the other BASELINE configs
+# ---------------------------------------------------------------- the other workloads
 SEQ_W, SEQ_H, SEQ_FRAMES, SEQ_FEATURES, SEQ_LEVELS = 1241, 376, 100, 1000, 5
 
 
@@ -299,7 +299,7 @@ def _dev_stats(a, b, ok):
 
 
 def config_sequence(ctx, dev, stream, frames):
-    """one camera, 1241x376, 100 frames, 5 levels, 1000 features kept by re-detection.
+    """Single-camera sequence: one camera, 1241x376, 100 frames, 5 levels, 1000 features kept by re-detection.
     The plain GPU path (the drop-in call sequence: build, track, select with its blocking readback)
     against the restated reference CPU tracker (single thread, one camera) in tracks/s; deviation of
     the GPU tracks from the CPU tracker's on the same inputs, and both from the ground truth."""
@@ -364,7 +364,7 @@ def config_sequence(ctx, dev, stream, frames):
 
 
 def config_stereo_plain(ctx, dev, stream):
-    """one stereo pair plus next frame at 752x480, 4 levels, 512 features: the plain GPU
+    """Stereo pair, plain path: one stereo pair plus next frame at 752x480, 4 levels, 512 features: the plain GPU
     path (three pyramids, selection, LK left->next and the horizontal left->right) and the restated
     reference CPU tracker (left->next), per-frame latency."""
     import torch
@@ -631,7 +631,7 @@ def stream_bases():
 
 
 def config_stream(ctx, dev, stream, bases):
-    """16 stereo pairs (32 images) at 1920x1200, 30 consecutive frames, 8192 features
+    """Forward + backward stream: 16 stereo pairs (32 images) at 1920x1200, 30 consecutive frames, 8192 features
     per image; per frame the forward tracker and the implicit adjoint of the mean squared distance to
     ground truth run in one captured CUDA graph, the pyramids rebuilt for the backward instead of kept.
     Frames: each camera's rendered base frame warped on the GPU by its per-frame similarity (a stand-in
@@ -1019,18 +1019,18 @@ def main():
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         adjoint = adjoint_bench(ctx, dev, stream, timed)
-    configs = None
+    workloads = None
     if want_configs:
-        configs = {}
-        for name, fn in (("1_stereo_plain", lambda: config_stereo_plain(ctx, dev, stream)),
-                         ("2_sequence", lambda: config_sequence(ctx, dev, stream, seq_frames)),
+        workloads = {}
+        for name, fn in (("stereo_plain", lambda: config_stereo_plain(ctx, dev, stream)),
+                         ("sequence", lambda: config_sequence(ctx, dev, stream, seq_frames)),
                          ("l2r_stereo", lambda: config_l2r(ctx, dev, stream)),
                          ("affine_st", lambda: config_affine(ctx, dev, stream)),
-                         ("5_stream_fwd_bwd", lambda: config_stream(ctx, dev, stream, bases))):
+                         ("stream_fwd_bwd", lambda: config_stream(ctx, dev, stream, bases))):
             try:
-                configs[name] = fn()
+                workloads[name] = fn()
             except Exception as ex:  # reported, not fatal: the headline line must still print
-                configs[name] = {"error": f"{type(ex).__name__}: {ex}"}
+                workloads[name] = {"error": f"{type(ex).__name__}: {ex}"}
             torch.cuda.synchronize()
 
     if rank == 0:
@@ -1056,7 +1056,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": kernels_per_step * args.steps,
             "adjoint": adjoint,
-            "other_configs": configs,
+            "other_configs": workloads,
         }
         print(json.dumps(line), flush=True)
     batch.close()

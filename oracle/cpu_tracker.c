@@ -1,4 +1,4 @@
-/* CPU restatement of cuVSLAM's CPU tracking front-end (use_gpu = false).  TEST AND BASELINE
+/* CPU restatement of cuVSLAM's CPU tracking front-end (use_gpu = false).  TEST AND CPU-baseline
  * INFRASTRUCTURE ONLY: bench.py times it as the reference CPU arm; nothing in the product links it.
  *
  * The reference's own CPU code cannot be compiled here (it needs Eigen 3.4.1, fetched over the network

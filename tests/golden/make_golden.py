@@ -153,7 +153,7 @@ def make_reference(out_dir):
                 for q, arr in (("img", lv), ("gx", gx), ("gy", gy)):
                     compact[f"{name}/{tag}/L{l}/{q}/sha"] = np.array(_sha(arr))
                     full[f"{name}/{tag}/L{l}/{q}"] = arr
-        # 4-level pyramids (BASELINE config 1 caps levels at 4)
+        # 4-level pyramids (the stereo-pair workload caps levels at 4)
         for l, (lv, gx, gy) in enumerate(ref_pyramid(lib, prev, 4)):
             compact[f"{name}/prev4/L{l}/img/sha"] = np.array(_sha(lv))
         h, w = prev.shape
