@@ -87,8 +87,9 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp",
-                                 f"clocks_{os.getpid()}.csv")
+        import tempfile
+
+        self.path = os.path.join(tempfile.gettempdir(), f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
