@@ -243,58 +243,108 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
   }
   __syncthreads();
 
-  // C. vertical 7-tap and the measure (gftt.cu:61-66, 148-160) for 34 rows x 66 columns, one
-  //    column pair per work item, packed FP32x2 arithmetic
-  for (int it = tid; it < (TH + 2) * (RW / 2); it += kThreads) {
-    const int r = it / (RW / 2), q = (it - r * (RW / 2)) * 2;
-    float2 xx = dup(0.f), xy = dup(0.f), yy = dup(0.f);
+  // C. vertical 7-tap and the measure (gftt.cu:61-66, 148-160) for 34 rows x 66 columns, packed
+  //    FP32x2 arithmetic: a column pair and a strip of kStrip rows per thread (the last strip starts
+  //    at row 29 and stores rows 30-33 only).  Each staged row of horizontal sums is added into every
+  //    output row it is a tap of; an output row's taps still arrive in order j = 0..6.
+  {
+    constexpr int kStrip = 5, kStrips = (TH + 2 + kStrip - 1) / kStrip;
+    static_assert(kStrips * (RW / 2) <= kThreads, "one strip per thread");
+    if (tid < kStrips * (RW / 2)) {
+      const int s = tid / (RW / 2), q = (tid - s * (RW / 2)) * 2;
+      const int r0 = min(s * kStrip, TH + 2 - kStrip), keep = s * kStrip - r0;
+      float2 xx[kStrip], xy[kStrip], yy[kStrip];
 #pragma unroll
-    for (int j = 0; j < 7; ++j) {
-      const float2 cj = dup(gauss7(j));
-      xx = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hxx + (r + j) * HS + q), xx);
-      xy = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hxy + (r + j) * HS + q), xy);
-      yy = __ffma2_rn(cj, *reinterpret_cast<const float2*>(hyy + (r + j) * HS + q), yy);
+      for (int o = 0; o < kStrip; ++o) xx[o] = xy[o] = yy[o] = dup(0.f);
+#pragma unroll
+      for (int k = 0; k < kStrip + 6; ++k) {
+        const float2 a = *reinterpret_cast<const float2*>(hxx + (r0 + k) * HS + q);
+        const float2 bb = *reinterpret_cast<const float2*>(hxy + (r0 + k) * HS + q);
+        const float2 cc = *reinterpret_cast<const float2*>(hyy + (r0 + k) * HS + q);
+#pragma unroll
+        for (int o = 0; o < kStrip; ++o) {
+          const int j = k - o;
+          if (j < 0 || j > 6) continue;
+          const float2 cj = dup(gauss7(j));
+          xx[o] = __ffma2_rn(cj, a, xx[o]);
+          xy[o] = __ffma2_rn(cj, bb, xy[o]);
+          yy[o] = __ffma2_rn(cj, cc, yy[o]);
+        }
+      }
+#pragma unroll
+      for (int o = 0; o < kStrip; ++o) {
+        if (o < keep) continue;
+        const float2 d = __fadd2_rn(xx[o], make_float2(-yy[o].x, -yy[o].y));
+        const float2 D2 = __ffma2_rn(__fmul2_rn(dup(4.f), xy[o]), xy[o], __fmul2_rn(d, d));
+        const float2 T = __fadd2_rn(xx[o], yy[o]);
+        const float2 D = make_float2(__fsqrt_rn(D2.x), __fsqrt_rn(D2.y));
+        const float2 e1 = __fadd2_rn(__fmul2_rn(__fadd2_rn(T, make_float2(-D.x, -D.y)), dup(0.5f)), dup(1.f));
+        *reinterpret_cast<float2*>(resp + (r0 + o) * RS + q) = make_float2(__logf(e1.x), __logf(e1.y));
+      }
     }
-    const float2 d = __fadd2_rn(xx, make_float2(-yy.x, -yy.y));
-    const float2 D2 = __ffma2_rn(__fmul2_rn(dup(4.f), xy), xy, __fmul2_rn(d, d));
-    const float2 T = __fadd2_rn(xx, yy);
-    const float2 D = make_float2(__fsqrt_rn(D2.x), __fsqrt_rn(D2.y));
-    const float2 e1 = __fadd2_rn(__fmul2_rn(__fadd2_rn(T, make_float2(-D.x, -D.y)), dup(0.5f)), dup(1.f));
-    *reinterpret_cast<float2*>(resp + r * RS + q) = make_float2(__logf(e1.x), __logf(e1.y));
   }
   __syncthreads();
 
-  // D. NMS on the core with clamped neighbours, then (single-camera path) the burn mask
+  // D. NMS on the core with clamped neighbours, then (single-camera path) the burn mask; four
+  //    pixels (x .. x+3, x a multiple of 4) per work item from three rows of six response values
   const int words = (w + 31) / 32;
-  for (int i = tid; i < TW * TH; i += kThreads) {
-    const int r = i / TW, q = i - r * TW;
+  const bool resp_vec = (w & 3) == 0 && (reinterpret_cast<uintptr_t>(c.resp) & 15) == 0;
+  for (int i = tid; i < TW * TH / 4; i += kThreads) {
+    const int r = i / (TW / 4), q = (i - r * (TW / 4)) * 4;
     const int x = X + q, y = Y + r;
-    if (x >= w || y >= h) {
-      nms[r * TW + q] = 0.f;
-      continue;
-    }
-    const float* rp = resp + (r + 1) * RS + (q + 1);
-    const float v = rp[0];
-    bool is_max;
-    if (x > 0 && y > 0 && x < w - 1 && y < h - 1) {
-      is_max = rp[-RS - 1] <= v && rp[-RS] <= v && rp[-RS + 1] <= v && rp[-1] <= v && rp[1] <= v &&
-               rp[RS - 1] <= v && rp[RS] <= v && rp[RS + 1] <= v;
-    } else {
-      is_max = true;
+    float m[4] = {0.f, 0.f, 0.f, 0.f};
+    if (y < h && x < w) {
+      float n[3][6];  // response rows y-1 .. y+1, columns x-1 .. x+4
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy)
+      for (int k = 0; k < 3; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(resp + (r + k) * RS + q);
+        const float2 e = *reinterpret_cast<const float2*>(resp + (r + k) * RS + q + 4);
+        n[k][0] = a.x;
+        n[k][1] = a.y;
+        n[k][2] = a.z;
+        n[k][3] = a.w;
+        n[k][4] = e.x;
+        n[k][5] = e.y;
+      }
+      const bool inner = x > 0 && y > 0 && x + 4 < w && y < h - 1;  // every pixel's 8 neighbours inside
+      const uint32_t burn = kSplit ? 0u : __ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31);
+      float v[4];
 #pragma unroll
-        for (int dx = -1; dx <= 1; ++dx) {
-          if (!dx && !dy) continue;
-          const int yy = min(max(y + dy, 0), h - 1) - Y + 1, xx = min(max(x + dx, 0), w - 1) - X + 1;
-          is_max &= resp[yy * RS + xx] <= v;
+      for (int p = 0; p < 4; ++p) {
+        v[p] = n[1][p + 1];
+        bool is_max;
+        if (inner) {
+          is_max = n[0][p] <= v[p] && n[0][p + 1] <= v[p] && n[0][p + 2] <= v[p] && n[1][p] <= v[p] &&
+                   n[1][p + 2] <= v[p] && n[2][p] <= v[p] && n[2][p + 1] <= v[p] && n[2][p + 2] <= v[p];
+        } else {
+          is_max = x + p < w;
+#pragma unroll
+          for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+              if (!dx && !dy) continue;
+              const int yy = min(max(y + dy, 0), h - 1) - Y + 1, xx = min(max(x + p + dx, 0), w - 1) - X + 1;
+              is_max = is_max && resp[yy * RS + xx] <= v[p];
+            }
         }
+        m[p] = is_max && !((burn >> p) & 1u) ? v[p] : 0.f;
+      }
+      if (kSplit || b.debug) {
+        float* o = c.resp + (size_t)y * w + x;
+        if (resp_vec && x + 3 < w) {
+          *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+#pragma unroll
+          for (int p = 0; p < 4; ++p)
+            if (x + p < w) o[p] = v[p];
+        }
+      }
+      if (!kSplit && b.debug)
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+          if (x + p < w) c.nms[(size_t)y * w + x + p] = m[p];
     }
-    float m = is_max ? v : 0.f;
-    if (!kSplit && ((__ldg(c.burn + (size_t)y * words + (x >> 5)) >> (x & 31)) & 1u)) m = 0.f;
-    nms[r * TW + q] = m;
-    if (kSplit || b.debug) c.resp[(size_t)y * w + x] = v;
-    if (!kSplit && b.debug) c.nms[(size_t)y * w + x] = m;
+    *reinterpret_cast<float4*>(nms + r * TW + q) = make_float4(m[0], m[1], m[2], m[3]);
   }
   __syncthreads();
 
