@@ -348,18 +348,23 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
   }
   __syncthreads();
 
-  // E. 32 cells of 8x8, four per warp, with the reference's lane order and tie rule (in the
-  //    batched path before the burn: cells_kernel redoes the cells that alive features reach)
+  // E. 32 cells of 8x8 (in the batched path before the burn: cells_kernel redoes the cells that
+  //    alive features reach), eight threads per cell.  The reference's warp (lane l holds pixels l and
+  //    l + 32, the second taken only when strictly greater, then a shfl_down tree whose merges keep
+  //    the lower lane on ties) yields the first maximum in (lane, element) order.  Here thread g of a
+  //    cell scans lanes 4g .. 4g+3 in that order with the same strict rule, and a 3-level shfl_down
+  //    merge within the cell's eight threads keeps the lower thread on ties: the same pixel.
   const int cw = w / 8, ch = h / 8;
-  for (int cc = wid; cc < 32; cc += kThreads / 32) {
+  static_assert(kThreads == 32 * 8, "eight threads per cell");
+  {
+    const int cc = tid >> 3, g = tid & 7;
     const int ccx = cc & 7, ccy = cc >> 3;
     const int cellx = X / 8 + ccx, celly = Y / 8 + ccy;
-    if (cellx >= cw || celly >= ch) continue;  // warp-uniform
     float m = 0.f;
     unsigned idx = 0;
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int f = lane + 32 * e, dy = f >> 3, dx = f & 7;
+    for (int k = 0; k < 8; ++k) {
+      const int f = 4 * g + (k >> 1) + 32 * (k & 1), dy = f >> 3, dx = f & 7;
       const float v = nms[(ccy * 8 + dy) * TW + ccx * 8 + dx];
       if (v > m) {
         m = v;
@@ -367,15 +372,15 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
       }
     }
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const float m2 = __shfl_down_sync(0xffffffffu, m, d);
-      const unsigned i2 = __shfl_down_sync(0xffffffffu, idx, d);
+    for (int d = 1; d < 8; d <<= 1) {
+      const float m2 = __shfl_down_sync(0xffffffffu, m, d, 8);
+      const unsigned i2 = __shfl_down_sync(0xffffffffu, idx, d, 8);
       if (m2 > m) {
         m = m2;
         idx = i2;
       }
     }
-    if (lane == 0) {
+    if (g == 0 && cellx < cw && celly < ch) {
       const int cell = celly * cw + cellx;
       const int px = cellx * 8 + (int)(idx & 0xffffu), py = celly * 8 + (int)(idx >> 16);
       float out_m = 0.f;
