@@ -1,0 +1,179 @@
+"""Index arithmetic of the levels 0-2 tile kernel (pyramid.cu, namespace l012), restated on the CPU.
+
+For each frame size, the tiles on the frame's edges and one interior tile are modelled (interior
+tiles are translations of one another).  For each modelled tile the test checks that every
+shared-memory read is inside its region (the uint8 tile, 163 x 176 bytes; the level-1 region,
+79 rows of 80 floats; the level-2 region, 38 rows of 40 floats).  Every value that reaches an
+output must also come from a cell that holds data:
+  - for the uint8 tile, a pixel of the frame;
+  - for the level-1 and level-2 regions, a cell that the strips or the corner fixes wrote.
+
+The kernel runs for frames with at least three levels (level 2 at least 15 px, so the frame is at
+least 57 px), where one reflection of `mirror_index` always lands inside the frame.  Everything
+here is restated from the kernel's source; it checks bounds, not pixel values, which the GPU parity
+tests compare with the oracle."""
+
+import numpy as np
+import pytest
+
+from cuvslam_b200.types import level_sizes
+
+T2, S0W, S0H, S1, S1S, S2, S2S = 32, 176, 163, 79, 80, 38, 40
+
+
+def mirror(i, n):
+    i = i if i >= 0 else -i - 1
+    return i if i < n else 2 * n - i - 1
+
+
+def tiles(w2, h2):
+    tx, ty = -(-w2 // T2), -(-h2 // T2)
+    xs = sorted({0, 1, tx // 2, tx - 2, tx - 1} & set(range(tx)))
+    ys = sorted({0, 1, ty // 2, ty - 2, ty - 1} & set(range(ty)))
+    return [(x * T2, y * T2) for y in ys for x in xs]
+
+
+def check_tile(sizes, X2, Y2):
+    (w0, h0), (w1, h1), (w2, h2) = sizes[:3]
+    a0x, a0y = 4 * X2 - 32, 4 * Y2 - 19
+    a1x, a1y = 2 * X2 - 8, 2 * Y2 - 8
+    a2x, a2y = X2 - 4, Y2 - 3
+
+    def b0(row, col):  # a read of the uint8 tile at tile coordinates whose value is used
+        assert 0 <= row < S0H and 0 <= col < S0W, (row, col)
+        assert 0 <= a0y + row < h0 and 0 <= a0x + col < w0, "read outside the frame"
+
+    # level 1: column strips of 14 rows, six bands
+    done1 = np.zeros((S1, S1S), bool)
+    for tid in range(S1 * 6):
+        c, band = tid % S1, tid // S1
+        x1 = a1x + c
+        ys, ye = max(a1y + band * 14, 0), min(a1y + min(band * 14 + 14, S1), h1)
+        if not (0 <= x1 < w1 and ys < ye):
+            continue
+        cols = [mirror(2 * x1 - 2 + l, w0) - a0x for l in range(5)]
+        contiguous = 2 * x1 - 2 >= 0 and 2 * x1 + 2 < w0
+        rows = [mirror(r, h0) - a0y for r in range(2 * ys - 2, 2 * (ye - 1) + 3)]
+        for r in rows:
+            if contiguous:
+                wofs = cols[0] & ~3
+                assert wofs >= 0 and wofs + 8 <= S0W  # the two aligned words
+                assert cols == list(range(cols[0], cols[0] + 5))
+            for cc in cols:
+                b0(r, cc)
+        for y in range(ys, ye):
+            done1[y - a1y, c] = True
+    for tid in range(4):  # corners redone with the 25-tap rule
+        x1, y1 = (w1 - 1 if tid & 1 else 0), (h1 - 1 if tid & 2 else 0)
+        if a1x <= x1 < a1x + S1 and a1y <= y1 < a1y + S1:
+            for k in range(5):
+                for l in range(5):
+                    xc, yc = 2 * x1 - 2 + l, 2 * y1 - 2 + k
+                    if (xc < 0 or xc >= w0) and (yc < 0 or yc >= h0):
+                        continue
+                    b0(mirror(yc, h0) - a0y, mirror(xc, w0) - a0x)
+            done1[y1 - a1y, x1 - a1x] = True
+
+    # level 2: column strips of 3 rows, 13 bands
+    done2 = np.zeros((S2, S2S), bool)
+    for tid in range(S2 * 13):
+        c, band = tid % S2, tid // S2
+        x2 = X2 - 3 + c
+        ys, ye = max(a2y + band * 3, 0), min(a2y + min(band * 3 + 3, S2), h2)
+        if not (0 <= x2 < w2 and ys < ye):
+            continue
+        cols = [mirror(2 * x2 - 2 + l, w1) - a1x for l in range(5)]
+        for r in range(2 * ys - 2, 2 * (ye - 1) + 3):
+            rr = mirror(r, h1) - a1y
+            for cc in cols:
+                assert 0 <= rr < S1 and 0 <= cc < S1S and done1[rr, cc], (rr, cc)
+        for y in range(ys, ye):
+            assert 0 <= x2 - a2x < S2S
+            done2[y - a2y, x2 - a2x] = True
+
+    def l2_taps(x, y, sw, sh, ax, ay, done, rows, stride):  # downscale_px on a region
+        x0, y0 = 2 * x - 2, 2 * y - 2
+        for k in range(5):
+            for l in range(5):
+                xc, yc = x0 + l, y0 + k
+                if (xc < 0 or xc >= sw) and (yc < 0 or yc >= sh):
+                    continue
+                rr, cc = mirror(yc, sh) - ay, mirror(xc, sw) - ax
+                assert 0 <= rr < rows and 0 <= cc < stride and done[rr, cc], (rr, cc)
+
+    for tid in range(4):
+        x2, y2 = (w2 - 1 if tid & 1 else 0), (h2 - 1 if tid & 2 else 0)
+        if X2 - 3 <= x2 < X2 + 35 and a2y <= y2 < a2y + S2:
+            l2_taps(x2, y2, w1, h1, a1x, a1y, done1, S1, S1S)
+            done2[y2 - a2y, x2 - a2x] = True
+
+    # level 3's image on the tile's 16x16 core (when the pyramid has a level 3)
+    if len(sizes) > 3:
+        w3, h3 = sizes[3]
+        for tid in range(256):
+            x3, y3 = (X2 >> 1) + (tid & 15), (Y2 >> 1) + (tid >> 4)
+            if x3 < w3 and y3 < h3:
+                l2_taps(x3, y3, w2, h2, a2x, a2y, done2, S2, S2S)
+
+    # level-0 outputs: four pixels per item
+    for q in range(128 * 32):
+        y, x = 4 * Y2 + (q >> 5), 4 * X2 + (q & 31) * 4
+        if y >= h0 or x >= w0:
+            continue
+        r, c = y - a0y, x - a0x
+        assert 3 <= r and r + 3 < S0H and c >= 4 and c + 8 <= S0W  # every word read
+        for i in range(4):
+            if x + i >= w0:
+                continue
+            b0(r, c + i)  # the image value
+            if 2 < x + i < w0 - 3:
+                for j in range(-3, 4):
+                    b0(r, c + i + j)
+            if 2 < y < h0 - 3:
+                for j in range(-3, 4):
+                    b0(r + j, c + i)
+
+    # level-1 and level-2 outputs: four pixels per item
+    for q in range(64 * 16 + 32 * 8):
+        lev1 = q < 64 * 16
+        qq = q if lev1 else q - 64 * 16
+        qpr = 16 if lev1 else 8
+        lw, lh = (w1, h1) if lev1 else (w2, h2)
+        y = (2 * Y2 if lev1 else Y2) + qq // qpr
+        x = (2 * X2 if lev1 else X2) + (qq % qpr) * 4
+        if y >= lh or x >= lw:
+            continue
+        rows, stride, done = (S1, S1S, done1) if lev1 else (S2, S2S, done2)
+        r, c = y - (a1y if lev1 else a2y), x - (a1x if lev1 else a2x)
+        assert r >= 3 and r + 3 < rows and c >= 4 and c + 8 <= stride  # every 16-byte read
+
+        def used(rr, cc):
+            assert done[rr, cc], (lev1, rr, cc)
+
+        for i in range(4):
+            if x + i >= lw:
+                continue
+            used(r, c + i)
+            if 2 < x + i < lw - 3:
+                for j in range(-3, 4):
+                    used(r, c + i + j)
+            if 2 < y < lh - 3:
+                for j in range(-3, 4):
+                    used(r + j, c + i)
+
+
+SIZES = [(57, 57), (58, 61), (63, 120), (97, 61), (130, 57), (640, 480), (752, 480), (1241, 376),
+         (1280, 720), (1920, 1200), (2047, 1535), (4096, 4096)]
+
+
+@pytest.mark.parametrize("w,h", SIZES)
+def test_tile_reads_stay_inside_and_use_written_cells(w, h):
+    sizes = level_sizes(w, h)
+    assert len(sizes) >= 3
+    (w2, h2) = sizes[2]
+    for X2, Y2 in tiles(w2, h2):
+        check_tile(sizes, X2, Y2)
+
+
+def test_smallest_frame_of_the_kernel():
+    assert len(level_sizes(57, 57)) >= 3 and len(level_sizes(56, 57)) == 2
