@@ -11,7 +11,11 @@ output must also come from a cell that holds data:
 The kernel runs for frames with at least three levels (level 2 at least 15 px, so the frame is at
 least 57 px), where one reflection of `mirror_index` always lands inside the frame.  Everything
 here is restated from the kernel's source; it checks bounds, not pixel values, which the GPU parity
-tests compare with the oracle."""
+tests compare with the oracle.
+
+The generic stage kernel (pyramid_stage_kernel: FP32 sources, frames with fewer than three levels)
+is restated the same way below: each level's staged region holds every tap of the levels and
+gradients computed from it, mirrored taps included."""
 
 import numpy as np
 import pytest
@@ -177,3 +181,88 @@ def test_tile_reads_stay_inside_and_use_written_cells(w, h):
 
 def test_smallest_frame_of_the_kernel():
     assert len(level_sizes(57, 57)) >= 3 and len(level_sizes(56, 57)) == 2
+
+
+# ---------------------------------------------------------------- generic stages
+# pyramid_stage_kernel<InT, NL, KT>: a CTA owns a KT x KT core of the deepest produced level NL and
+# stages, per level k, the region [a_k, a_k + S_k) in x (the same in y): a_NL = X - 3,
+# a_k = 2 a_{k+1} - 2, S_NL = KT + 6, S_k = 2 S_{k+1} + 3.  Level 0 of the stage is its source.
+
+def region_size(kt, nl, k):
+    return kt + 6 if k == nl else 2 * region_size(kt, nl, k + 1) + 3
+
+
+def check_stage(dims, nl, kt, write_level0, X, Y):
+    a, ay = [0] * (nl + 1), [0] * (nl + 1)
+    a[nl], ay[nl] = X - 3, Y - 3
+    for k in range(nl - 1, -1, -1):
+        a[k], ay[k] = 2 * a[k + 1] - 2, 2 * ay[k + 1] - 2
+    S = [region_size(kt, nl, k) for k in range(nl + 1)]
+    valid = []
+    w, h = dims[0]
+    rr, cc = np.meshgrid(np.arange(S[0]), np.arange(S[0]), indexing="ij")
+    valid.append((a[0] + cc >= 0) & (ay[0] + rr >= 0) & (a[0] + cc < w) & (ay[0] + rr < h))
+    for k in range(1, nl + 1):
+        (sw, sh), (w, h) = dims[k - 1], dims[k]
+        v = np.zeros((S[k], S[k]), bool)
+        for r in range(S[k]):
+            for c in range(S[k]):
+                gx, gy = a[k] + c, ay[k] + r
+                if not (0 <= gx < w and 0 <= gy < h):
+                    continue
+                x0, y0 = 2 * gx - 2, 2 * gy - 2
+                for kk in range(5):
+                    for l in range(5):
+                        xc, yc = x0 + l, y0 + kk
+                        if (xc < 0 or xc >= sw) and (yc < 0 or yc >= sh):
+                            continue
+                        r2, c2 = mirror(yc, sh) - ay[k - 1], mirror(xc, sw) - a[k - 1]
+                        assert 0 <= r2 < S[k - 1] and 0 <= c2 < S[k - 1], (k, r2, c2)
+                        assert valid[k - 1][r2, c2], (k, r2, c2)
+                v[r, c] = True
+        valid.append(v)
+    for k in range(0 if write_level0 else 1, nl + 1):
+        w, h = dims[k]
+        C = kt << (nl - k)
+        cx0, cy0 = X << (nl - k), Y << (nl - k)
+        for r in range(C):
+            for c in range(C):
+                x, y = cx0 + c, cy0 + r
+                if x >= w or y >= h:
+                    continue
+                pr, pc = y - ay[k], x - a[k]
+                taps = [(pr, pc)]
+                if 2 < x < w - 3:
+                    taps += [(pr, pc + j) for j in range(-3, 4)]
+                if 2 < y < h - 3:
+                    taps += [(pr + j, pc) for j in range(-3, 4)]
+                for tr, tc in taps:
+                    assert 0 <= tr < S[k] and 0 <= tc < S[k] and valid[k][tr, tc], (k, tr, tc)
+
+
+def halvings(w, h, n):
+    dims = [(w, h)]
+    for _ in range(n):
+        w, h = (w + 1) // 2, (h + 1) // 2
+        dims.append((w, h))
+    return dims
+
+
+STAGE_SOURCES = [(1, 1), (5, 7), (15, 15), (16, 29), (29, 29), (30, 31), (57, 57), (97, 61), (130, 57),
+                 (640, 480), (1241, 376)]
+
+
+@pytest.mark.parametrize("nl", [0, 1, 2])
+@pytest.mark.parametrize("kt", [8, 16])
+def test_stage_regions_hold_every_tap(nl, kt):
+    for w, h in STAGE_SOURCES:
+        dims = halvings(w, h, nl)
+        if any(dw < 15 or dh < 15 for dw, dh in dims[1:]):
+            continue  # the planner never produces a level below 15 px
+        dw, dh = dims[nl]
+        tx, ty = -(-dw // kt), -(-dh // kt)
+        xs = sorted({0, 1, tx // 2, tx - 2, tx - 1} & set(range(tx)))
+        ys = sorted({0, 1, ty // 2, ty - 2, ty - 1} & set(range(ty)))
+        for ty_ in ys:
+            for tx_ in xs:
+                check_stage(dims, nl, kt, True, tx_ * kt, ty_ * kt)
