@@ -87,14 +87,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) lk_kernel(const __grid_const
 
 template <int SAMPLING, bool HORIZ, int MODE, int WARPS, int MINB>
 cudaError_t launch_shape(const LkLaunch& p, cudaStream_t s) {
-  static int resident = 0;  // blocks of this shape resident on the device (persistent grid)
-  if (!resident) {
+  // blocks of this shape resident on the device (persistent grid), found once per process
+  static const int resident = [] {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lk_kernel<SAMPLING, HORIZ, MODE, WARPS, MINB>, WARPS * 32, 0);
-    resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-  }
+    return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }();
   int blocks = (p.total + WARPS - 1) / WARPS;
   if (p.counter) blocks = min(blocks, resident);
   lk_kernel<SAMPLING, HORIZ, MODE, WARPS, MINB><<<blocks, WARPS * 32, 0, s>>>(p);

@@ -595,14 +595,14 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjoint_kernel(const __grid
 
 template <int MODE>
 int adjoint_blocks() {
-  static int blocks = 0;
-  if (!blocks) {
+  // blocks resident on the device, found once per process
+  static const int blocks = [] {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<MODE>, kAdjWarps * 32, 0);
-    blocks = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-  }
+    return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }();
   return blocks;
 }
 

@@ -906,16 +906,15 @@ bool encode_frame_tmap(StageJob& job) {
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static Encode encode = nullptr;
-  static bool looked_up = false;
-  if (!looked_up) {
+  // looked up once per process; the initialisation of a function-local static is thread-safe
+  static const Encode encode = []() -> Encode {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      encode = reinterpret_cast<Encode>(fn);
-    looked_up = true;
-  }
+      return reinterpret_cast<Encode>(fn);
+    return nullptr;
+  }();
   job.use_tma = 0;
   if (!encode) return false;
   // TMA needs a 16-byte aligned base and pitch; frames smaller than the box use plain loads

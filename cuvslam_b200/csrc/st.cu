@@ -640,14 +640,14 @@ __global__ void __launch_bounds__(kWarps * 32) st_build_kernel(const __grid_cons
 
 template <int SAMPLING, bool CACHED>
 cudaError_t launch_track(const StLaunch& p, cudaStream_t s) {
-  static int resident = 0;  // blocks resident on the device (persistent grid)
-  if (!resident) {
+  // blocks resident on the device (persistent grid), found once per process
+  static const int resident = [] {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, st_track_kernel<SAMPLING, CACHED>, kWarps * 32, 0);
-    resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-  }
+    return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }();
   cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   const int blocks = min((p.n + kWarps - 1) / kWarps, resident);

@@ -250,14 +250,14 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) stereo_kernel(const _
 
 template <int SAMPLING, bool HORIZ>
 cudaError_t launch_sampling(const StereoLaunch& p, cudaStream_t s) {
-  static int resident = 0;
-  if (!resident) {
+  // blocks resident on the device (persistent grid), found once per process
+  static const int resident = [] {
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stereo_kernel<SAMPLING, HORIZ>, kWarps * 32, 0);
-    resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-  }
+    return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }();
   const long long total = (long long)p.rounds * p.round;
   const int blocks = (int)max(1LL, min((long long)resident, (total + kWarps - 1) / kWarps));
   stereo_kernel<SAMPLING, HORIZ><<<blocks, kWarps * 32, 0, s>>>(p);

@@ -8,6 +8,9 @@
  *   - take device pointers, sizes in elements/pixels and pitches in BYTES;
  *   - enqueue work on the caller's stream and return without synchronising, unless stated;
  *   - return an fe_status code and never throw across the ABI.
+ * A context, a batch or an adjoint plan is used by one host thread at a time, as the reference's
+ * wrapper objects are (not thread-safe per object); distinct contexts are independent.  Entries
+ * that share state across streams say so (fe_select, fe_select_noalloc, the affine tracker).
  * Citations are to cuVSLAM 18.0.0 (libs/...).
  */
 #ifndef CUVSLAM_FE_H
