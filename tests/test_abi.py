@@ -87,3 +87,81 @@ def test_track_record_layout():
     assert TRACK_DTYPE.fields["ncc"][1] == 72
     t = np.zeros(1, TRACK_DTYPE)
     assert t.view(np.uint8).size == 80
+
+
+def _c_layout(structs, fields, constants):
+    """sizeof and offsetof of the header's structs, and the values of its constants, as a C
+    compiler lays them out (gcc on the header)."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "cuvslam_fe.h"', "int main(void) {"]
+    for s in structs:
+        lines.append(f'  printf("sizeof {s} %zu\\n", sizeof({s}));')
+        for f in fields[s]:
+            lines.append(f'  printf("offset {s}.{f} %zu\\n", offsetof({s}, {f}));')
+    for c in constants:
+        lines.append(f'  printf("const {c} %d\\n", (int)({c}));')
+    lines.append("  return 0;\n}")
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run([gcc, "-std=c99", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    got = {}
+    for line in out.splitlines():
+        kind, name, value = line.split()
+        got[(kind, name)] = int(value)
+    return got
+
+
+def test_ctypes_structs_match_the_header():
+    """Every ctypes restatement in _lib.py has the header's size, field names and offsets, and the
+    Python constants equal the header's."""
+    import ctypes
+
+    from cuvslam_b200 import frontend
+
+    pairs = {"fe_pyramid": _lib.FePyramid, "fe_track_finish": _lib.FeTrackFinish,
+             "fe_finish_camera": _lib.FeFinishCamera, "fe_camera_frame": _lib.FeCameraFrame,
+             "fe_adjoint_job": _lib.FeAdjointJob, "fe_epipolar_curves": _lib.FeEpipolarCurves,
+             "fe_stereo_pair": _lib.FeStereoPair}
+    fields = {c: [f[0] for f in py._fields_] for c, py in pairs.items()}
+    fields["fe_track_data"] = ["track", "offset", "info", "track_status", "cache_index", "initial_guess_map",
+                               "search_radius_px", "ncc_threshold", "ncc"]
+    fields["fe_affine_cache"] = ["patch", "patch_sums", "level_mask"]
+    constants = ["FE_MAX_LEVELS", "FE_ABI_VERSION", "FE_OK", "FE_ERR_INVALID_ARGUMENT", "FE_SAMPLE_TEXTURE",
+                 "FE_SAMPLE_EXACT", "FE_SAMPLE_TEXTURE_WIDE", "FE_SAMPLE_HARDWARE", "FE_ADJOINT_IMPLICIT",
+                 "FE_ADJOINT_UNROLLED"]
+    c = _c_layout(list(fields), fields, constants)
+    for name, py in pairs.items():
+        assert c[("sizeof", name)] == ctypes.sizeof(py), name
+        for f in fields[name]:
+            assert c[("offset", f"{name}.{f}")] == getattr(py, f).offset, (name, f)
+    assert c[("sizeof", "fe_track_data")] == TRACK_DTYPE.itemsize
+    for f in fields["fe_track_data"]:
+        assert c[("offset", f"fe_track_data.{f}")] == TRACK_DTYPE.fields[f][1], f
+    assert c[("sizeof", "fe_affine_cache")] == frontend.AFFINE_CACHE_BYTES
+    assert c[("const", "FE_MAX_LEVELS")] == _lib.MAX_LEVELS
+    for k in constants[2:]:
+        assert c[("const", k)] == getattr(_lib, k), k
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
+def test_header_is_plain_c_and_cxx(lang, std):
+    """The header compiles alone, warning-free and pedantic, for C consumers (ctypes, cgo, JNI stubs)
+    and for C++."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("compiler not available")
+    r = subprocess.run([cc, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-I",
+                        os.path.join(ROOT, "include"), "-x", lang, "-"], input='#include "cuvslam_fe.h"\n',
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
