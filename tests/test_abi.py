@@ -165,3 +165,41 @@ def test_header_is_plain_c_and_cxx(lang, std):
                         os.path.join(ROOT, "include"), "-x", lang, "-"], input='#include "cuvslam_fe.h"\n',
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def _prototypes():
+    """name -> (return type, [parameter types]) of every FE_API declaration, comments removed."""
+    src = open(os.path.join(ROOT, "include", "cuvslam_fe.h")).read()
+    src = re.sub(r"/\*.*?\*/", " ", src, flags=re.S)
+    out = {}
+    for ret, name, params in re.findall(r"FE_API\s+([\w\s\*]+?)\b(fe_\w+)\s*\(([^)]*)\)\s*;", src):
+        types = []
+        for p in [p.strip() for p in params.split(",") if p.strip() and p.strip() != "void"]:
+            types.append(re.sub(r"\s*\b\w+$", "", p) if re.search(r"[\w\*]\s+\**\w+$", p) else p)
+        out[name] = (" ".join(ret.split()), [" ".join(t.replace("*", " * ").split()) for t in types])
+    return out
+
+
+def _c_kind(t):
+    if "*" in t or t in ("fe_stream",):
+        return "ptr"
+    return {"int": "i32", "int32_t": "i32", "int64_t": "i64", "float": "f32", "size_t": "i64"}[t]
+
+
+def _py_kind(t):
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+        return "ptr"
+    return {ctypes.c_int: "i32", ctypes.c_int32: "i32", ctypes.c_int64: "i64", ctypes.c_float: "f32"}[t]
+
+
+def test_ctypes_signatures_match_the_prototypes():
+    """Each _lib.py signature has the header prototype's arity, and every argument and return value
+    the same kind (pointer, 32-bit or 64-bit integer, float)."""
+    protos = _prototypes()
+    assert sorted(protos) == sorted(_lib._SIGS)
+    for name, (res, args) in _lib._SIGS.items():
+        cret, cargs = protos[name]
+        assert len(args) == len(cargs), (name, len(args), len(cargs))
+        assert _py_kind(res) == _c_kind(cret), (name, cret)
+        for i, (a, ca) in enumerate(zip(args, cargs)):
+            assert _py_kind(a) == _c_kind(ca), (name, i, ca)
