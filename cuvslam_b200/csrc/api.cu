@@ -1836,7 +1836,7 @@ int fe_adjoint_backward(fe_adjoint* a, fe_stream stream) {
 }
 
 int fe_adjoint_kernel_count(const fe_adjoint* a, int backward) {
-  if (!a) return 0;
+  if (!a) return -1;
   if (backward == 2) {  // pyramid builds
     int n = 0;
     for (const auto& stage : a->build) n += (int)stage.size();

@@ -387,7 +387,8 @@ typedef enum {
 } fe_batch_part;
 /* Enqueues one part of the planned step directly (no graph). */
 FE_API int fe_batch_run_part(fe_batch* batch, int part, fe_stream stream);
-/* Number of kernel launches in one fe_batch_run (kernel nodes of the captured graph). */
+/* Number of kernel launches in one fe_batch_run (kernel nodes of the captured graph); -1 for a
+ * NULL batch. */
 FE_API int fe_batch_kernel_count(fe_batch* batch);
 /* The same step as a plain per-camera sequence of fe_build_pyramid / fe_track / fe_select
  * (the drop-in launch pattern), for comparison. */
@@ -464,7 +465,8 @@ FE_API int fe_adjoint_forward(fe_adjoint* adj, fe_stream stream);
  * Unrolled mode uses the iterates the plan's last forward recorded; before any forward it replays
  * the forward itself. */
 FE_API int fe_adjoint_backward(fe_adjoint* adj, fe_stream stream);
-/* Kernel launches of one forward (backward = 0), backward (1) or build_pyramids (2) call. */
+/* Kernel launches of one forward (backward = 0), backward (1) or build_pyramids (2) call; -1 for a
+ * NULL plan. */
 FE_API int fe_adjoint_kernel_count(const fe_adjoint* adj, int backward);
 /* Enqueues a copy, into the device int32 at `device_out`, of the number of tracks of the last
  * backward whose unrolled iterates on one level spread over more than 20 texels: those get NaN

@@ -203,3 +203,34 @@ def test_ctypes_signatures_match_the_prototypes():
         assert _py_kind(res) == _c_kind(cret), (name, cret)
         for i, (a, ca) in enumerate(zip(args, cargs)):
             assert _py_kind(a) == _c_kind(ca), (name, i, ca)
+
+
+def test_every_entry_rejects_null_handles():
+    """Every entry point called with NULL pointers and zero sizes returns FE_ERR_INVALID_ARGUMENT
+    (the two launch-count queries: -1) without touching a device, each in a child process so that
+    a crash would show as a failure rather than end the test run."""
+    import subprocess
+    import sys
+
+    host_only = {"fe_abi_version", "fe_status_string", "fe_last_cuda_error", "fe_pyramid_levels", "fe_pyramid_bytes"}
+    names = [n for n in _lib._SIGS if n not in host_only]
+    code = """
+import ctypes, json, sys
+from cuvslam_b200 import _lib
+lib = _lib.load()
+out = {}
+for name in sys.argv[1:]:
+    res, args = _lib._SIGS[name]
+    vals = [0.0 if a is ctypes.c_float else (0 if a in (ctypes.c_int, ctypes.c_int64) else None) for a in args]
+    out[name] = getattr(lib, name)(*vals)
+print(json.dumps(out))
+"""
+    r = subprocess.run([sys.executable, "-c", code] + names, capture_output=True, text=True, timeout=120,
+                       cwd=ROOT, env={**os.environ, "PYTHONPATH": ROOT})
+    assert r.returncode == 0, r.stderr
+    import json
+
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    for name in names:
+        want = -1 if name.endswith("kernel_count") else _lib.FE_ERR_INVALID_ARGUMENT
+        assert got[name] == want, (name, got[name])
