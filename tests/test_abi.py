@@ -234,3 +234,28 @@ print(json.dumps(out))
     for name in names:
         want = -1 if name.endswith("kernel_count") else _lib.FE_ERR_INVALID_ARGUMENT
         assert got[name] == want, (name, got[name])
+
+
+_CITE = re.compile(r"\b[\w/]+\.(?:cpp|cu|cuh|h):\d+|counterpart")
+# entries that replace a reference interface: each cites it in its own comment
+_DROP_IN = ["fe_create", "fe_build_pyramid", "fe_build_pyramid_rgb", "fe_build_pyramid_f32", "fe_select", "fe_track",
+            "fe_track_mono", "fe_track_stereo", "fe_finish_tracks", "fe_track_affine", "fe_affine_build_cache",
+            "fe_track_affine_cached", "fe_pyramid_levels"]
+
+
+def test_header_cites_the_reference_it_replaces():
+    """Each declaration's section of the header, from its banner down to the declaration, cites a
+    reference file:line or says the entry has no counterpart; the drop-in entries cite it in the
+    comment right above them."""
+    src = open(os.path.join(ROOT, "include", "cuvslam_fe.h")).read()
+    banners = [m.start() for m in re.finditer(r"/\* -{20,} \*/\n/\*", src)]
+    decls = list(re.finditer(r"FE_API\s+[\w\s\*]+?\b(fe_\w+)\s*\(", src))
+    for m in decls:
+        start = max([b for b in banners if b < m.start()], default=0)
+        assert _CITE.search(src[start:m.start()]), m.group(1)
+    for m in decls:
+        if m.group(1) not in _DROP_IN:
+            continue
+        before = src[:m.start()]
+        comment = before[before.rfind("/*"):before.rfind("*/")]
+        assert _CITE.search(comment) and "counterpart" not in comment, m.group(1)
