@@ -23,7 +23,8 @@ _MODES = {"implicit": IMPLICIT, "unrolled": UNROLLED, IMPLICIT: IMPLICIT, UNROLL
 
 
 class DiffTracker:
-    """Differentiable LK over `batch` cameras of one size with `n_tracks` tracks each.
+    """Differentiable LK over `batch` cameras of one size with `n_tracks` tracks each (no counterpart
+    in the reference, which has no backward).
 
     Owns the frames (`prev_img`, `cur_img`, as given: the intensity scale is applied inside the
     pyramid build), the pyramids, the track records and the gradient buffers, and one fe_adjoint

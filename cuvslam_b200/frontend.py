@@ -29,7 +29,8 @@ def _ptr(t):
 
 
 class Context:
-    """Owns the library's per-device scratch (fe_create / fe_destroy)."""
+    """Owns the library's per-device scratch (fe_create / fe_destroy): the per-wrapper state of
+    GPUSelection and GPULKFeatureTracker (selection_v2.h:28-58, lk_tracker.h:27-37)."""
 
     def __init__(self, device=0):
         self.lib = _lib.load()
@@ -52,7 +53,8 @@ class Context:
 
 
 class ImagePyramid:
-    """Image pyramid + gradient pyramid in one device buffer (fe_pyramid)."""
+    """Image pyramid + gradient pyramid in one device buffer (fe_pyramid): GaussianGPUImagePyramid +
+    GPUGradientPyramid (image_pyramid.h:56-162, gradient_pyramid.h:30-59)."""
 
     def __init__(self, width, height, max_levels=10, device="cuda"):
         lib = _lib.load()
@@ -129,14 +131,16 @@ class ImagePyramid:
 
 
 def track_mono(ctx, prev, cur, tracks, retrack_ncc=0.85, sampling=_lib.FE_SAMPLE_TEXTURE, stream=None):
-    """MonoSOFGPU::launch's track + retrack passes as collect merges them (fe_track_mono)."""
+    """MonoSOFGPU::launch's track + retrack passes as collect merges them (fe_track_mono;
+    sof_mono_gpu.cpp:34-104)."""
     _lib.check(ctx.lib.fe_track_mono(ctx.handle, ctypes.byref(prev.desc), ctypes.byref(cur.desc), _ptr(tracks),
                                      tracks.shape[0], ctypes.c_float(retrack_ncc), int(sampling),
                                      _stream_handle(stream)), "fe_track_mono")
 
 
 def tracks_to_device(tracks, device="cuda"):
-    """TRACK_DTYPE records -> (n, 80) uint8 CUDA tensor (the TrackData array the kernels update)."""
+    """TRACK_DTYPE records -> (n, 80) uint8 CUDA tensor (the TrackData array the kernels update,
+    cuda_kernels.h:76-87)."""
     arr = np.ascontiguousarray(tracks, dtype=TRACK_DTYPE)
     return torch.from_numpy(arr.view(np.uint8).reshape(len(arr), 80).copy()).to(device)
 
@@ -146,7 +150,8 @@ def tracks_from_device(t):
 
 
 class LKFeatureTracker:
-    """GPULKFeatureTracker (horizontal=False) / GPULKTrackerHorizontal (horizontal=True)."""
+    """GPULKFeatureTracker (horizontal=False) / GPULKTrackerHorizontal (horizontal=True):
+    track_points of cuda_modules/lk_tracker.cpp:24-73 (kernels lk_tracker.cu:69-379, 381-665)."""
 
     def __init__(self, ctx, horizontal=False, sampling=_lib.FE_SAMPLE_TEXTURE):
         self.ctx = ctx
@@ -237,7 +242,8 @@ class STFeatureTrackerWithCache(STFeatureTracker):
 
 
 class Selection:
-    """GPUSelection: Shi-Tomasi response + deterministic feature selection on pyramid level 0."""
+    """GPUSelection: Shi-Tomasi response + deterministic feature selection on pyramid level 0
+    (computeGFTTAndSelectFeatures, selection_v2.cpp:27-184)."""
 
     def __init__(self, ctx):
         self.ctx = ctx
@@ -290,7 +296,8 @@ class _DeviceArray:
 
 
 class TrackFinish:
-    """MonoSOFGPU's retrack pass and finish filters for one camera (fe_track_finish).  age: (n,)
+    """MonoSOFGPU's retrack pass and finish filters for one camera (fe_track_finish;
+    sof_mono_gpu.cpp:80-104,144-208, sof_mono_base.cpp:40-125).  age: (n,)
     int32/uint32 CUDA tensor of track ages (0 = dead), updated in place; predicted: optional (n, 2)
     float32 CUDA tensor (NaN = no prediction); mask: optional (h, w) uint8 CUDA tensor."""
 
@@ -327,7 +334,9 @@ def finish_tracks(ctx, tracks, finish, width, height, border=(0, 0, 0, 0), strea
 
 
 class CameraFrame:
-    """One camera of a batched frame step (fe_camera_frame); finish: optional TrackFinish."""
+    """One camera of a batched frame step (fe_camera_frame); finish: optional TrackFinish.  No
+    counterpart in the reference, which runs cameras one after another
+    (MultiSOFBase::trackNextFrame, sof_multicamera_base.cpp:62-116)."""
 
     def __init__(self, image_u8, cur, prev=None, tracks=None, num_desired=0, border=(0, 0, 0, 0), finish=None):
         self.image = image_u8.contiguous()
@@ -343,7 +352,8 @@ class CameraFrame:
 
 
 class Batch:
-    """Batched multi-camera frame step captured in a CUDA graph (fe_batch_*)."""
+    """Batched multi-camera frame step captured in a CUDA graph (fe_batch_*); no counterpart in the
+    reference (sof_multicamera_base.cpp:62-116 loops over the cameras)."""
 
     def __init__(self, ctx, frames, sampling=_lib.FE_SAMPLE_TEXTURE):
         self.ctx = ctx
