@@ -1,5 +1,8 @@
 // C ABI of the front-end (include/cuvslam_fe.h): argument checking, scratch management, launch
-// planning for single cameras and batches, and CUDA-graph capture of batched frame steps.
+// planning for single cameras and batches, and CUDA-graph capture of batched frame steps.  It takes
+// the place of the reference's host wrappers: GaussianGPUImagePyramid::build (image_pyramid.h:81-98),
+// GPUGradientPyramid::set (gradient_pyramid.cpp:83-118), GPUSelection::computeGFTTAndSelectFeatures
+// (selection_v2.cpp:27-184) and GPULKFeatureTracker::track_points (cuda_modules/lk_tracker.cpp:24-73).
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -2,7 +2,9 @@
 // contributions to the pyramids' planes as small window records; a tile-segmented reduction sums
 // the records of every 32x32 tile of every plane in track order; the pyramid adjoint then applies
 // the transposed gradient filters and the transposed 5x5 decimation from the top level down to the
-// level-0 images.  Everything is deterministic: no floating-point atomics.
+// level-0 images.  Everything is deterministic: no floating-point atomics.  No counterpart in the
+// reference, which has no backward; the forward it differentiates follows lk_track_kernel's rule
+// (lk_tracker.cu:69-379).
 //
 // Forward model (lk_track.cuh, exact bilinear sampling): per level l a template at s_l
 // (P1, Gx, Gy on the 9x9 taps; a = Gx - mean, b = Gy - mean; H = I + sum w g g^T) and steps

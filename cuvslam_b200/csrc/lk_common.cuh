@@ -1,5 +1,7 @@
 // Shared device pieces of the LK tracker (lk.cu) and its adjoint (lk_adjoint.cu): window sizes,
 // the bilinear tap geometry of a 9x9 patch, sampling from shared-memory windows and window staging.
+// The taps are those lk_track_kernel fetches from its linear-filtered textures (lk_tracker.cu:69-379,
+// texture setup cuda_helper.h:402-431).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -9,6 +9,7 @@
 // every GPU that loads the library holds until the process exits.
 //
 // The kernels are the ones fe_select launches (select.cu); only where their scratch lives differs.
+// No counterpart in the reference (GPUSelection allocates its buffers, selection_v2.h:28-58).
 #include <cuda_runtime.h>
 
 #include <algorithm>
