@@ -13,6 +13,11 @@ MAX_LEVELS = 10
 
 FE_OK = 0
 FE_ERR_INVALID_ARGUMENT = 1
+FE_ERR_CUDA = 2
+FE_ERR_OUT_OF_MEMORY = 3
+FE_ERR_CAPACITY = 4
+FE_ERR_DEVICE_FAULT = 5
+FE_DEFAULT_WAIT_LIMIT = 1 << 22
 FE_SAMPLE_TEXTURE = 0
 FE_SAMPLE_EXACT = 1
 FE_SAMPLE_TEXTURE_WIDE = 2
@@ -143,6 +148,8 @@ _SIGS = {
     "fe_last_cuda_error": (_I, []),
     "fe_create": (_I, [_I, ctypes.POINTER(_P)]),
     "fe_destroy": (_I, [_P]),
+    "fe_device_status": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int32)]),
+    "fe_set_wait_limit": (_I, [_P, _I]),
     "fe_pyramid_levels": (_I, [_I, _I, _I]),
     "fe_pyramid_bytes": (_I64, [_I, _I, _I]),
     "fe_pyramid_init": (_I, [_P, _I64, _I, _I, _I, ctypes.POINTER(FePyramid)]),

@@ -25,14 +25,8 @@ namespace {
 
 thread_local int g_last_cuda_error = 0;
 
-// cudaMalloc that leaves no error state behind when it succeeds: the runtime has been seen to return
-// success from cudaMalloc while recording cudaErrorInvalidValue as the thread's last error, which the
-// next kernel launch's cudaGetLastError() check would then report as its own failure.
-cudaError_t dev_alloc(void** p, size_t bytes) {
-  const cudaError_t e = cudaMalloc(p, bytes);
-  if (e == cudaSuccess) (void)cudaGetLastError();
-  return e;
-}
+// Every device allocation of the library (one place to count or instrument them).
+cudaError_t dev_alloc(void** p, size_t bytes) { return cudaMalloc(p, bytes); }
 
 int cuda_fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
@@ -286,6 +280,8 @@ struct fe_context {
   void* stereo_mem = nullptr;  // left-to-right matching scratch (grown on demand)
   size_t stereo_bytes = 0;
   bool debug = false;
+  int* dev_status = nullptr;  // device flags the kernels set (fe_device_status reads and clears them)
+  int wait_limit = fe::kDefaultWaitLimit;  // bounded waits' iteration limit (fe_set_wait_limit)
   // FE_SAMPLE_HARDWARE: texture objects of the planes tracked on, created on first use
   struct Tex {
     const void* ptr;
@@ -297,6 +293,16 @@ struct fe_context {
 };
 
 namespace {
+
+// Points every pyramid launch of a plan at the context's device status word and gives it the
+// context's wait limit.
+void stamp_plan(StagePlan& plan, const fe_context* ctx) {
+  for (auto& stage : plan)
+    for (auto& g : stage) {
+      g.batch.status = ctx->dev_status;
+      g.batch.wait_limit = ctx->wait_limit;
+    }
+}
 
 // The texture object (linear filtering, clamped, unnormalised coordinates: the reference's sampling
 // of its pyramid planes) of one plane, from the context's cache or created now.
@@ -401,7 +407,7 @@ int sel_caps(int w, int h, int n_alive, int num_desired, int* bin_key_cap, int* 
   }
   *bin_key_cap = next_pow2(mx);
   const int cells = std::max(cw * ch, 1);
-  *q_cap = std::min(cells, std::max(n_alive, 0) + num_desired + 64);
+  *q_cap = (int)std::min<int64_t>(cells, (int64_t)std::max(n_alive, 0) + num_desired + 64);
   *final_key_cap = next_pow2(*q_cap);
   if (*bin_key_cap > 16384 || *final_key_cap > 16384) return FE_ERR_CAPACITY;
   return FE_OK;
@@ -495,9 +501,12 @@ int fe_create(int device, fe_context** out) {
   cudaError_t e = dev_alloc((void**)&c->lk_counter, 256);
   if (e == cudaSuccess) e = dev_alloc((void**)&c->stage_done, 64 * 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->stage_done, 0, 64 * 8 * sizeof(int));
+  if (e == cudaSuccess) e = dev_alloc((void**)&c->dev_status, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->dev_status, 0, 4 * sizeof(int));
   if (e != cudaSuccess) {
     if (c->lk_counter) cudaFree(c->lk_counter);
     if (c->stage_done) cudaFree(c->stage_done);
+    if (c->dev_status) cudaFree(c->dev_status);
     delete c;
     return cuda_fail(e);
   }
@@ -511,6 +520,7 @@ int fe_destroy(fe_context* ctx) {
   if (ctx->sel.mem) cudaFree(ctx->sel.mem);
   if (ctx->lk_counter) cudaFree(ctx->lk_counter);
   if (ctx->stage_done) cudaFree(ctx->stage_done);
+  if (ctx->dev_status) cudaFree(ctx->dev_status);
   if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
   if (ctx->finish_cells) cudaFree(ctx->finish_cells);
   if (ctx->sel.resp) cudaFree(ctx->sel.resp);
@@ -561,7 +571,7 @@ int build_from_level0(fe_context* ctx, const fe_pyramid* pyr, cudaStream_t s) {
   StagePlan plan;
   int rc = plan_pyramid(pyr->image[0], pyr->pitch_bytes[0], false, *pyr, plan);
   if (rc) return rc;
-  (void)ctx;
+  stamp_plan(plan, ctx);
   return run_plan(plan, s);
 }
 
@@ -583,6 +593,7 @@ int fe_build_pyramid(fe_context* ctx, const uint8_t* image, int64_t image_pitch_
   int rc = plan_pyramid(image, image_pitch_bytes, true, *pyr, plan, 1.f, 8, done, &used, 4, box3 != 0);
   if (!rc) rc = finish_l012_plan(plan, done + 4, &nq, 2);
   if (rc) return rc;
+  stamp_plan(plan, ctx);
   return run_plan(plan, (cudaStream_t)stream);
 }
 
@@ -606,6 +617,7 @@ int fe_build_pyramid_f32(fe_context* ctx, const float* image, int64_t image_pitc
   StagePlan plan;
   int rc = plan_pyramid(image, image_pitch_bytes, false, *pyr, plan);
   if (rc) return rc;
+  stamp_plan(plan, ctx);
   return run_plan(plan, (cudaStream_t)stream);
 }
 
@@ -649,6 +661,23 @@ int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int border
   c.out_count = out_count;
   c.tile_begin = 0;
   FE_CUDA(fe::launch_select(b, c.tiles_x * c.tiles_y, bin_cap, final_cap, st));
+  return FE_OK;
+}
+
+int fe_device_status(fe_context* ctx, fe_stream stream, int32_t* flags) {
+  if (!ctx) return FE_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  int h[4] = {0, 0, 0, 0};
+  FE_CUDA(cudaStreamSynchronize(st));
+  FE_CUDA(cudaMemcpy(h, ctx->dev_status, sizeof(h), cudaMemcpyDeviceToHost));
+  FE_CUDA(cudaMemset(ctx->dev_status, 0, sizeof(h)));
+  if (flags) *flags = h[0];
+  return h[0] ? FE_ERR_DEVICE_FAULT : FE_OK;
+}
+
+int fe_set_wait_limit(fe_context* ctx, int iterations) {
+  if (!ctx || iterations < 0) return FE_ERR_INVALID_ARGUMENT;
+  ctx->wait_limit = iterations;
   return FE_OK;
 }
 
@@ -1056,6 +1085,7 @@ int replan_pyramids(fe_batch* b, int kt) {
   int nq = 0;
   int rc = finish_l012_plan(plan, b->stage_done + 4 * b->ncams, &nq, 8);
   if (rc) return rc;
+  stamp_plan(plan, b->ctx);
   b->plan = std::move(plan);
   b->stage_tile = kt;
   return FE_OK;
@@ -1736,6 +1766,7 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
                         2 * njobs);
     if (rc) return fail(rc);
   }
+  stamp_plan(a->build, ctx);
 
   memset(&a->adj, 0, sizeof(a->adj));
   a->adj.cams = (const fe::AdjCam*)(base + o_cams);

@@ -37,8 +37,12 @@ struct alignas(64) StageJob {
 
 constexpr int kMaxStageJobs = 48;  // jobs per launch (the job table is a kernel parameter)
 
+// Default iteration limit of the levels 0-2 kernel's bounded waits (a few hundred ms at most).
+constexpr int kDefaultWaitLimit = 1 << 22;
+
 struct StageBatch {
   int njobs;
+  int wait_limit;           // iterations of a bounded wait before it gives up (0: at once)
   int* status;              // device flags: bit 0 = a TMA wait ran out (tile skipped), bit 1 = a
                             // deeper-level item's wait ran out (item skipped)
   int* queue;               // levels 0-2 kernel with deeper-level items: [0] next item, [1] CTAs

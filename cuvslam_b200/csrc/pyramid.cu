@@ -282,9 +282,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Bounded wait on an mbarrier phase: false when it ran out (the caller reports it and gives up).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-  for (int i = 0; i < (1 << 22); ++i) {
+// Bounded wait on an mbarrier phase: false when `limit` polls all found it incomplete (the caller
+// reports it and gives up).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int limit) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -409,12 +410,13 @@ __device__ void rest_item(const Level* tail, int n, float* sm) {
   }
 }
 
-// Thread 0 waits (bounded) until *ctr >= target; false (and status bit 1) when the wait ran out.
+// Thread 0 waits (at most batch.wait_limit polls) until *ctr >= target; false (and status bit 1)
+// when the wait ran out.
 __device__ bool wait_count(const StageBatch& batch, int* ctr, int target) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     int ok = 0;
-    for (int i = 0; i < (1 << 22); ++i) {
+    for (int i = 0; i < batch.wait_limit; ++i) {
       if (*reinterpret_cast<volatile int*>(ctr) >= target) {
         ok = 1;
         break;
@@ -430,7 +432,8 @@ __device__ bool wait_count(const StageBatch& batch, int* ctr, int target) {
 }
 
 // Deeper-level item idx of job J.  J.done: [0] tiles finished, [1] phase-3 bands, [2] phase-4
-// bands; the rest item, the job's last, returns them to zero for the next launch.
+// bands; the launch's last CTA returns them to zero for the next launch (not the rest item: if one
+// of its waits gave up, tiles and bands may still be counting).
 __device__ void deep_item(const StageBatch& batch, const StageJob& J, int idx, float* sm) {
   int* ctr = J.done;
   const int ntiles = J.tiles_x * J.tiles_y;
@@ -448,12 +451,6 @@ __device__ void deep_item(const StageBatch& batch, const StageJob& J, int idx, f
     const int r = J.deep_rest;
     if (wait_count(batch, r == 0 ? ctr : ctr + r, r == 0 ? ntiles : J.deep_bands[r - 1]))
       rest_item(J.tail + r, J.tail_levels - r, sm);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      ctr[0] = 0;
-      ctr[1] = 0;
-      ctr[2] = 0;
-    }
   }
 }
 
@@ -551,11 +548,12 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
           "l"(reinterpret_cast<uint64_t>(&job.tmap)), "r"(a0x), "r"(a0y), "r"(smem_u32(bar))
           : "memory");
     }
-    const bool ok = mbar_wait(bar, 0);
+    const bool ok = mbar_wait(bar, 0, batch.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0 && batch.status) atomicOr(batch.status, 1);
-      // the copy may still land: wait once more (bounded) so no write targets a retired CTA
-      mbar_wait(bar, 0);
+      // the copy may still land: wait once more, with the full bound whatever the launch's limit, so
+      // no write targets a retired CTA
+      mbar_wait(bar, 0, kDefaultWaitLimit);
       if (job.tail_levels > 0 && tid == 0) atomicAdd(job.done, 1);  // still counted (its level 3 is not written)
       return;
     }
@@ -819,11 +817,22 @@ __global__ void __launch_bounds__(kThreads, MINB) pyramid_l012_kernel(const __gr
     }
   }
   if (batch.queue) {
-    // the last CTA to finish returns the queue to zero for the next launch
+    // the last CTA to finish returns the queue and the jobs' item counters to zero for the next
+    // launch: every other CTA has counted itself finished after its own counter updates
     __syncthreads();
-    if (tid == 0 && atomicAdd(batch.queue + 1, 1) == (int)gridDim.x - 1) {
-      batch.queue[0] = 0;
-      batch.queue[1] = 0;
+    if (tid == 0) {
+      __threadfence();
+      if (atomicAdd(batch.queue + 1, 1) == (int)gridDim.x - 1) {
+        __threadfence();
+        for (int k = 0; k < batch.njobs; ++k)
+          if (batch.job[k].tail_levels > 0) {
+            batch.job[k].done[0] = 0;
+            batch.job[k].done[1] = 0;
+            batch.job[k].done[2] = 0;
+          }
+        batch.queue[0] = 0;
+        batch.queue[1] = 0;
+      }
     }
   }
 }

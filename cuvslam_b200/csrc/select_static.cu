@@ -25,7 +25,7 @@ namespace {
 // Limits of the static scratch.
 constexpr int kMaxW = 2048;
 constexpr int kMaxH = 2048;
-constexpr int kMaxKept = 16384;  // kept candidates: n_alive + num_desired + 64 rounded down to this
+constexpr int kMaxKept = 16384;  // kept candidates: min(cells, n_alive + num_desired + 64), fe_select's limit
 
 constexpr size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
@@ -66,12 +66,17 @@ std::mutex g_setup_lock;
 void* g_scratch_addr[kMaxDevices] = {};
 
 // Once per device, with that device current: the scratch's device address and the selection
-// kernels' shared-memory attributes.
-int setup_current_device(void** addr) {
+// kernels' shared-memory attributes.  That set-up cannot run inside a stream capture (the symbol
+// lookup and attribute calls are not capturable): a first call on a device made while `stream`
+// captures is refused with FE_ERR_INVALID_ARGUMENT before anything is enqueued.
+int setup_current_device(cudaStream_t stream, void** addr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FE_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_setup_lock);
   if (!g_scratch_addr[dev]) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) return FE_ERR_CUDA;
+    if (cap != cudaStreamCaptureStatusNone) return FE_ERR_INVALID_ARGUMENT;
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_select_scratch) != cudaSuccess || !p) return FE_ERR_CUDA;
     if (fe::select_init() != cudaSuccess) return FE_ERR_CUDA;
@@ -98,20 +103,25 @@ extern "C" FE_API int fe_select_noalloc(const fe_pyramid* pyr, int border_top, i
     return FE_ERR_INVALID_ARGUMENT;
   if ((n_alive > 0 && !alive_xy) || (num_desired > 0 && !out_xy)) return FE_ERR_INVALID_ARGUMENT;
   const int w = pyr->width[0], h = pyr->height[0];
+  // the same level-0 checks as fe_select's: the response tiles copy the gradient planes with 16-byte
+  // asynchronous copies, which need 16-byte aligned sources and pitches
   if (w <= 0 || h <= 0 || pyr->pitch_bytes[0] % 16 != 0 || pyr->pitch_bytes[0] < (int64_t)w * 4)
     return FE_ERR_INVALID_ARGUMENT;
+  if (((uintptr_t)pyr->grad_x[0] | (uintptr_t)pyr->grad_y[0]) % 16 != 0) return FE_ERR_INVALID_ARGUMENT;
   if (mask && mask_pitch_bytes < w) return FE_ERR_INVALID_ARGUMENT;
-  // sizes beyond the static scratch are rejected, never truncated
-  if (w > kMaxW || h > kMaxH || (int64_t)n_alive + num_desired + 64 > kMaxKept) return FE_ERR_CAPACITY;
+  // sizes beyond the static scratch are rejected, never truncated; within 2048x2048 the limits are
+  // fe_select's own (num_desired <= 16384, at most 16384 kept candidates)
+  if (w > kMaxW || h > kMaxH || num_desired > 16384) return FE_ERR_CAPACITY;
+  const int cw = w / 8, ch = h / 8;  // 8x8 cells
+  const int q_cap = (int)std::min<int64_t>(std::max(cw * ch, 1), (int64_t)n_alive + num_desired + 64);
+  if (q_cap > kMaxKept) return FE_ERR_CAPACITY;
 
   void* base = nullptr;
-  int rc = setup_current_device(&base);
+  int rc = setup_current_device((cudaStream_t)stream, &base);
   if (rc) return rc;
 
   // shared-memory key capacities: the largest candidate-cell rectangle of a bin, the kept keys
-  const int cw = w / 8, ch = h / 8;  // 8x8 cells
   const int bw = w / 8, bh = h / 8;  // bin size in pixels (8x8 bins)
-  const int q_cap = std::min(std::max(cw * ch, 1), n_alive + num_desired + 64);
   int bin_cap = 1;
   if (bw > 0 && bh > 0) {
     int mx = 1, my = 1;

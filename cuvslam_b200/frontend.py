@@ -40,6 +40,21 @@ class Context:
         _lib.check(self.lib.fe_create(self.device.index or 0, ctypes.byref(h)), "fe_create")
         self.handle = h
 
+    def device_status(self, stream=None):
+        """Synchronises `stream`, then reads and clears the device flags of this context's kernels
+        (fe_device_status): 0 when no bounded wait ran out.  Raises FeError on a device fault."""
+        flags = ctypes.c_int32(0)
+        st = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        rc = self.lib.fe_device_status(self.handle, st, ctypes.byref(flags))
+        if rc == _lib.FE_ERR_DEVICE_FAULT:
+            raise _lib.FeError(f"device fault: flags {flags.value:#x} (a bounded wait ran out)")
+        _lib.check(rc, "fe_device_status")
+        return flags.value
+
+    def set_wait_limit(self, iterations):
+        """Iteration limit of the pyramid's bounded waits for launches planned from now on."""
+        _lib.check(self.lib.fe_set_wait_limit(self.handle, int(iterations)), "fe_set_wait_limit")
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.fe_destroy(self.handle)

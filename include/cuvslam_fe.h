@@ -118,6 +118,22 @@ FE_API int fe_last_cuda_error(void);
 FE_API int fe_create(int device, fe_context** out);
 FE_API int fe_destroy(fe_context* ctx);
 
+/* Device-side failure reporting.  The reference throws on every failed CUDA call (CUDA_CHECK,
+ * cuda_helper.h:42-56) and has no kernel that waits on another; this library's single-launch
+ * pyramid does wait (a tile for its TMA copy, a deeper level for the tiles it reads), each wait
+ * bounded.  A wait that runs out skips its work and sets a flag in the context's device status word
+ * instead of hanging: bit 0 = a tile's staging copy did not arrive (the tile is not written), bit 1 =
+ * a deeper-level item gave up waiting for its inputs (its levels are not written).  Every pyramid
+ * launched through this context (fe_build_pyramid*, batches, adjoint plans) reports there.
+ * fe_device_status synchronises `stream`, copies the word to *flags (may be NULL), clears it and
+ * returns FE_ERR_DEVICE_FAULT when any flag was set, FE_OK otherwise. */
+FE_API int fe_device_status(fe_context* ctx, fe_stream stream, int32_t* flags);
+/* Iteration limit of those bounded waits for launches planned after this call (pyramid builds;
+ * batches and adjoint plans created afterwards).  Default 4194304 (a few hundred milliseconds at
+ * most).  0 makes every such wait give up at once, which exercises the failure path without a
+ * fault: the kernels still finish and fe_device_status reports the flags. */
+FE_API int fe_set_wait_limit(fe_context* ctx, int iterations);
+
 /* ---------------------------------------------------------------------------------------- */
 /* Pyramid                                                                                   */
 /* ---------------------------------------------------------------------------------------- */
@@ -184,12 +200,15 @@ FE_API int fe_select(fe_context* ctx, const fe_pyramid* pyr, int border_top, int
  * process whose device memory all belongs to its own pool allocator).  No counterpart in the
  * reference: it has no allocation-free selection.
  * Scratch is a static device array of about 1.5 MB inside the library, held by every GPU that
- * loads it until the process exits.  Limits: width, height <= 2048 and n_alive + num_desired
- * <= 16320; larger requests return FE_ERR_CAPACITY.  The first call on a device sets up that
- * device (looks up the array's device address, sets kernel attributes) and must come before any
- * stream capture on it.  All calls share the one array: calls whose GPU work overlaps (other
- * streams, other host threads) race and must be serialised by the caller.  Results equal
- * fe_select's. */
+ * loads it until the process exits.  Limits: width, height <= 2048 (FE_ERR_CAPACITY beyond), and
+ * within that fe_select's own limits (num_desired <= 16384; at most 16384 kept candidates, i.e.
+ * min(width/8 * height/8, n_alive + num_desired + 64) <= 16384).  Level-0 planes must be 16-byte
+ * aligned, as fe_select requires.  The first call on a device sets up that device (looks up the
+ * array's device address, sets kernel attributes) and must come before any stream capture on it:
+ * a first call made while `stream` captures returns FE_ERR_INVALID_ARGUMENT and enqueues nothing.
+ * All calls share the one array and each starts by clearing the part that must start at zero:
+ * calls whose GPU work overlaps (other streams, other host threads) race and must be serialised by
+ * the caller.  Results equal fe_select's bit for bit. */
 FE_API int fe_select_noalloc(const fe_pyramid* pyr, int border_top, int border_bottom, int border_left,
                              int border_right, const uint8_t* mask, int64_t mask_pitch_bytes, const float* alive_xy,
                              int n_alive, int num_desired, float* out_xy, int32_t* out_count, fe_stream stream);
