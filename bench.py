@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the LK adjoint measurement")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity check against the reference's own kernels (after the timed regions)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other workloads (stereo plain, 100-frame sequence, fwd+bwd stream, L2R, affine)")
     ap.add_argument("--profile", choices=["pyramid", "lk", "select", "step", "implicit", "unrolled", "affine"],
@@ -158,8 +160,10 @@ def throughput(units_all_ranks, steps, ms_max):
     return units_all_ranks * steps / (ms_max / 1e3)
 
 
-def cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads):
-    """A callable running one frame step of the restated reference CPU tracker over all cameras."""
+def cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads, features_parallel=False):
+    """A callable running one frame step of the restated reference CPU tracker over all cameras: one
+    camera per thread, or (features_parallel) the cameras in turn with each camera's tracking spread
+    over the threads."""
     from oracle import oracle as O
 
     prev_cams = [O.CpuCamera(w, h).build(p) for (w, h), p in zip(shapes, prevs)]
@@ -168,17 +172,51 @@ def cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads):
     attempted = sum(len(f) for f in feats)
 
     def step():
-        return O.cpu_frame_step(prev_cams, cur_cams, nexts, feats, None, counts, nthreads)
+        return O.cpu_frame_step(prev_cams, cur_cams, nexts, feats, None, counts, nthreads, features_parallel)
 
     return step, attempted
+
+
+def host_cpu():
+    """The host's CPU model and the cores this process may use."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_cores": usable}
+
+
+def cpu_baseline_variants(shapes, counts, prevs, nexts, nthreads, reps):
+    """Times both parallel forms of the restated CPU tracker (reps steps each after one warm-up);
+    returns ({variant: tracks/s}, fastest variant's step function, attempted tracks per step)."""
+    out, best = {}, None
+    for name, fp in (("camera_per_thread", False), ("features_parallel", True)):
+        step, att = cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads, fp)
+        step()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            step()
+        out[name] = att * reps / (time.perf_counter() - t0)
+        if best is None or out[name] > out[best[0]]:
+            best = (name, step, att)
+    return out, best
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    nthreads = os.cpu_count() or 1
+    cpu = host_cpu()
+    nthreads = cpu["usable_cores"]
     shapes, counts, prevs, nexts = workload()
-    step, attempted = cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads)
+    variants, (variant, step, attempted) = cpu_baseline_variants(shapes, counts, prevs, nexts, nthreads, 1)
     for _ in range(max(args.warmup, 1)):
         step()
     t0 = time.perf_counter()
@@ -191,12 +229,54 @@ def run_reference(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "tracks_per_step": attempted},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"full 32-camera frame step x {args.steps} steps, one camera per thread"},
+                             "sample": f"full 32-camera frame step x {args.steps} steps, {variant.replace('_', ' ')} "
+                                       f"(the faster of the two parallel forms: {variants})", **cpu},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 ADJ_CAMS, ADJ_W, ADJ_H, ADJ_TRACKS = 8, 1280, 720, 4096
+
+
+def reference_parity(prevs, nexts, counts, host_tracks, frames, run_step):
+    """Checker, run after every timed region: the batched step's results against the reference's own
+    GPU kernels (oracle/_ref: cuVSLAM's lk_track_kernel and GPUSelection sequence, built from its
+    sources) on the same frames and the same input tracks.  LK: status agreement over all tracks,
+    and the distance between the positions of the tracks both keep (median, p99, max).  Selection:
+    the features selected on the previous frames (the step's input tracks) and the step's new
+    features (with the step's own survivors alive) equal the reference's selection as sets."""
+    import torch
+
+    from oracle import ref as R
+    from cuvslam_b200.frontend import tracks_from_device
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref (the reference's kernels built from its sources) is not built here"}
+    run_step()
+    torch.cuda.synchronize()
+    dists, agree, sel_eq, n_all, n_new = [], 0, 0, 0, 0
+    for i, f in enumerate(frames):
+        got = tracks_from_device(f.tracks)
+        want = R.lk(prevs[i], nexts[i], host_tracks[i])
+        sg, sw = got["track_status"] != 0, want["track_status"] != 0
+        both = sg & sw
+        dists.append(np.linalg.norm(got["track"][both].astype(np.float64) - want["track"][both], axis=1))
+        agree += int((sg == sw).sum())
+        n_all += len(got)
+        r0 = R.select(prevs[i], np.zeros((0, 2), np.float32), counts[i])["sel"]
+        alive = got["track"][sg].astype(np.float32)
+        n = int(f.new_count.item())
+        new = f.new_xy[:n].cpu().numpy()
+        r1 = R.select(nexts[i], alive, max(0, counts[i] - len(alive)))["sel"]
+        n_new += n
+        sel_eq += int(R.same_features(host_tracks[i]["track"], r0, 1e-5) and R.same_features(new, r1, 1e-5))
+    d = np.concatenate(dists)
+    return {"median_px": float(np.median(d)), "p99_px": float(np.percentile(d, 99)), "max_px": float(d.max()),
+            "status_agree": agree / max(n_all, 1), "selection_equal": sel_eq == len(frames),
+            "cameras_selection_equal": sel_eq, "cameras": len(frames), "tracks": n_all, "tracks_kept_both": len(d),
+            "new_features": n_new,
+            "against": "the reference's own kernels (lk_track_kernel, GPUSelection) built from its sources, "
+                       "same frames and input tracks; checked after the timed regions"}
 
 
 def adjoint_inputs(ctx, dev):
@@ -267,6 +347,7 @@ def adjoint_bench(ctx, dev, stream, timed, reps=20):
 
 # ---------------------------------------------------------------- the other workloads
 SEQ_W, SEQ_H, SEQ_FRAMES, SEQ_FEATURES, SEQ_LEVELS = 1241, 376, 100, 1000, 5
+SEQ_PARITY_FRAMES = 10  # frame pairs checked against the reference's own kernels
 
 
 def _seq_frame(f):
@@ -320,9 +401,13 @@ def config_sequence(ctx, dev, stream, frames):
     cpu_cur = O.CpuCamera(SEQ_W, SEQ_H)
     cpu_s, cpu_xy = 0.0, cpu_prev.select(None, SEQ_FEATURES)
     cpu_attempted = 0
+    from oracle import ref as R
+    par_frames = SEQ_PARITY_FRAMES if R.available() else 0
+    par_d, par_agree, par_n, par_sel = [], 0, 0, 0
     for f in range(1, SEQ_FRAMES):
         prev_p, cur_p = pyr[(f - 1) % 2], pyr[f % 2]
-        td = tracks_to_device(make_tracks(xy, None, float(SEQ_W), 0.8), dev)
+        recs = make_tracks(xy, None, float(SEQ_W), 0.8)
+        td = tracks_to_device(recs, dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         cur_p.build(ctx, imgs[f], stream=stream)
@@ -334,6 +419,14 @@ def config_sequence(ctx, dev, stream, frames):
                                                    max(0, SEQ_FEATURES - int(ok.sum())), stream).cpu().numpy()
         gpu_s += time.perf_counter() - t0
         attempted += len(xy)
+        if f <= par_frames:  # checker: the reference's own kernels on the same frame pair and tracks
+            want = R.lk(frames[f - 1][0], frames[f][0], recs, SEQ_LEVELS)
+            sw = want["track_status"] != 0
+            par_d.append(np.linalg.norm(out["track"][ok & sw].astype(np.float64) - want["track"][ok & sw], axis=1))
+            par_agree += int((ok == sw).sum())
+            par_n += len(recs)
+            rs = R.select(frames[f][0], out["track"][ok], max(0, SEQ_FEATURES - int(ok.sum())))["sel"]
+            par_sel += int(R.same_features(new.reshape(-1, 2), rs, 1e-5))
         # the CPU tracker on the same inputs (deviation), and the ground truth
         cpu_cur.build(frames[f][0])
         cxy, cst = cpu_cur.track_from(cpu_prev, xy)
@@ -361,7 +454,17 @@ def config_sequence(ctx, dev, stream, frames):
                               "ms_per_frame": cpu_s / (SEQ_FRAMES - 1) * 1e3},
             "gpu_over_cpu": (attempted / gpu_s) / (cpu_attempted / cpu_s),
             "deviation_gpu_vs_cpu_px": {"median": float(np.median(d)), "p99": float(np.percentile(d, 99)), "n": len(d)},
-            "error_vs_truth_px": {"gpu_median": float(np.median(g)), "cpu_median": float(np.median(c))}}
+            "error_vs_truth_px": {"gpu_median": float(np.median(g)), "cpu_median": float(np.median(c))},
+            "parity": _parity_summary(par_d, par_agree, par_n, par_sel, par_frames)}
+
+
+def _parity_summary(dists, agree, n, sel_equal, frames):
+    if not frames:
+        return {"unavailable": "oracle/_ref (the reference's kernels built from its sources) is not built here"}
+    d = np.concatenate(dists)
+    return {"frames": frames, "median_px": float(np.median(d)), "p99_px": float(np.percentile(d, 99)),
+            "max_px": float(d.max()), "status_agree": agree / max(n, 1), "selection_equal": sel_equal == frames,
+            "against": "the reference's own lk_track_kernel and GPUSelection on the same frame pairs and tracks"}
 
 
 def config_stereo_plain(ctx, dev, stream):
@@ -1003,19 +1106,24 @@ def main():
             if line.startswith("dram_bytes_per_step:"):
                 traffic = int(line.split(":")[1])
 
+    # ---- parity against the reference's own kernels (checker; after every timed region), rank 0
+    parity = None
+    if rank == 0 and not args.no_parity:
+        try:
+            parity = reference_parity(prevs, nexts, counts, host_tracks, frames, step_batched)
+        except Exception as ex:  # reported, not fatal: the headline line must still print
+            parity = {"error": f"{type(ex).__name__}: {ex}"}
+
     # ---- CPU baseline (restated reference CPU tracker), rank 0 at N=1 only
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        nthreads = os.cpu_count() or 1
-        stepc, att = cpu_reference_step_fn(shapes, counts, prevs, nexts, nthreads)
-        stepc()
-        t0 = time.perf_counter()
+        host = host_cpu()
         nrep = 3
-        for _ in range(nrep):
-            stepc()
-        dt = time.perf_counter() - t0
-        cpu = {"value": att * nrep / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"full 32-camera frame step x {nrep}, restated reference CPU tracker, one camera per thread"}
+        variants, (variant, _, _) = cpu_baseline_variants(shapes, counts, prevs, nexts, host["usable_cores"], nrep)
+        cpu = {"value": variants[variant], "unit": UNIT, "cores": host["usable_cores"], "kind": "port",
+               "sample": f"full 32-camera frame step x {nrep} per variant, restated reference CPU tracker; "
+                         f"value = the faster variant ({variant.replace('_', ' ')})",
+               "variants": variants, **host}
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:
@@ -1054,6 +1162,7 @@ def main():
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": alg_bytes, "peak_source": peak_src},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks,
             "gpu_launches": kernels_per_step * args.steps,
             "adjoint": adjoint,

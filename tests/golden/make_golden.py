@@ -18,6 +18,9 @@ The committed tests/golden/reference.npz is the step-2 output.
 DIR/stereo_reference.npz.
 `st-reference --out DIR` runs the reference's affine tracker (st_track, st_build_cache +
 st_track_with_cache; oracle/ref_harness.cu ref_st_track) and writes DIR/st_reference.npz.
+`headline-reference --out DIR` runs the reference's selection and LK at the batched workload's
+camera sizes (1280x720 and 1920x1200, 3000 features each; frames drawn from their seeds, hashed so
+a test can check it regenerated the same ones) and writes DIR/headline_reference.npz.
 """
 
 import argparse
@@ -34,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 from cuvslam_b200 import synthetic  # noqa: E402
 from cuvslam_b200.types import TRACK_DTYPE, level_sizes, make_tracks  # noqa: E402
+from oracle import ref as REF  # noqa: E402
 
 # name -> (width, height, camera id)
 CASES = {
@@ -55,15 +59,7 @@ def make_inputs(path):
 
 
 def _lib():
-    p = os.path.join(ROOT, "oracle", "_ref", "libcuvslam_ref.so")
-    lib = ctypes.CDLL(p)
-    P = ctypes.c_void_p
-    I = ctypes.c_int
-    lib.ref_pyramid.argtypes = [P, I, I, I, P, P, P, P]
-    lib.ref_select.argtypes = [P, I, I, P, I, I, I, I, I, I, P, P, P, P, P, P, P, P, P]
-    lib.ref_lk.argtypes = [P, P, I, I, I, P, I, I]
-    lib.ref_tex_probe.argtypes = [P, I, I, P, I, P]
-    return lib
+    return REF.lib()
 
 
 def _ptr(a):
@@ -71,58 +67,19 @@ def _ptr(a):
 
 
 def ref_pyramid(lib, img, max_levels=10):
-    h, w = img.shape
-    sizes = level_sizes(w, h, max_levels)
-    total = sum(a * b for a, b in sizes)
-    lv, gx, gy = (np.zeros(total, np.float32) for _ in range(3))
-    n = ctypes.c_int(0)
-    img = np.ascontiguousarray(img)
-    rc = lib.ref_pyramid(_ptr(img), w, h, max_levels, ctypes.byref(n), _ptr(lv), _ptr(gx), _ptr(gy))
-    assert rc == 0 and n.value == len(sizes), (rc, n.value)
-    out, off = [], 0
-    for (a, b) in sizes:
-        out.append((lv[off:off + a * b].reshape(b, a), gx[off:off + a * b].reshape(b, a), gy[off:off + a * b].reshape(b, a)))
-        off += a * b
-    return out
+    return REF.pyramid(img, max_levels)
 
 
 def ref_select(lib, img, alive, num_desired, borders=(0, 0, 0, 0)):
-    h, w = img.shape
-    cw, ch = w // 8, h // 8
-    cap = max(cw * ch, 1)
-    gftt = np.zeros((h, w), np.float32)
-    nms = np.zeros((h, w), np.float32)
-    cmax = np.zeros(cap, np.float32)
-    cidx = np.zeros(cap * 2, np.uint32)
-    kp = np.zeros(cap * 3, np.float32)
-    bins = np.zeros(64, np.float32)
-    sel = np.zeros(max(num_desired, 1) * 2, np.float32)
-    nkp, nsel = ctypes.c_int(0), ctypes.c_int(0)
-    alive = np.ascontiguousarray(alive, np.float32).reshape(-1, 2)
-    img = np.ascontiguousarray(img)
-    rc = lib.ref_select(_ptr(img), w, h, _ptr(alive), len(alive), num_desired, *borders, _ptr(gftt), _ptr(nms),
-                        _ptr(cmax), _ptr(cidx), _ptr(kp), ctypes.byref(nkp), _ptr(bins), _ptr(sel), ctypes.byref(nsel))
-    assert rc == 0, rc
-    return dict(gftt=gftt, nms=nms, cell_max=cmax[:cw * ch].reshape(ch, cw), cell_idx=cidx[:2 * cw * ch].reshape(ch, cw, 2),
-                kp=kp[:3 * nkp.value].reshape(-1, 3), bins=bins, sel=sel[:2 * nsel.value].reshape(-1, 2))
+    return REF.select(img, alive, num_desired, borders)
 
 
 def ref_lk(lib, prev, nxt, tracks, max_levels=10, horizontal=False):
-    h, w = prev.shape
-    t = np.ascontiguousarray(tracks.copy())
-    rc = lib.ref_lk(_ptr(np.ascontiguousarray(prev)), _ptr(np.ascontiguousarray(nxt)), w, h, max_levels, _ptr(t),
-                    len(t), int(horizontal))
-    assert rc == 0, rc
-    return t
+    return REF.lk(prev, nxt, tracks, max_levels, horizontal)
 
 
 def ref_tex_probe(lib, img, xy):
-    h, w = img.shape
-    out = np.zeros(len(xy), np.float32)
-    rc = lib.ref_tex_probe(_ptr(np.ascontiguousarray(img, np.float32)), w, h, _ptr(np.ascontiguousarray(xy, np.float32)),
-                           len(xy), _ptr(out))
-    assert rc == 0, rc
-    return out
+    return REF.tex_probe(img, xy)
 
 
 def _sha(a):
@@ -401,10 +358,92 @@ def make_st_reference(out_dir):
     print("wrote st_reference.npz")
 
 
+# Headline-size fixtures: one camera of each large size of the batched 32-camera workload (its camera
+# index gives the scene seed), 3000 Shi-Tomasi features selected by the reference on the previous
+# frame, LK with zero and with predicted offsets, and the selection on the next frame with the zero-
+# offset run's survivors alive (the batched step's selection).
+HEADLINE_CASES = {"hd": (1280, 720, 12), "fhd": (1920, 1200, 24)}  # name -> (width, height, camera)
+HEADLINE_FEATURES = 3000
+
+
+def headline_frames(name):
+    w, h, cam = HEADLINE_CASES[name]
+    return synthetic.frame_pair(cam, w, h)
+
+
+def headline_runs(pts, gt, w):
+    """name -> input TrackData records of the headline fixtures' LK runs."""
+    rng = np.random.default_rng(17)
+    pred = gt + rng.normal(0.0, 0.7, gt.shape).astype(np.float32)
+    return {"lk_zero": make_tracks(pts, None, float(w), 0.8), "lk_pred": make_tracks(pts, pred - pts, float(w), 0.8)}
+
+
+def make_headline_reference(out_dir):
+    compact = {}
+    for name, (w, h, cam) in HEADLINE_CASES.items():
+        prev, nxt, warp = headline_frames(name)
+        compact[f"{name}/prev/sha"] = np.array(_sha(prev))
+        compact[f"{name}/next/sha"] = np.array(_sha(nxt))
+        s0 = REF.select(prev, np.zeros((0, 2), np.float32), HEADLINE_FEATURES)
+        pts = s0["sel"].astype(np.float32)
+        compact[f"{name}/sel0"] = pts
+        gt = synthetic.flow_texture(warp, pts.astype(np.float64)).astype(np.float32)
+        compact[f"{name}/gt"] = gt
+        for tag, t in headline_runs(pts, gt, w).items():
+            out = REF.lk(prev, nxt, t)
+            compact[f"{name}/{tag}/offset"] = t["offset"].copy()
+            compact[f"{name}/{tag}/track"] = out["track"].copy()
+            compact[f"{name}/{tag}/status"] = out["track_status"].copy()
+            if tag == "lk_zero":
+                alive = out["track"][out["track_status"] != 0].astype(np.float32)
+                s1 = REF.select(nxt, alive, HEADLINE_FEATURES - len(alive))
+                compact[f"{name}/sel1/alive"] = alive
+                compact[f"{name}/sel1/sel"] = s1["sel"]
+        print(name, "features", len(pts), "tracked", int((compact[f"{name}/lk_zero/status"] != 0).sum()),
+              "new", len(compact[f"{name}/sel1/sel"]))
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "headline_reference.npz"), **compact)
+    print("wrote headline_reference.npz")
+
+
+# CPU-path pinning: the reference's GPU pyramid of a 512x512 random uint8 frame (levels 0-3 are what
+# the reference's own test compares with its CPU uint8 pyramid, image_pyramid_test.cpp:143-227), plain
+# and box prefiltered (ref_pyramid_ex), as SHA-256 hashes of every level.
+CPU_PYR_SIZE = 512
+
+
+def cpu_pyramid_frame():
+    """Random uint8 frame as the reference's test draws it (ImageMatrix<uint8_t>::Random * 100, which
+    wraps modulo 256), from a fixed seed."""
+    rng = np.random.default_rng(143)
+    return ((rng.integers(0, 256, (CPU_PYR_SIZE, CPU_PYR_SIZE)) * 100) % 256).astype(np.uint8)
+
+
+def make_cpu_pyramid_reference(out_dir):
+    img = cpu_pyramid_frame()
+    compact = {"frame/sha": np.array(_sha(img))}
+    lib = _lib()
+    for box in (0, 1):
+        sizes = level_sizes(CPU_PYR_SIZE, CPU_PYR_SIZE, 10)
+        total = sum(a * b for a, b in sizes)
+        lv, gx, gy = (np.zeros(total, np.float32) for _ in range(3))
+        n = ctypes.c_int(0)
+        rc = lib.ref_pyramid_ex(_ptr(img), CPU_PYR_SIZE, CPU_PYR_SIZE, 0, box, 10, ctypes.byref(n), _ptr(lv), _ptr(gx),
+                                _ptr(gy))
+        assert rc == 0 and n.value == len(sizes), (rc, n.value)
+        off = 0
+        for l, (a, b) in enumerate(sizes):
+            compact[f"box{box}/L{l}/sha"] = np.array(_sha(lv[off:off + a * b].reshape(b, a)))
+            off += a * b
+    os.makedirs(out_dir, exist_ok=True)
+    np.savez_compressed(os.path.join(out_dir, "cpu_pyramid_reference.npz"), **compact)
+    print("wrote cpu_pyramid_reference.npz")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("step", choices=["inputs", "reference", "stereo-inputs", "stereo-reference", "input-reference",
-                                        "st-reference"])
+                                        "st-reference", "headline-reference", "cpu-pyramid-reference"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if a.step == "inputs":
@@ -417,5 +456,9 @@ if __name__ == "__main__":
         make_input_reference(a.out)
     elif a.step == "st-reference":
         make_st_reference(a.out)
+    elif a.step == "headline-reference":
+        make_headline_reference(a.out)
+    elif a.step == "cpu-pyramid-reference":
+        make_cpu_pyramid_reference(a.out)
     else:
         make_reference(a.out)

@@ -1,7 +1,7 @@
 """The product path stays apart from the checker: the package never imports the oracle, the native
 library links neither the oracle nor the reference harness, bench.py imports the oracle only in
-its CPU-baseline and reference legs, and without the native library the package fails loudly
-(there is no CPU fallback)."""
+its CPU-baseline and reference legs and its parity checker (run after the timed regions), and
+without the native library the package fails loudly (there is no CPU fallback)."""
 
 import ast
 import glob
@@ -45,9 +45,10 @@ def test_bench_uses_the_oracle_only_in_cpu_legs():
     for node in ast.walk(tree):
         if isinstance(node, ast.FunctionDef) and any(m.split(".")[0] == "oracle" for m in _imports(node)):
             users.add(node.name)
-    # the reference arm / CPU baseline of the headline, and the CPU legs of the other workloads
+    # the reference arm / CPU baseline of the headline, the CPU legs of the other workloads, and the
+    # parity checker against the reference's own kernels
     assert users <= {"cpu_reference_step_fn", "config_sequence", "config_stereo_plain", "config_l2r",
-                     "config_affine"}, users
+                     "config_affine", "reference_parity"}, users
     assert "main" not in users
 
 
