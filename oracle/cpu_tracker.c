@@ -18,7 +18,8 @@
  *                   on integer boxes (image_pyramid_float.h:56-65,158-208), +1 regulariser, <= 10
  *                   iterations, |v| < 0.08 px, radius and 5x5 NCC gates; MonoSOFCPU::trackFeatures
  *                   (sof_mono_cpu.cpp:140-185) retries a failed track without prediction at NCC 0.85.
- * A frame step over many cameras runs one camera per thread (pthreads).
+ * A frame step over many cameras runs one camera per thread (pthreads), or the cameras in turn with
+ * each camera's tracking spread over threads in chunks of features (cpu_frame_step_features).
  */
 #include <float.h>
 #include <math.h>
@@ -146,8 +147,35 @@ void cpu_cam_destroy(cpu_cam* c) {
   free(c);
 }
 
-void cpu_cam_build(cpu_cam* c, const uint8_t* image) {
-  memcpy(c->u8[0], image, (size_t)c->w[0] * c->h[0]);
+/* BoxBlur3Cpu (sof/box_blur.cpp:25-55): interior pixels get the [1 2 1] x [1 2 1] / 16 window sum,
+ * truncated to uint8 (the sum of exact float products is exact, so it is the integer sum >> 4); the
+ * one-pixel border keeps the input. */
+static void box_blur3(const uint8_t* in, int w, int h, uint8_t* out) {
+  for (int y = 1; y < h - 1; ++y)
+    for (int x = 1; x < w - 1; ++x) {
+      const uint8_t* r0 = in + (size_t)(y - 1) * w + x;
+      const uint8_t* r1 = r0 + w;
+      const uint8_t* r2 = r1 + w;
+      const int s = r0[-1] + 2 * r0[0] + r0[1] + 2 * (r1[-1] + 2 * r1[0] + r1[1]) + r2[-1] + 2 * r2[0] + r2[1];
+      out[(size_t)y * w + x] = (uint8_t)(s >> 4);
+    }
+  for (int x = 0; x < w; ++x) {
+    out[x] = in[x];
+    out[(size_t)(h - 1) * w + x] = in[(size_t)(h - 1) * w + x];
+  }
+  for (int y = 1; y < h - 1; ++y) {
+    out[(size_t)y * w] = in[(size_t)y * w];
+    out[(size_t)y * w + w - 1] = in[(size_t)y * w + w - 1];
+  }
+}
+
+/* ImagePyramidU8::build (image_pyramid_u8.cpp:24-57) with blur_filter = box3, then the levels cast
+ * to float and their gradients. */
+void cpu_cam_build_ex(cpu_cam* c, const uint8_t* image, int box3) {
+  if (box3)
+    box_blur3(image, c->w[0], c->h[0], c->u8[0]);
+  else
+    memcpy(c->u8[0], image, (size_t)c->w[0] * c->h[0]);
   for (int l = 1; l < c->levels; ++l)
     scale_down(c->u8[l - 1], c->w[l - 1], c->h[l - 1], c->u8[l], c->w[l], c->h[l], c->buf);
   for (int l = 0; l < c->levels; ++l) {
@@ -157,7 +185,13 @@ void cpu_cam_build(cpu_cam* c, const uint8_t* image) {
   }
 }
 
+void cpu_cam_build(cpu_cam* c, const uint8_t* image) { cpu_cam_build_ex(c, image, 0); }
+
 int cpu_cam_levels(const cpu_cam* c) { return c->levels; }
+
+/* computePatch (image_pyramid_float.h:158-208) of a 9x9 patch at (x, y) on level l's image; 0 when
+ * its integer box leaves the level. */
+int cpu_cam_patch(const cpu_cam* c, int l, float x, float y, float* out);
 
 void cpu_cam_level(const cpu_cam* c, int l, int* w, int* h, float* img, float* gx, float* gy) {
   *w = c->w[l];
@@ -369,6 +403,11 @@ static int patch(const float* img, int w, int h, float x, float y, float* out) {
   return 1;
 }
 
+int cpu_cam_patch(const cpu_cam* c, int l, float x, float y, float* out) {
+  if (l < 0 || l >= c->levels) return 0;
+  return patch(c->img[l], c->w[l], c->h[l], x, y, out);
+}
+
 static int lk_point(const cpu_cam* P, const cpu_cam* C, float tx, float ty, float ox, float oy, float radius,
                     float ncc_thr, float* out_x, float* out_y) {
   if (radius < 0.f) return 0;
@@ -488,6 +527,60 @@ int cpu_cam_track(const cpu_cam* prev, const cpu_cam* cur, const float* xy, cons
   return ok;
 }
 
+/* The same over the features on nthreads threads: chunks of 16 features taken from a shared
+ * counter (a dynamic schedule; each feature's attempts are independent, the pyramids only read). */
+typedef struct {
+  const cpu_cam *prev, *cur;
+  const float *xy, *pred;
+  int n;
+  float* out;
+  uint8_t* status;
+  int next, ok;
+  pthread_mutex_t lock;
+} track_job;
+
+static void* track_worker(void* arg) {
+  track_job* j = (track_job*)arg;
+  const float radius = (float)j->prev->w[0];
+  int ok = 0;
+  for (;;) {
+    pthread_mutex_lock(&j->lock);
+    const int b = j->next;
+    j->next += 16;
+    pthread_mutex_unlock(&j->lock);
+    if (b >= j->n) break;
+    const int e = b + 16 < j->n ? b + 16 : j->n;
+    for (int k = b; k < e; ++k) {
+      const float x = j->xy[2 * k], y = j->xy[2 * k + 1];
+      const float px = j->pred ? j->pred[2 * k] : x, py = j->pred ? j->pred[2 * k + 1] : y;
+      float nx = x, ny = y;
+      int r = lk_point(j->prev, j->cur, x, y, px - x, py - y, radius, 0.8f, &nx, &ny);
+      if (!r) r = lk_point(j->prev, j->cur, x, y, 0.f, 0.f, radius, 0.85f, &nx, &ny);
+      j->out[2 * k] = nx;
+      j->out[2 * k + 1] = ny;
+      j->status[k] = (uint8_t)r;
+      ok += r;
+    }
+  }
+  pthread_mutex_lock(&j->lock);
+  j->ok += ok;
+  pthread_mutex_unlock(&j->lock);
+  return NULL;
+}
+
+int cpu_cam_track_par(const cpu_cam* prev, const cpu_cam* cur, const float* xy, const float* pred_xy, int n,
+                      float* out_xy, uint8_t* status, int nthreads) {
+  if (nthreads <= 1) return cpu_cam_track(prev, cur, xy, pred_xy, n, out_xy, status);
+  track_job j = {prev, cur, xy, pred_xy, n, out_xy, status, 0, 0};
+  pthread_mutex_init(&j.lock, NULL);
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)nthreads);
+  for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, track_worker, &j);
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  free(th);
+  pthread_mutex_destroy(&j.lock);
+  return j.ok;
+}
+
 /* ---------------------------------------------------------------- multi-camera frame step */
 typedef struct {
   cpu_cam** prev;
@@ -529,6 +622,32 @@ static void* frame_worker(void* arg) {
     j->new_n[i] = j->num_desired[i] > 0 ? cpu_cam_select(j->cur[i], alive, na, j->num_desired[i], 0, 0, 0, 0, j->new_xy[i]) : 0;
     free(alive);
   }
+}
+
+/* The features-parallel variant of a frame step: the cameras one after another, each camera's
+ * tracking spread over nthreads threads (pyramid build and selection stay single-threaded, as in
+ * MonoSOFCPU). */
+int cpu_frame_step_features(cpu_cam** prev, cpu_cam** cur, const uint8_t** images, const float** xy, const float** pred,
+                       const int* n, const int* num_desired, float** out_xy, uint8_t** status, float** new_xy,
+                       int* new_n, int ncams, int nthreads) {
+  for (int i = 0; i < ncams; ++i) {
+    cpu_cam_build(cur[i], images[i]);
+    const int m = n[i];
+    float* alive = (float*)malloc(sizeof(float) * 2 * (size_t)(m > 0 ? m : 1));
+    int na = 0;
+    if (prev && prev[i] && m > 0) {
+      cpu_cam_track_par(prev[i], cur[i], xy[i], pred ? pred[i] : NULL, m, out_xy[i], status[i], nthreads);
+      for (int k = 0; k < m; ++k)
+        if (status[i][k]) {
+          alive[2 * na] = out_xy[i][2 * k];
+          alive[2 * na + 1] = out_xy[i][2 * k + 1];
+          ++na;
+        }
+    }
+    new_n[i] = num_desired[i] > 0 ? cpu_cam_select(cur[i], alive, na, num_desired[i], 0, 0, 0, 0, new_xy[i]) : 0;
+    free(alive);
+  }
+  return 0;
 }
 
 /* One frame step of `ncams` cameras on `nthreads` threads (one camera per thread at a time):

@@ -73,11 +73,14 @@ _CPU_SIGS = [
     ("cpu_cam_create", [I, I], P),
     ("cpu_cam_destroy", [P], None),
     ("cpu_cam_build", [P, P], None),
+    ("cpu_cam_build_ex", [P, P, I], None),
+    ("cpu_cam_patch", [P, I, F, F, P], I),
     ("cpu_cam_levels", [P], I),
     ("cpu_cam_level", [P, I, P, P, P, P, P], None),
     ("cpu_cam_track", [P, P, P, P, I, P, P], I),
     ("cpu_cam_select", [P, P, I, I, I, I, I, I, P], I),
     ("cpu_frame_step", [P, P, P, P, P, P, P, P, P, P, P, I, I], I),
+    ("cpu_frame_step_features", [P, P, P, P, P, P, P, P, P, P, P, I, I], I),
 ]
 
 
@@ -383,11 +386,18 @@ class CpuCamera:
         self.w, self.h = int(width), int(height)
         self.h_ = lib().cpu_cam_create(self.w, self.h)
 
-    def build(self, img_u8):
+    def build(self, img_u8, box3=False):
+        """ImagePyramidU8::build (image_pyramid_u8.cpp:24-57), box prefiltered when box3."""
         img = np.ascontiguousarray(img_u8, np.uint8)
         assert img.shape == (self.h, self.w)
-        lib().cpu_cam_build(self.h_, _p(img))
+        lib().cpu_cam_build_ex(self.h_, _p(img), int(bool(box3)))
         return self
+
+    def patch(self, level, x, y):
+        """computePatch's 9x9 exact-bilinear patch at (x, y) on a level's image, or None outside."""
+        out = np.zeros((9, 9), np.float32)
+        ok = lib().cpu_cam_patch(self.h_, int(level), ctypes.c_float(x), ctypes.c_float(y), _p(out))
+        return out if ok else None
 
     def levels(self):
         return lib().cpu_cam_levels(self.h_)
@@ -420,9 +430,10 @@ class CpuCamera:
             pass
 
 
-def cpu_frame_step(prev_cams, cur_cams, images, xy, pred, num_desired, nthreads):
-    """One multi-camera frame step of the restated CPU tracker on `nthreads` threads.
-    Returns (tracked positions, status, new features) per camera."""
+def cpu_frame_step(prev_cams, cur_cams, images, xy, pred, num_desired, nthreads, features_parallel=False):
+    """One multi-camera frame step of the restated CPU tracker on `nthreads` threads: one camera per
+    thread, or (features_parallel) the cameras in turn with each camera's tracking spread over the
+    threads.  Returns (tracked positions, status, new features) per camera."""
     n = len(cur_cams)
     PA = ctypes.c_void_p * n
     imgs = [np.ascontiguousarray(i, np.uint8) for i in images]
@@ -434,11 +445,12 @@ def cpu_frame_step(prev_cams, cur_cams, images, xy, pred, num_desired, nthreads)
     counts = np.zeros(n, np.int32)
     ns = np.array([len(a) for a in xys], np.int32)
     nd = np.array(num_desired, np.int32)
-    lib().cpu_frame_step(PA(*[c.h_ for c in prev_cams]) if prev_cams is not None else None, PA(*[c.h_ for c in cur_cams]),
-                         PA(*[i.ctypes.data for i in imgs]), PA(*[a.ctypes.data for a in xys]),
-                         None if preds is None else PA(*[a.ctypes.data for a in preds]), _p(ns), _p(nd),
-                         PA(*[a.ctypes.data for a in outs]), PA(*[a.ctypes.data for a in sts]),
-                         PA(*[a.ctypes.data for a in news]), _p(counts), n, nthreads)
+    step = lib().cpu_frame_step_features if features_parallel else lib().cpu_frame_step
+    step(PA(*[c.h_ for c in prev_cams]) if prev_cams is not None else None, PA(*[c.h_ for c in cur_cams]),
+         PA(*[i.ctypes.data for i in imgs]), PA(*[a.ctypes.data for a in xys]),
+         None if preds is None else PA(*[a.ctypes.data for a in preds]), _p(ns), _p(nd),
+         PA(*[a.ctypes.data for a in outs]), PA(*[a.ctypes.data for a in sts]),
+         PA(*[a.ctypes.data for a in news]), _p(counts), n, nthreads)
     return outs, sts, [a[:c] for a, c in zip(news, counts)]
 
 
