@@ -16,12 +16,14 @@ def build_library(extra_flags=""):
     return os.path.join(HERE, "libcuvslam_fe.so")
 
 
-def build_checkers():
-    """Test infrastructure: the CPU oracle and, where the reference checkout exists, the harness
-    around the reference's own kernels (oracle/_ref)."""
+def build_checkers(reference=None):
+    """Test infrastructure: the CPU oracle and, given a cuVSLAM checkout (`reference`, else the
+    CUVSLAM_REFERENCE environment variable), the harness around the reference's own kernels
+    (oracle/_ref)."""
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
-    # builds oracle/_ref when the reference checkout is present, and does nothing otherwise
-    subprocess.check_call(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")])
+    # builds oracle/_ref when a checkout with the kernels is given, and does nothing otherwise
+    ref = reference or os.environ.get("CUVSLAM_REFERENCE", "")
+    subprocess.check_call(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")] + ([ref] if ref else []))
 
 
 def build():

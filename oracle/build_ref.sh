@@ -5,9 +5,16 @@
 #
 # The reference's C++ (Eigen-based) CPU tracker is not built: Eigen, gflags and googletest are
 # fetched over the network by the reference's CMake and are absent here.
+#
+# Usage: oracle/build_ref.sh <cuVSLAM checkout>   (or with CUVSLAM_REFERENCE set).  Without either,
+# or when the checkout has no kernels, nothing is built and the script exits 0.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${CUVSLAM_REFERENCE:-/root/reference}"
+REF="${1:-${CUVSLAM_REFERENCE:-}}"
+if [ -z "$REF" ]; then
+  echo "no cuVSLAM checkout given (argument or CUVSLAM_REFERENCE); oracle/_ref not built" >&2
+  exit 0
+fi
 K="$REF/libs/cuda_modules/cuda_kernels"
 if [ ! -d "$K" ]; then
   echo "reference kernels not found under $REF; oracle/_ref not built" >&2
