@@ -101,12 +101,20 @@ class ClockSampler:
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
+            import atexit
+
+            atexit.register(self.__exit__)  # stopped even if the measurements in between raise
+            # the sampler takes a moment to start: wait (at most 5 s) for its first sample so that the
+            # timed region is covered from its start
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
-        if self.proc is not None:
+        if self.proc is not None and self.proc.poll() is None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -992,10 +1000,10 @@ def main():
         torch.cuda.synchronize()
         return reduce_max(s.elapsed_time(e), dist, dev)
 
-    # ---- headline: batched, device-resident inputs
-    with ClockSampler(local) as clk:
-        ms = timed(step_batched, args.steps, args.warmup)
-    clocks = clk.summary()
+    # ---- headline: batched, device-resident inputs.  Clocks are sampled from just before this
+    #      timed region through the last GPU measurement below (the window the samples cover).
+    clk = ClockSampler(local).__enter__()
+    ms = timed(step_batched, args.steps, args.warmup)
     total_units = reduce_sum(attempted, dist, dev)
     value = throughput(total_units, args.steps, ms)
 
@@ -1084,12 +1092,30 @@ def main():
     ms_e2e = reduce_max(s0.elapsed_time(s1), dist, dev)
     e2e_value = throughput(total_units, args.steps, ms_e2e)
 
-    # ---- dominant part and its roofline (pyramid stages: HBM-bound)
-    def part(p):
-        return lambda: batch.run_part(p, stream)
+    # ---- the parts of the step, each launch timed alone with CUDA events on its stream (the tracks
+    #      restored, and for the selection LK run, outside the event pair), and their rooflines
+    def part_launch_ms(p, reps, warm=2):
+        pairs = []
+        for r in range(warm + reps):
+            restore()
+            if p == 2:
+                batch.run_part(1, stream)  # the selection reads LK's survivors
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            batch.run_part(p, stream)
+            s1.record(stream)
+            if r >= warm:
+                pairs.append((s0, s1))
+        torch.cuda.synchronize()
+        return reduce_max(sum(a.elapsed_time(b) for a, b in pairs) / reps, dist, dev)
 
     reps = 10
-    part_ms = {name: timed(part(p), reps, 2) / reps for name, p in (("pyramid", 0), ("lk", 1), ("select", 2))}
+    part_ms = {name: part_launch_ms(p, reps) for name, p in (("pyramid", 0), ("lk", 1), ("select", 2))}
+    clk.__exit__()
+    clocks = clk.summary()
+    if clocks is not None:
+        clocks["window"] = ("50 ms samples from just before the headline timed region through the per-part "
+                            "timings (all GPU measurements of the step)")
     alg_bytes = 0
     for (w, h) in shapes:
         alg_bytes += w * h + 12 * sum(a * b for a, b in level_sizes(w, h))
@@ -1099,12 +1125,30 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = alg_bytes / (part_ms["pyramid"] / 1e3) / 1e9
-    traffic = None
+    traffic, traffic_src = None, None
     prof = os.path.join(ROOT, "profiles", "pyramid_multicam32_traffic.txt")
     if os.path.exists(prof):
+        captured_on = None
         for line in open(prof):
             if line.startswith("dram_bytes_per_step:"):
                 traffic = int(line.split(":")[1])
+            if line.startswith("kernel_source_sha256:"):
+                captured_on = line.split(":")[1].strip()
+        import hashlib
+        current = hashlib.sha256(open(os.path.join(ROOT, "cuvslam_b200", "csrc", "pyramid.cu"), "rb").read()).hexdigest()[:16]
+        traffic_src = {"from": "ncu capture of this workload's pyramid launch (profiles/pyramid_multicam32_traffic.txt), "
+                               "not measured in this run",
+                       "captured_on_pyramid_cu": captured_on, "current_pyramid_cu": current,
+                       "current": captured_on == current}
+    # LK: algorithmic FLOPs by the convention of the work counters (per level set up 2592, per
+    # Gauss-Newton step 1134, per NCC evaluation 200), counted by the kernel itself in one extra run
+    restore()
+    lk_levels, lk_steps, lk_ncc = batch.lk_work(stream)
+    lk_flops = 2592 * lk_levels + 1134 * lk_steps + 200 * lk_ncc
+    props = torch.cuda.get_device_properties(dev)
+    sm_max = (clocks or {}).get("sm_max_mhz") or 1965.0
+    fp32_peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    lk_achieved = lk_flops / (part_ms["lk"] / 1e3) / 1e12
 
     # ---- parity against the reference's own kernels (checker; after every timed region), rank 0
     parity = None
@@ -1160,7 +1204,15 @@ def main():
                     "pipeline": "two batches in ping-pong, uploads and downloads on their own streams"},
             "roofline": {"bound": "hbm", "kernel": "pyramid stages (all cameras)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes": alg_bytes, "peak_source": peak_src},
+                         "traffic_source": traffic_src, "algorithmic_bytes": alg_bytes, "peak_source": peak_src},
+            "roofline_lk": {"bound": "fp32 issue / latency", "kernel": "LK (all tracks)", "achieved": lk_achieved,
+                            "peak": fp32_peak, "unit": "TFLOP/s", "frac": lk_achieved / fp32_peak,
+                            "flops_per_launch": lk_flops, "ms_per_launch": part_ms["lk"],
+                            "work": {"levels_set_up": lk_levels, "gauss_newton_steps": lk_steps, "ncc": lk_ncc},
+                            "convention": "2592 per level set up + 1134 per Gauss-Newton step + 200 per NCC "
+                                          "evaluation, counted by the kernel",
+                            "peak_source": f"nominal: {props.multi_processor_count} SMs x 128 FP32 lanes x 2 x "
+                                           f"{sm_max:.0f} MHz (no measured FP32 peak)"},
             "cpu_baseline": cpu,
             "parity": parity,
             "clocks": clocks,

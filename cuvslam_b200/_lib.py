@@ -171,6 +171,7 @@ _SIGS = {
     "fe_batch_run_plain": (_I, [_P, _P]),
     "fe_batch_run_part": (_I, [_P, _I, _P]),
     "fe_batch_kernel_count": (_I, [_P]),
+    "fe_batch_lk_work": (_I, [_P, _P, _P]),
     "fe_batch_autotune": (_I, [_P, _I, _P]),
     "fe_batch_tuning": (_I, [_P, _P, _P, _P]),
     "fe_batch_set_tuning": (_I, [_P, _I, _I, _I]),

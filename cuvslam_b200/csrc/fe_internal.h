@@ -160,6 +160,8 @@ struct LkLaunch {
   LkCam single;                 // used when cams == nullptr
   const LkTex* texs;            // FE_SAMPLE_HARDWARE: device array parallel to cams, or nullptr
   LkTex single_tex;             // FE_SAMPLE_HARDWARE with cams == nullptr
+  unsigned long long* counts;   // optional work counters (emulated sampling): [0] levels set up,
+                                // [1] Gauss-Newton steps, [2] NCC evaluations, summed over tracks
 };
 
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) lk_kernel(const __grid_const
       __syncwarp();
     }
     track_one<SAMPLING, HORIZ, MODE>(cam, td, smem[wid], lane, p.iters, p.tol2,
-                                     MODE == kModeUnrolled && p.recs ? p.recs + g : nullptr);
+                                     MODE == kModeUnrolled && p.recs ? p.recs + g : nullptr, p.counts);
     if (MODE == kModeRef && cam.retrack_ncc > 0.f) {
       // MonoSOFGPU's retrack pass, merged as collect reads it: a track the first pass lost (its
       // record still holds the inputs) runs again with the retrack NCC threshold
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) lk_kernel(const __grid_const
         __syncwarp();
         if (lane == 0) td.ncc_threshold = cam.retrack_ncc;
         __syncwarp();
-        track_one<SAMPLING, HORIZ, MODE>(cam, td, smem[wid], lane, p.iters, p.tol2, nullptr);
+        track_one<SAMPLING, HORIZ, MODE>(cam, td, smem[wid], lane, p.iters, p.tol2, nullptr, p.counts);
         __syncwarp();
         if (lane == 0) td.ncc_threshold = keep;
       }

@@ -21,9 +21,12 @@ namespace lk {
 constexpr int kModeRef = 0, kModeImplicit = 1, kModeUnrolled = 2;
 
 // `rec` (unrolled mode only, may be null) receives the per-level record the adjoint replays.
+// `cnt` (may be null) counts the work done: [0] levels set up (previous patch and gradients sampled,
+// Hessian formed), [1] Gauss-Newton steps (current patch sampled, update solved), [2] NCC
+// evaluations.
 template <int SAMPLING, bool HORIZ, int MODE>
 __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int lane, int iters, float tol2,
-                          LkRecord* rec = nullptr) {
+                          LkRecord* rec = nullptr, unsigned long long* cnt = nullptr) {
   if (MODE == kModeUnrolled && rec) {
     if (lane < kMaxLevels) rec->flags[lane] = 0;
     __syncwarp();
@@ -83,6 +86,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
       rec->flags[level] = 0;
     }
     if (good) {
+      if (cnt && lane == 0) atomicAdd(cnt, 1ull);
       // previous-frame patch: image and gradients
       const int bx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, by = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
       __syncwarp();
@@ -211,6 +215,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           good = false;
           break;
         }
+        if (cnt && lane == 0) atomicAdd(cnt + 1, 1ull);
         conv = HORIZ ? fabsf(vx) < 0.12f : __fmaf_rn(vx, vx, __fmul_rn(vy, vy)) < thr2;
         if (MODE != kModeUnrolled && conv) break;
         if (MODE == kModeUnrolled && rec && lane == 0) {
@@ -232,6 +237,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
         if (__fmaf_rn(dx, dx, __fmul_rn(dy, dy)) > __fmul_rn(r, r)) conv = false;
       }
       if (conv) {
+        if (cnt && lane == 0) atomicAdd(cnt + 2, 1ull);
         float s1 = 0.f, s2 = 0.f, s11 = 0.f, s22 = 0.f, s12 = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {

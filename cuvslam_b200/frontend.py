@@ -408,6 +408,14 @@ class Batch:
     def kernel_count(self):
         return self.ctx.lib.fe_batch_kernel_count(self.handle)
 
+    def lk_work(self, stream=None):
+        """Runs the batch's LK part once with the kernel's work counters on (fe_batch_lk_work) and
+        returns (levels set up, Gauss-Newton steps, NCC evaluations) summed over all tracks."""
+        c = torch.zeros(3, dtype=torch.int64, device=self.ctx.device)
+        _lib.check(self.ctx.lib.fe_batch_lk_work(self.handle, _ptr(c), _stream_handle(stream)), "fe_batch_lk_work")
+        (stream or torch.cuda.current_stream()).synchronize()
+        return tuple(int(v) for v in c.cpu())
+
     def autotune(self, reps=10, stream=None):
         """Chooses the LK block shape, the response-tile overlap and the pyramid stage tile by
         timing the step (fe_batch_autotune); returns the chosen shapes."""

@@ -415,6 +415,14 @@ typedef enum {
 } fe_batch_part;
 /* Enqueues one part of the planned step directly (no graph). */
 FE_API int fe_batch_run_part(fe_batch* batch, int part, fe_stream stream);
+/* Work counters of the batch's LK (no counterpart in the reference): runs the LK part once, from the
+ * tracks as they are (they move as with fe_batch_run_part(FE_PART_TRACK)), with the kernel's own
+ * per-track counting on, and adds to device_counts[0..2] (device memory, zeroed by the caller) the
+ * number of pyramid levels at which a track was set up (previous patch and gradients sampled,
+ * Hessian formed), of Gauss-Newton steps (current patch sampled, update solved) and of NCC
+ * evaluations, over all tracks and both passes.  Timed steps never count.  Not for
+ * FE_SAMPLE_HARDWARE batches (FE_ERR_INVALID_ARGUMENT). */
+FE_API int fe_batch_lk_work(fe_batch* batch, uint64_t* device_counts, fe_stream stream);
 /* Number of kernel launches in one fe_batch_run (kernel nodes of the captured graph); -1 for a
  * NULL batch. */
 FE_API int fe_batch_kernel_count(fe_batch* batch);

@@ -142,3 +142,33 @@ def test_autotuned_batch_gives_the_same_results(ctx):
                     np.testing.assert_array_equal(na, nb)
                     for x, y in zip(pa, pb):
                         np.testing.assert_array_equal(x, y)
+
+
+def test_lk_work_counters(ctx):
+    """The kernel's work counters (fe_batch_lk_work) change no result, repeat exactly from the same
+    inputs, and bound the work: every kept track was set up, stepped and NCC-checked at least at level
+    0, and no level takes more than the 11 steps of the reference rule."""
+    frames, prevs, host = _setup(ctx, SHAPES[:3], seed=3)
+    b = Batch(ctx, frames)
+
+    def restore():
+        for f, t in zip(frames, host):
+            if f.tracks is not None:
+                f.tracks.copy_(tracks_to_device(t))
+
+    restore()
+    b.run_part(0)
+    b.run_part(1)
+    plain = [tracks_from_device(f.tracks) for f in frames if f.tracks is not None]
+    restore()
+    c1 = b.lk_work()
+    counted = [tracks_from_device(f.tracks) for f in frames if f.tracks is not None]
+    for x, y in zip(plain, counted):
+        assert_tracks_equal(x, y)
+    restore()
+    assert b.lk_work() == c1
+    levels, steps, ncc = c1
+    kept = sum(int((t["track_status"] != 0).sum()) for t in counted)
+    assert kept > 0 and levels >= kept and steps >= kept and ncc >= kept
+    assert steps <= 11 * levels
+    b.close()
