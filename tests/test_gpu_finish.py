@@ -107,3 +107,20 @@ def test_batched_step_with_finish_equals_plain_and_oracle(ctx, oracle):
         want, wage, _ = oracle.finish_tracks(lk, a, w, h, (2, 2, 2, 2))
         assert_tracks_equal(tb, want)
         np.testing.assert_array_equal(ab.astype(np.uint32), wage)
+
+
+def test_finish_known_answers(ctx):
+    """The CUDA filters on the hand-computed known answers of each rule (tests/finish_cases.py)."""
+    import finish_cases as FC
+
+    for name, (xy, st, age, w, h, border, pred, mask, collapse, want) in FC.cases().items():
+        t = FC.tracks_of(xy, st)
+        d = tracks_to_device(t)
+        age_d = torch.from_numpy(np.asarray(age, np.int32)).cuda()
+        fin = TrackFinish(age_d, predicted=None if pred is None else torch.from_numpy(np.asarray(pred, np.float32)).cuda(),
+                          mask=None if mask is None else torch.from_numpy(mask).cuda(), collapse=collapse)
+        finish_tracks(ctx, d, fin, w, h, border)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(age_d.cpu().numpy().astype(np.uint32), np.asarray(want, np.uint32), err_msg=name)
+        got = tracks_from_device(d)
+        np.testing.assert_array_equal(got["track_status"] != 0, np.asarray(want) != 0, err_msg=name)

@@ -82,3 +82,15 @@ def test_oracle_finish_equals_reference_loops(oracle, seed, opts):
     np.testing.assert_array_equal(gage, want)
     np.testing.assert_array_equal(got["track_status"], ((want != 0) & (t["track_status"] != 0)).astype(np.uint8))
     assert alive == int((want != 0).sum())
+
+
+def test_oracle_finish_known_answers(oracle):
+    """Hand-computed known answers of each filter rule (tests/finish_cases.py)."""
+    import finish_cases as FC
+
+    for name, (xy, st, age, w, h, border, pred, mask, collapse, want) in FC.cases().items():
+        t = FC.tracks_of(xy, st)
+        p = None if pred is None else np.asarray(pred, np.float32)
+        _, gage, alive = oracle.finish_tracks(t, np.asarray(age, np.uint32), w, h, border, p, mask, collapse)
+        np.testing.assert_array_equal(gage, np.asarray(want, np.uint32), err_msg=name)
+        assert alive == int((np.asarray(want) != 0).sum()), name
