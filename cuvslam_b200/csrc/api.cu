@@ -920,7 +920,6 @@ int fe_track_stereo(fe_context* ctx, const fe_stereo_pair* pairs, int npairs, fl
   const int64_t need = zero_bytes + ones_bytes + pos_elems * 8;
   if ((size_t)need > ctx->stereo_bytes) {
     if (ctx->stereo_mem) cudaFree(ctx->stereo_mem);
-  if (ctx->finish_cells) cudaFree(ctx->finish_cells);
     ctx->stereo_mem = nullptr;
     ctx->stereo_bytes = 0;
     FE_CUDA(dev_alloc((void**)&ctx->stereo_mem, (size_t)need));

@@ -121,7 +121,7 @@ void or64_debug_skip_pyramid_adjoint(int on);
 void or64_cam_adjoint_plane(const or64_cam* c, int level, int plane, double* out);
 void or64_fd(or64_cam* c, const double* prev0, const double* cur0, const or_track_data* in, int n, int mode,
              int iters, double tol, const double* gt, const uint8_t* mask, int nq, const int* which,
-             const int64_t* index, double h, double* out);
+             const int64_t* index, double h, double* out, int strict);
 
 #ifdef __cplusplus
 }

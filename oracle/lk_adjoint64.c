@@ -635,15 +635,28 @@ void or64_backward(or64_cam* c, const or_track_data* in, int n, int mode, int it
   memcpy(grad_cur0, c->dcimg[0], sizeof(double) * c->ws[0] * c->hs[0]);
 }
 
+/* A track's discrete decisions: status, and per level whether it was set up and accepted and how
+ * many steps it took. */
+static uint64_t decisions(const trec* R) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)R->status;
+  for (int l = 0; l < L64_MAX_LEVELS; ++l) {
+    h = (h ^ (uint64_t)(R->lv[l].processed + 2 * R->lv[l].ok)) * 1099511628211ull;
+    h = (h ^ (uint64_t)R->lv[l].K) * 1099511628211ull;
+  }
+  return h;
+}
+
 /* Mean squared distance to gt over the tracks in `mask` (tracks the caller counts), divided by n:
- * L = sum_{mask} |c_i - gt_i|^2 / n.  Sets *flipped when a masked track fails. */
+ * L = sum_{mask} |c_i - gt_i|^2 / n.  Sets *flipped when a masked track fails, or, given base
+ * (one value per track), when its decisions differ from base's. */
 static double mse(const or64_cam* c, const or_track_data* in, int n, int mode, int iters, double tol,
-                  const double* gt, const uint8_t* mask, int* flipped) {
+                  const double* gt, const uint8_t* mask, int* flipped, const uint64_t* base) {
   trec* R = (trec*)malloc(sizeof(trec));
   double L = 0;
   for (int i = 0; i < n; ++i) {
     if (!mask[i]) continue;
     track_one(c, &in[i], mode, iters, tol, R);
+    if (base && decisions(R) != base[i]) *flipped = 1;
     if (!R->status) {
       *flipped = 1;
       continue;
@@ -657,10 +670,23 @@ static double mse(const or64_cam* c, const or_track_data* in, int n, int mode, i
 
 /* Central finite differences of the loss above.  which[q]: 0 previous-image pixel index[q],
  * 1 current-image pixel index[q], 2 / 3 x / y of track index[q]'s position.  out[q] is NaN where
- * a perturbation changed which tracks succeed. */
+ * a perturbation changed which tracks succeed, or, with strict != 0, any counted track's decisions
+ * (levels set up and accepted, steps per level): the loss then jumps and the difference is not a
+ * derivative. */
 void or64_fd(or64_cam* c, const double* prev0, const double* cur0, const or_track_data* in, int n, int mode,
              int iters, double tol, const double* gt, const uint8_t* mask, int nq, const int* which,
-             const int64_t* index, double h, double* out) {
+             const int64_t* index, double h, double* out, int strict) {
+  uint64_t* base = NULL;
+  if (strict) {
+    base = (uint64_t*)calloc(n > 0 ? n : 1, sizeof(uint64_t));
+    trec* R = (trec*)malloc(sizeof(trec));
+    for (int i = 0; i < n; ++i)
+      if (mask[i]) {
+        track_one(c, &in[i], mode, iters, tol, R);
+        base[i] = decisions(R);
+      }
+    free(R);
+  }
   const size_t np = (size_t)c->ws[0] * c->hs[0];
   double* p = (double*)malloc(np * sizeof(double));
   double* q = (double*)malloc(np * sizeof(double));
@@ -686,7 +712,7 @@ void or64_fd(or64_cam* c, const double* prev0, const double* cur0, const or_trac
         tr[index[k]].track[which[k] - 2] = (float)(fsave + d);
       }
       if (which[k] <= 1) or64_cam_set(c, p, q);
-      lv[sgn] = mse(c, tr, n, mode, iters, tol, gt, mask, &flipped);
+      lv[sgn] = mse(c, tr, n, mode, iters, tol, gt, mask, &flipped, which[k] <= 1 ? base : NULL);
       if (which[k] == 0) p[index[k]] = save;
       else if (which[k] == 1) q[index[k]] = save;
       else tr[index[k]].track[which[k] - 2] = fsave;
@@ -704,4 +730,5 @@ void or64_fd(or64_cam* c, const double* prev0, const double* cur0, const or_trac
   free(p);
   free(q);
   free(tr);
+  free(base);
 }

@@ -466,7 +466,7 @@ _L64_SIGS = [
     ("or64_cam_plane", [P, I, I, P], None),
     ("or64_track", [P, P, I, I, I, ctypes.c_double, P, P], None),
     ("or64_backward", [P, P, I, I, I, ctypes.c_double, P, P, P, P, P], None),
-    ("or64_fd", [P, P, P, P, I, I, I, ctypes.c_double, P, P, I, P, P, ctypes.c_double, P], None),
+    ("or64_fd", [P, P, P, P, I, I, I, ctypes.c_double, P, P, I, P, P, ctypes.c_double, P, I], None),
 ]
 
 
@@ -520,7 +520,9 @@ class Diff64:
         _l64().or64_backward(self.h_, _p(tracks), n, mode, iters, tol, _p(g), _p(gp), _p(gc), _p(gt), _p(go))
         return gp, gc, gt, go
 
-    def fd(self, tracks, mode, iters, gt_xy, mask, which, index, h=1e-3, tol=1e-13):
+    def fd(self, tracks, mode, iters, gt_xy, mask, which, index, h=1e-3, tol=1e-13, strict=False):
+        """Central differences; NaN where a perturbation changed a counted track's success or, with
+        strict, any of its discrete decisions (levels set up and accepted, steps per level)."""
         tracks = np.ascontiguousarray(tracks)
         n = len(tracks)
         gt = np.ascontiguousarray(gt_xy, np.float64).reshape(n, 2)
@@ -529,7 +531,7 @@ class Diff64:
         ix = np.ascontiguousarray(index, np.int64)
         out = np.zeros(len(wh), np.float64)
         _l64().or64_fd(self.h_, _p(self.prev), _p(self.cur), _p(tracks), n, mode, iters, tol, _p(gt), _p(m), len(wh),
-                       _p(wh), _p(ix), h, _p(out))
+                       _p(wh), _p(ix), h, _p(out), int(bool(strict)))
         return out
 
     def __del__(self):

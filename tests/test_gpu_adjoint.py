@@ -133,3 +133,66 @@ def test_autograd_function(ctx, oracle):
     # the function's image gradient is the plan's gradient times the intensity scale
     torch.testing.assert_close(prev.grad, t.grad_prev * 255.0, rtol=0, atol=0)
     assert torch.isfinite(prev.grad).all() and prev.grad.abs().sum() > 0
+
+
+@pytest.mark.parametrize("mode", ["implicit", "unrolled"])
+def test_adjoint_finite_differences_eight_cameras(ctx, oracle, mode):
+    """At the LK adjoint configuration's size: 8 cameras of 1280x720, frames in [0, 1], 4096 tracks
+    each, one plan over all cameras; the image gradients against central finite differences
+    (h = 1e-3) of the FP64 forward on 256 random pixels (16 per camera and frame).  The loss counts
+    64 random kept tracks per camera (the forward tracks all of them), so that few perturbations
+    reach a track sitting on a decision threshold.  A pixel moves only its own camera's loss, so each
+    probe re-runs one camera's FP64 forward; the probes run on a spawned process pool.  Tolerance
+    1e-3 relative over the probes whose perturbation leaves every counted track's decisions (levels
+    set up and accepted, steps per level, success) unchanged; at least 80% of the probes."""
+    import multiprocessing as mp
+
+    import adjoint_fd_pool
+
+    cams, w, h = 8, 1280, 720
+    cases = [camera_case(oracle, 40 + c, w, h, 4096) for c in range(cams)]
+    n = min(len(c[2]) for c in cases)
+    t = DiffTracker(ctx, cams, h, w, n, mode=mode, iterations=ITERS[mode])
+    prev = torch.from_numpy(np.stack([c[0] for c in cases]).astype(np.float32) / 255.0).cuda()
+    cur = torch.from_numpy(np.stack([c[1] for c in cases]).astype(np.float32) / 255.0).cuda()
+    xy = torch.from_numpy(np.stack([np.ascontiguousarray(c[2]["track"][:n]) for c in cases])).cuda()
+    t.set_inputs(prev, cur, xy)
+    t.build_pyramids()
+    t.forward_step()
+    pos, st = t.outputs()
+    torch.cuda.synchronize()
+    pos, st = pos.double().cpu().numpy(), st.cpu().numpy()
+    s = np.float32(t.scale)
+    mo = oracle.IMPLICIT if mode == "implicit" else oracle.UNROLLED
+    levels0 = [((t.prev_img[c].cpu().numpy() * s).astype(np.float64), (t.cur_img[c].cpu().numpy() * s).astype(np.float64))
+               for c in range(cams)]
+    # the workers rebuild these from the seeds: check that they get the same images
+    again = adjoint_fd_pool.camera_inputs(40, w, h, 4096)
+    assert np.array_equal(again[0], levels0[0][0]) and np.array_equal(again[1], levels0[0][1])
+    g = np.zeros((cams, n, 2))
+    oks = []
+    rng = np.random.default_rng(11)
+    for c in range(cams):
+        D = oracle.Diff64(*levels0[c])
+        pos64, st64 = D.track(cases[c][2][:n], mo, ORACLE_ITERS[mode])
+        ok = st[c] & (st64 == 1) & (np.abs(pos[c] - pos64).max(1) < 1e-3)
+        keep = np.zeros(n, bool)
+        keep[rng.choice(np.flatnonzero(ok), min(64, int(ok.sum())), replace=False)] = True
+        oks.append(keep)
+        g[c] = mse_upstream(pos64, keep, cases[c][3][:n], n)
+    t.grad_xy.copy_(torch.from_numpy(g.astype(np.float32)).cuda())
+    t.backward_step()
+    torch.cuda.synchronize()
+    gp, gc = t.grad_prev.double().cpu().numpy(), t.grad_cur.double().cpu().numpy()
+    tasks, want = [], []
+    for c in range(cams):
+        for which, grad in ((0, gp[c]), (1, gc[c])):
+            for idx in rng.choice(np.flatnonzero(grad), 16, replace=False):
+                tasks.append((40 + c, w, h, 4096, n, mo, ORACLE_ITERS[mode], oks[c].astype(np.uint8), which,
+                              int(idx), 1e-3))
+                want.append(grad.ravel()[idx])
+    with mp.get_context("spawn").Pool(min(16, mp.cpu_count())) as pool:
+        fd = np.array(pool.map(adjoint_fd_pool.probe, tasks, chunksize=1))
+    good = np.isfinite(fd)
+    assert good.sum() >= 0.8 * len(fd), good.sum()
+    assert rel_err(np.array(want)[good], fd[good]) < TOL

@@ -124,3 +124,44 @@ def test_finish_known_answers(ctx):
         np.testing.assert_array_equal(age_d.cpu().numpy().astype(np.uint32), np.asarray(want, np.uint32), err_msg=name)
         got = tracks_from_device(d)
         np.testing.assert_array_equal(got["track_status"] != 0, np.asarray(want) != 0, err_msg=name)
+
+
+def test_finish_scratch_survives_stereo_scratch_growth(oracle):
+    """One context's scratch buffers are independent: growing the left-to-right matching scratch
+    (twice) leaves the finish filters' collapse cells allocated and correct, and no CUDA error is
+    left pending for the next call to report."""
+    import os
+
+    from conftest import ROOT
+    from cuvslam_b200.frontend import Context
+    from cuvslam_b200.stereo import StereoMatcher, StereoPair
+
+    c = Context(0)
+    try:
+        w, h, n = 640, 480, 3000
+        t, age, pred, mask = _finish_case(29, n, w, h)
+        want, wage, _ = oracle.finish_tracks(t, age, w, h, (0, 0, 0, 0), None, None, True)
+
+        def finish_once():
+            d = tracks_to_device(t)
+            a = torch.from_numpy(age.astype(np.int32)).cuda()
+            finish_tracks(c, d, TrackFinish(a), w, h, (0, 0, 0, 0))
+            torch.cuda.synchronize()
+            assert_tracks_equal(tracks_from_device(d), want)
+            np.testing.assert_array_equal(a.cpu().numpy().astype(np.uint32), wage)
+
+        finish_once()
+        inp = np.load(os.path.join(ROOT, "tests", "golden", "stereo_inputs.npz"))
+        left = np.load(os.path.join(ROOT, "tests", "golden", "inputs.npz"))["c1/prev"]
+        pp, sp = gpu_pyramid(c, left, 4), gpu_pyramid(c, inp["right"], 4)
+        uv = torch.from_numpy(inp["uv"]).cuda()
+        for k in (40, 400):  # a larger candidate list each time: the scratch grows twice
+            off = torch.from_numpy((np.arange(len(inp["uv"]) + 1) * 2).astype(np.int32)).cuda()
+            xy = torch.from_numpy(np.repeat(inp["uv"], 2, axis=0) - np.float32(k / 40)).cuda()
+            m = StereoMatcher(c)
+            m.track_primary_to_secondary([StereoPair(pp, sp, uv, None, cand_offsets=off, cand_xy=xy,
+                                                     max_candidates=2 * k // 40)])
+            torch.cuda.synchronize()
+        finish_once()
+    finally:
+        c.close()
