@@ -1842,7 +1842,7 @@ int fe_adjoint_create(fe_context* ctx, const fe_adjoint_job* jobs, int njobs, in
         }
         J.px_begin = px;
         px += P.w * P.h;
-        lv.max_blocks = std::max(lv.max_blocks, ((P.w + 31) / 32) * ((P.h + 7) / 8));
+        lv.max_blocks = std::max(lv.max_blocks, ((P.w + 127) / 128) * ((P.h + 7) / 8));
       }
     }
     lv.total_px = px;

@@ -167,7 +167,7 @@ struct LkLaunch {
 cudaError_t launch_lk(const LkLaunch& p, cudaStream_t s);
 // The reference rule with the texture unit's filtering (lk_hw.cu).
 cudaError_t launch_lk_hw(const LkLaunch& p, cudaStream_t s);
-constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2
+constexpr int kLkShapes = 4;  // warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 12x2
 
 // ---------------------------------------------------------------- track filters after LK
 struct FinishCam {
@@ -311,7 +311,7 @@ struct AdjPyrJob {
 
 struct AdjPyrLevel {
   int njobs, total_px;
-  int max_blocks;                    // 32x8-pixel blocks of the largest job
+  int max_blocks;                    // 128x8-pixel blocks of the largest job
   AdjPyrJob job[2 * kMaxCams];
 };
 

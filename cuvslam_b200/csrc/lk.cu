@@ -109,7 +109,7 @@ cudaError_t launch(const LkLaunch& p, cudaStream_t s) {
     switch (p.shape) {
       case 1: return launch_shape<SAMPLING, HORIZ, MODE, 8, 3>(p, s);
       case 2: return launch_shape<SAMPLING, HORIZ, MODE, 4, 8>(p, s);
-      case 3: return launch_shape<SAMPLING, HORIZ, MODE, 16, 2>(p, s);
+      case 3: return launch_shape<SAMPLING, HORIZ, MODE, 12, 2>(p, s);
       default: break;
     }
   }

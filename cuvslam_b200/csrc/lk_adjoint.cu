@@ -44,7 +44,8 @@ constexpr int kTile = 32;
 constexpr int kGatherThreads = 256;
 constexpr int kGatherWarps = kGatherThreads / 32;
 constexpr int kWarpList = 32;  // most records per tile that one warp sums (gather_warp_kernel)
-constexpr int kLongBlocks = 296;  // CTAs of gather_long_kernel (two per SM), looping over the long tiles
+constexpr int kLongThreads = 1024;  // gather_long_kernel: one CTA per SM, 32 warps per long tile
+constexpr int kLongWarps = kLongThreads / 32;
 
 struct AdjSmem {
   WarpSmem win;               // staging windows, as the forward
@@ -137,33 +138,58 @@ __device__ __forceinline__ void store_record(float* dst, int gs, const float* sr
 struct Templ {
   float p1[kNE], a[kNE], b[kNE];
   float sp, gxx, gxy, gyy, det_rcp;
-  int bx, by;
+  int bx, by;  // the patch's 12x12 texel window
+  int ax;      // its staged window's first column (bx rounded down to a multiple of 4)
   TapSet ts;
 };
 
+// The current-image window for a patch at c, staged from the 16-byte aligned column at or below
+// the patch's first texel minus 2 when the window (wbx, wby) does not cover the patch's 12x12 texels
+// (the tracker's rule, lk_track.cuh); the caller waits.  Returns whether it staged.
+__device__ __forceinline__ bool stage_cur(const Level& CL, float cx, float cy, int& wbx, int& wby, AdjSmem& sm,
+                                          int lane) {
+  const float xmin = __fadd_rn(cx, -4.f), ymin = __fadd_rn(cy, -4.f);
+  const int nbx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, nby = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
+  if (nbx < wbx || nbx + kPW > wbx + 4 * kCA || nby < wby || nby + kPW > wby + kCW) {
+    wbx = (nbx - 2) & ~3;
+    wby = nby - 2;
+    stage_aligned<kCW, kCA, kCAS>(sm.win.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+    return true;
+  }
+  return false;
+}
+
+// CL (may be null): the current image, whose window for the first patch at c (wbx, wby updated) is
+// staged together with the template's so that one wait covers both.
 __device__ void make_template(const Level& PL, float sx, float sy, const bool (&valid)[kNE], const int (&ix)[kNE],
-                              const int (&iy)[kNE], const float (&wt)[kNE], AdjSmem& sm, int lane, Templ& T) {
+                              const int (&iy)[kNE], const float (&wt)[kNE], AdjSmem& sm, int lane, Templ& T,
+                              const Level* CL = nullptr, float2 c = make_float2(0.f, 0.f), int* wbx = nullptr,
+                              int* wby = nullptr) {
   const float rcp81 = 1.f / 81.f;
   const float xmin = __fadd_rn(sx, -4.f), ymin = __fadd_rn(sy, -4.f);
   T.bx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1;
   T.by = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
+  T.ax = T.bx & ~3;
   __syncwarp();
-  stage<kPW, kPS>(sm.win.img, PL.img, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
-  stage<kPW, kPS>(sm.win.gx, PL.gx, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
-  stage<kPW, kPS>(sm.win.gy, PL.gy, PL.pitch, PL.w, PL.h, T.bx, T.by, lane);
+  {
+    float* const wv[3] = {sm.win.img, sm.win.gx, sm.win.gy};
+    const float* const iv[3] = {PL.img, PL.gx, PL.gy};
+    stage_planes<kPW, kPA, kPAS, 3>(wv, iv, PL.pitch, PL.w, PL.h, T.ax, T.by, lane);
+  }
+  if (CL) stage_cur(*CL, c.x, c.y, *wbx, *wby, sm, lane);
   cp_async_wait_all();
   __syncwarp();
-  T.ts = make_taps<FE_SAMPLE_EXACT>(xmin, ymin, T.bx, T.by, kPS, lane);
+  T.ts = make_taps<FE_SAMPLE_EXACT>(xmin, ymin, T.ax, T.by, kPAS, lane);
   float gxp[kNE], gyp[kNE];
   float sgx = 0.f, sgy = 0.f, sp = 0.f;
 #pragma unroll
   for (int e = 0; e < kNE; ++e) {
     gxp[e] = gyp[e] = T.p1[e] = 0.f;
-    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.bx, T.by, kPS);
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.ax, T.by, kPAS);
     if (valid[e]) {
-      gxp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gx, kPS, t);
-      gyp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gy, kPS, t);
-      T.p1[e] = sample<FE_SAMPLE_EXACT>(sm.win.img, kPS, t);
+      gxp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gx, kPAS, t);
+      gyp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gy, kPAS, t);
+      T.p1[e] = sample<FE_SAMPLE_EXACT>(sm.win.img, kPAS, t);
       sgx = __fadd_rn(sgx, gxp[e]);
       sgy = __fadd_rn(sgy, gyp[e]);
       sp = __fadd_rn(sp, T.p1[e]);
@@ -200,16 +226,16 @@ __device__ void finish_template(const AdjLaunch& p, int g, int level, int W, int
   float sx = 0.f, sy = 0.f;
 #pragma unroll
   for (int e = 0; e < kNE; ++e) {
-    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.bx, T.by, kPS);
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.ax, T.by, kPAS);
     if (valid[e]) {
       float v, dx, dy;
-      sample_vg(sm.win.img, kPS, t, v, dx, dy);
+      sample_vg(sm.win.img, kPAS, t, v, dx, dy);
       sx = __fmaf_rn(p1b[e], dx, sx);
       sy = __fmaf_rn(p1b[e], dy, sy);
-      sample_vg(sm.win.gx, kPS, t, v, dx, dy);
+      sample_vg(sm.win.gx, kPAS, t, v, dx, dy);
       sx = __fmaf_rn(gxb[e], dx, sx);
       sy = __fmaf_rn(gxb[e], dy, sy);
-      sample_vg(sm.win.gy, kPS, t, v, dx, dy);
+      sample_vg(sm.win.gy, kPAS, t, v, dx, dy);
       sx = __fmaf_rn(gyb[e], dx, sx);
       sy = __fmaf_rn(gyb[e], dy, sy);
     }
@@ -243,21 +269,16 @@ __device__ __forceinline__ void finish_track(const AdjCam& cam, int i, float gtx
   }
 }
 
-// Stages the current-image 16x16 window for a patch at c when the window (wbx, wby) does not cover
-// it (as the forward does) and returns the patch's tap set.
+// The current-image window for a patch at c (staged and waited for when it does not cover the
+// patch) and the patch's tap set.
 __device__ __forceinline__ TapSet cur_taps(const Level& CL, float cx, float cy, int& wbx, int& wby, AdjSmem& sm,
                                            int lane) {
-  const float xmin = __fadd_rn(cx, -4.f), ymin = __fadd_rn(cy, -4.f);
-  const int nbx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, nby = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
-  if (nbx < wbx || nbx + kPW > wbx + kCW || nby < wby || nby + kPW > wby + kCW) {
-    wbx = nbx - 2;
-    wby = nby - 2;
-    __syncwarp();
-    stage<kCW, kCS>(sm.win.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+  __syncwarp();
+  if (stage_cur(CL, cx, cy, wbx, wby, sm, lane)) {
     cp_async_wait_all();
     __syncwarp();
   }
-  return make_taps<FE_SAMPLE_EXACT>(xmin, ymin, wbx, wby, kCS, lane);
+  return make_taps<FE_SAMPLE_EXACT>(__fadd_rn(cx, -4.f), __fadd_rn(cy, -4.f), wbx, wby, kCAS, lane);
 }
 
 __device__ __forceinline__ int patch_base(float c) {
@@ -305,17 +326,17 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
     const Level& CL = cam.lk.cur.lv[0];
     const int W = CL.w, H = CL.h;
     Templ T;
-    make_template(PL, sx, sy, valid, ix, iy, wt, sm, lane, T);
     int wbx = INT_MIN / 2, wby = INT_MIN / 2;
+    make_template(PL, sx, sy, valid, ix, iy, wt, sm, lane, T, &CL, make_float2(cx, cy), &wbx, &wby);
     const TapSet tc = cur_taps(CL, cx, cy, wbx, wby, sm, lane);
     float p2[kNE], dx[kNE], dy[kNE];
     float sc = 0.f, sdx = 0.f, sdy = 0.f;
 #pragma unroll
     for (int e = 0; e < kNE; ++e) {
       p2[e] = dx[e] = dy[e] = 0.f;
-      const Tap t = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCS);
+      const Tap t = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCAS);
       if (valid[e]) {
-        sample_vg(sm.win.cur, kCS, t, p2[e], dx[e], dy[e]);
+        sample_vg(sm.win.cur, kCAS, t, p2[e], dx[e], dy[e]);
         sc = __fadd_rn(sc, p2[e]);
         sdx = __fadd_rn(sdx, dx[e]);
         sdy = __fadd_rn(sdy, dy[e]);
@@ -422,8 +443,10 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
       const int W = CL.w, H = CL.h;
       const float2 s = R.s[level];
       Templ T;
-      make_template(PL, s.x, s.y, valid, ix, iy, wt, sm, lane, T);
       const int K = R.K[level];
+      int wbx = INT_MIN / 2, wby = INT_MIN / 2;  // current-image window (the first step replayed, t = K - 1)
+      make_template(PL, s.x, s.y, valid, ix, iy, wt, sm, lane, T, K > 0 ? &CL : nullptr,
+                    K > 0 ? R.it[level][K - 1] : make_float2(0.f, 0.f), &wbx, &wby);
       int lox = INT_MAX, loy = INT_MAX, hix = INT_MIN, hiy = INT_MIN;
       for (int t = 0; t < K; ++t) {
         const int bx = patch_base(R.it[level][t].x), by = patch_base(R.it[level][t].y);
@@ -467,7 +490,6 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
         pending = false;
       };
       float hxx = 0.f, hxy = 0.f, hyx = 0.f, hyy = 0.f;
-      int wbx = INT_MIN / 2, wby = INT_MIN / 2;
       for (int t = K - 1; t >= 0; --t) {
         const float2 c = R.it[level][t];
         const float2 v = R.v[level][t];
@@ -477,8 +499,8 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
           p2[e] = dx[e] = dy[e] = 0.f;
-          const Tap tp = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCS);
-          if (valid[e]) sample_vg(sm.win.cur, kCS, tp, p2[e], dx[e], dy[e]);
+          const Tap tp = tap_of<FE_SAMPLE_EXACT>(tc, ix[e], iy[e], wbx, wby, kCAS);
+          if (valid[e]) sample_vg(sm.win.cur, kCAS, tp, p2[e], dx[e], dy[e]);
         }
         // v = H^-1 e is recorded; mu = H^-1 cbar, Hbar -= mu v^T
         const float mux = __fmul_rn(__fmaf_rn(T.gyy, cbx, -__fmul_rn(T.gxy, cby)), T.det_rcp);
@@ -641,8 +663,8 @@ __global__ void bin_kernel(const __grid_constant__ AdjGather G) {
     }
 }
 
-// Exclusive prefix sum of the per-tile counts (one CTA); clears the fill cursors and lists the tiles
-// with more than kWarpList records.
+// Exclusive prefix sum of the per-tile counts (one CTA, four tiles per thread per pass); clears the
+// fill cursors and lists the tiles with more than kWarpList records.
 __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjGather G) {
   __shared__ int warp_tot[32];
   __shared__ int carry;
@@ -652,11 +674,16 @@ __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjG
     *G.long_count = 0;
   }
   __syncthreads();
-  for (int base = 0; base < G.total_tiles; base += 1024) {
-    const int t = base + tid;
-    const int v = t < G.total_tiles ? G.count[t] : 0;
-    if (v > kWarpList) G.long_tiles[atomicAdd(G.long_count, 1)] = t;  // processing order is free
-    int x = v;
+  for (int base = 0; base < G.total_tiles; base += 4096) {
+    const int t0 = base + 4 * tid;
+    int v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = t0 + k < G.total_tiles ? G.count[t0 + k] : 0;
+      if (v[k] > kWarpList) G.long_tiles[atomicAdd(G.long_count, 1)] = t0 + k;  // processing order is free
+    }
+    const int mine = v[0] + v[1] + v[2] + v[3];
+    int x = mine;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, d);
@@ -674,10 +701,14 @@ __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ AdjG
       warp_tot[lane] = w;  // inclusive
     }
     __syncthreads();
-    const int before = carry + (wid > 0 ? warp_tot[wid - 1] : 0) + x - v;
-    if (t < G.total_tiles) {
-      G.off[t] = before;
-      G.cursor[t] = 0;
+    int before = carry + (wid > 0 ? warp_tot[wid - 1] : 0) + x - mine;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (t0 + k < G.total_tiles) {
+        G.off[t0 + k] = before;
+        G.cursor[t0 + k] = 0;
+      }
+      before += v[k];
     }
     __syncthreads();
     if (tid == 0) carry += warp_tot[31];
@@ -767,12 +798,13 @@ __global__ void __launch_bounds__(kGatherThreads) gather_warp_kernel(const __gri
 }
 
 // Tiles with more than kWarpList records (coarse levels), from the scan's list: a CTA sorts the
-// tile's slots, warp k adds the k-th contiguous part of the sorted list (32 records at a time) into
-// its registers, and the eight partial tiles are summed in warp order.
-__global__ void __launch_bounds__(kGatherThreads) gather_long_kernel(const __grid_constant__ AdjGather G) {
+// tile's slots, warp k of 32 adds the k-th contiguous part of the sorted list (32 records at a time)
+// into its registers, and the 32 partial tiles are summed in warp order.  Each record costs its warp
+// one memory round trip, so the records of a tile are spread over as many warps as one CTA holds.
+__global__ void __launch_bounds__(kLongThreads, 1) gather_long_kernel(const __grid_constant__ AdjGather G) {
   extern __shared__ __align__(16) unsigned char gsm[];
-  float* part = reinterpret_cast<float*>(gsm);                                  // [kGatherWarps][1024]
-  int* keys = reinterpret_cast<int*>(gsm + kGatherWarps * kTile * kTile * 4);  // [list_cap]
+  float* part = reinterpret_cast<float*>(gsm);                                // [kLongWarps][1024]
+  int* keys = reinterpret_cast<int*>(gsm + kLongWarps * kTile * kTile * 4);  // [list_cap]
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nlong = *G.long_count;
   for (int li = blockIdx.x; li < nlong; li += gridDim.x) {
@@ -784,11 +816,11 @@ __global__ void __launch_bounds__(kGatherThreads) gather_long_kernel(const __gri
     int np2 = 1;
     while (np2 < n) np2 <<= 1;
     __syncthreads();  // the previous tile's readers of keys and part are done
-    for (int k = tid; k < np2; k += kGatherThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
+    for (int k = tid; k < np2; k += kLongThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
     __syncthreads();
     for (int size = 2; size <= np2; size <<= 1) {
       for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int k = tid; k < np2; k += kGatherThreads) {
+        for (int k = tid; k < np2; k += kLongThreads) {
           const int o = k ^ stride;
           if (o > k) {
             const int a = keys[k], b = keys[o];
@@ -804,7 +836,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_long_kernel(const __gri
     float acc[kTile];
 #pragma unroll
     for (int r = 0; r < kTile; ++r) acc[r] = 0.f;
-    const int r0 = (int)((long long)n * wid / kGatherWarps), r1 = (int)((long long)n * (wid + 1) / kGatherWarps);
+    const int r0 = (int)((long long)n * wid / kLongWarps), r1 = (int)((long long)n * (wid + 1) / kLongWarps);
     for (int g0 = r0; g0 < r1; g0 += 32) {
       const int m = min(32, r1 - g0);
       warp_add_records(G, lane < m ? keys[g0 + lane] : 0, m, X0, Y0, acc, lane);
@@ -812,11 +844,11 @@ __global__ void __launch_bounds__(kGatherThreads) gather_long_kernel(const __gri
 #pragma unroll
     for (int r = 0; r < kTile; ++r) part[wid * kTile * kTile + r * kTile + lane] = acc[r];
     __syncthreads();
-    for (int k = tid; k < kTile * kTile; k += kGatherThreads) {
+    for (int k = tid; k < kTile * kTile; k += kLongThreads) {
       const int X = X0 + (k & (kTile - 1)), Y = Y0 + k / kTile;
       if (X < P.w && Y < P.h) {
         float v = part[k];
-        for (int w = 1; w < kGatherWarps; ++w) v += part[w * kTile * kTile + k];
+        for (int w = 1; w < kLongWarps; ++w) v += part[w * kTile * kTile + k];
         P.dst[(size_t)Y * P.pitch + X] = v;
       }
     }
@@ -828,13 +860,11 @@ __device__ __forceinline__ float binom5(int k) {
   return k == 2 ? 6.f / 16.f : (k == 1 || k == 3) ? 4.f / 16.f : 1.f / 16.f;
 }
 
-// One launch per level; blockIdx.y = job (one pyramid of one camera), 32x8-pixel blocks.
-__global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_constant__ AdjPyrLevel L) {
-  const AdjPyrJob& J = L.job[blockIdx.y];
-  const int bx = (J.w + 31) >> 5;
-  const int x = (int)(blockIdx.x % bx) * 32 + (threadIdx.x & 31);
-  const int y = (int)(blockIdx.x / bx) * 8 + (threadIdx.x >> 5);
-  if (x >= J.w || y >= J.h) return;
+// Complete gradient of pixel (x, y) of one level: the summed records, the transposed 7-tap
+// derivatives of the gradient planes' adjoints (previous frame only) and the transposed 5x5
+// decimation of the next level's complete gradient.  Taps are added in a fixed order: derivative
+// taps j = 0..6 along x, then along y, then the decimation's rows and columns in ascending order.
+__device__ float adjoint_pixel(const AdjPyrJob& J, int x, int y) {
   float v = J.img[(size_t)y * J.pitch + x];
   if (J.gx) {
     // transposed 7-tap derivatives: gx(x') = sum_j D_j img(x' - 3 + j) for 2 < x' < w - 3
@@ -892,7 +922,79 @@ __global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_const
       }
     }
   }
-  J.img[(size_t)y * J.pitch + x] = v;
+  return v;
+}
+
+__device__ __forceinline__ void load4(const float* p, float* out) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  out[0] = q.x;
+  out[1] = q.y;
+  out[2] = q.z;
+  out[3] = q.w;
+}
+
+// One launch per level; blockIdx.y = job (one pyramid of one camera).  A thread takes four pixels
+// x .. x+3 (x a multiple of 4) of a row, 128x8-pixel blocks.  Away from the borders, with 16-byte
+// aligned planes, the taps come from 16-byte loads: the gradient row x-4 .. x+7, seven gradient
+// rows at x .. x+3, and two or three rows of the next level's gradient from the 4-aligned column at
+// or below x/2 - 1; every pixel adds the same taps in the same order as adjoint_pixel.  Elsewhere
+// each pixel runs adjoint_pixel.
+__global__ void __launch_bounds__(256) pyramid_adjoint_kernel(const __grid_constant__ AdjPyrLevel L) {
+  const AdjPyrJob& J = L.job[blockIdx.y];
+  const int bx = (J.w + 127) >> 7;
+  const int x = ((int)(blockIdx.x % bx) * 32 + (threadIdx.x & 31)) * 4;
+  const int y = (int)(blockIdx.x / bx) * 8 + (threadIdx.x >> 5);
+  if (x >= J.w || y >= J.h) return;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(J.img) | reinterpret_cast<uintptr_t>(J.gx) |
+                         reinterpret_cast<uintptr_t>(J.gy) | reinterpret_cast<uintptr_t>(J.up)) & 15) == 0 &&
+                       ((J.pitch | J.gpitch | J.up_pitch) & 3) == 0;
+  const int ub = (x >> 1) - 1 >= 0 ? (((x >> 1) - 1) & ~3) : 0;  // first next-level column loaded
+  const bool fast = aligned && x >= 8 && x + 10 <= J.w && y >= 6 && y + 7 <= J.h &&
+                    (!J.up || (ub + 8 <= J.up_w && ((y + 2) >> 1) < J.up_h));
+  if (!fast) {
+    for (int i = 0; i < 4 && x + i < J.w; ++i) {
+      const float v = adjoint_pixel(J, x + i, y);
+      J.img[(size_t)y * J.pitch + x + i] = v;
+    }
+    return;
+  }
+  float v[4];
+  load4(J.img + (size_t)y * J.pitch + x, v);
+  if (J.gx) {
+    // x' = x + i - j + 3 runs over x - 3 .. x + 6, all inside (2, w - 3): row values x - 4 .. x + 7
+    float r[12];
+    const float* gr = J.gx + (size_t)y * J.gpitch + x - 4;
+    load4(gr, r);
+    load4(gr + 4, r + 4);
+    load4(gr + 8, r + 8);
+#pragma unroll
+    for (int j = 0; j < 7; ++j)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = __fmaf_rn(dsp_tap(j), r[i - j + 7], v[i]);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      float c[4];
+      load4(J.gy + (size_t)(y - j + 3) * J.gpitch + x, c);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = __fmaf_rn(dsp_tap(j), c[i], v[i]);
+    }
+  }
+  if (J.up) {
+    // pixel x + i reads next-level columns (x + i + 2 - kx) / 2 for kx of its parity, rows likewise
+    for (int ky = y & 1; ky < 5; ky += 2) {
+      const int Y = (y + 2 - ky) >> 1;
+      float u[8];
+      const float* ur = J.up + (size_t)Y * J.up_pitch + ub;
+      load4(ur, u);
+      load4(ur + 4, u + 4);
+      const float wy = binom5(ky);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int kx = i & 1; kx < 5; kx += 2) v[i] = __fmaf_rn(__fmul_rn(wy, binom5(kx)), u[((x + i + 2 - kx) >> 1) - ub], v[i]);
+    }
+  }
+  *reinterpret_cast<float4*>(J.img + (size_t)y * J.pitch + x) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
 }  // namespace
@@ -902,7 +1004,7 @@ size_t lk_record_bytes() { return sizeof(LkRecord); }
 
 cudaError_t adjoint_init() {
   cudaError_t e = cudaFuncSetAttribute(gather_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kGatherWarps * kTile * kTile * 4 + kMaxSelectKeys * 4);
+                                       kLongWarps * kTile * kTile * 4 + kMaxSelectKeys * 4);
   return e;
 }
 
@@ -927,9 +1029,15 @@ cudaError_t launch_adjoint_gather(const AdjGather& g, cudaStream_t s) {
   if (nb > 0) bin_kernel<false><<<nb, 256, 0, s>>>(g);
   scan_kernel<<<1, 1024, 0, s>>>(g);
   if (nb > 0) bin_kernel<true><<<nb, 256, 0, s>>>(g);
-  const size_t smem = kGatherWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4;
+  const size_t smem = kLongWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4;
   gather_warp_kernel<<<(g.total_tiles + kGatherWarps - 1) / kGatherWarps, kGatherThreads, 0, s>>>(g);
-  gather_long_kernel<<<kLongBlocks, kGatherThreads, smem, s>>>(g);
+  static const int sms = [] {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+  }();
+  gather_long_kernel<<<sms, kLongThreads, smem, s>>>(g);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,12 @@ namespace lk {
 
 constexpr int kPW = 12, kPS = 13;  // previous-frame window 12x12, row stride 13
 constexpr int kCW = 16, kCS = 17;  // current-frame window 16x16, row stride 17
+// The tracker's windows start at a 16-byte aligned column (the origin rounded down to a multiple of
+// 4 texels) and are staged as 16-byte row chunks: 12 rows of 4 chunks (16 texels) for the previous
+// frame, 16 rows of 5 chunks (20 texels) for the current frame, which covers the 12- and 16-texel
+// windows from any origin.
+constexpr int kPA = 4, kPAS = 16;  // previous-frame chunks per row, row stride
+constexpr int kCA = 5, kCAS = 20;  // current-frame chunks per row, row stride
 constexpr int kNE = 3;             // taps per lane: ceil(81 / 32)
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -48,6 +54,33 @@ template <int SAMPLING>
 __device__ __forceinline__ TapSet make_taps(float xmin, float ymin, int bx, int by, int stride, int lane) {
   TapSet s;
   const bool is_col = lane < 9, is_row = lane >= 16 && lane < 25;
+  // Common case, decided warp-uniformly without shuffles: when xmin and xmin + 8 share an FP32
+  // exponent (no binade boundary inside the patch; xmin >= 0 here), every xmin + i is exact, and
+  // so are the - 0.5 and the fraction; the columns then have consecutive texels and one fraction,
+  // and the same holds for the rows.  The per-lane values below are those the general path
+  // computes, which would find the taps uniform too.
+  if ((((__float_as_uint(xmin) ^ __float_as_uint(__fadd_rn(xmin, 8.f))) |
+        (__float_as_uint(ymin) ^ __float_as_uint(__fadd_rn(ymin, 8.f)))) >> 23) == 0) {
+    const float pbx = __fsub_rn(xmin, 0.5f), pby = __fsub_rn(ymin, 0.5f);
+    const float flx = floorf(pbx), fly = floorf(pby);
+    const float frx = __fsub_rn(pbx, flx), fry = __fsub_rn(pby, fly);
+    const int b0x = (int)flx, b0y = (int)fly;
+    const int q0x = quantised(SAMPLING) ? (int)floorf(__fmaf_rn(frx, 256.f, 0.5f)) : 0;
+    const int q0y = quantised(SAMPLING) ? (int)floorf(__fmaf_rn(fry, 256.f, 0.5f)) : 0;
+    s.uniform = true;
+    s.base = is_col ? b0x + lane : (is_row ? b0y + (lane - 16) : b0y);
+    s.fr = is_col ? frx : fry;
+    s.q = is_col ? q0x : q0y;
+    if (quantised(SAMPLING)) {
+      tex_weights(q0x, q0y, s.u);
+    } else {
+      s.u.w00 = frx;
+      s.u.w10 = fry;
+      s.u.w01 = s.u.w11 = 0.f;
+    }
+    s.u.off = (b0y - by) * stride + (b0x - bx);
+    return s;
+  }
   const float p = is_col ? __fadd_rn(xmin, (float)lane) : __fadd_rn(ymin, (float)(is_row ? lane - 16 : 0));
   const float pb = __fsub_rn(p, 0.5f);
   const float fl = floorf(pb);
@@ -129,12 +162,57 @@ __device__ __forceinline__ void stage(float* win, const float* img, int pitch, i
   }
 }
 
-struct WarpSmem {
-  float img[kPW * kPS];
-  float gx[kPW * kPS];
-  float gy[kPW * kPS];
-  float cur[kCW * kCS];
+// Rows [by, by + ROWS) x columns [ax, ax + 4 CHUNKS) (ax a multiple of 4) of NP planes that share
+// one pitch, clamped to the image as the texture's clamp mode: 16-byte asynchronous copies when the
+// block lies inside the image (its rows start 16-byte aligned: 16-byte aligned planes and pitches),
+// else one texel at a time, each lane owning a column (its clamped x computed once) and a share of
+// the rows.  The caller waits (cp_async_wait_all) and then __syncwarp()s.
+template <int ROWS, int CHUNKS, int S, int NP>
+__device__ __forceinline__ void stage_planes(float* const (&win)[NP], const float* const (&img)[NP], int pitch, int w,
+                                             int h, int ax, int by, int lane) {
+  if (ax >= 0 && by >= 0 && ax + 4 * CHUNKS <= w && by + ROWS <= h) {
+#pragma unroll
+    for (int i = lane; i < ROWS * CHUNKS; i += 32) {
+      const int r = i / CHUNKS, k = i - r * CHUNKS;
+      const size_t go = (size_t)(by + r) * pitch + ax + 4 * k;
+#pragma unroll
+      for (int q = 0; q < NP; ++q) cp_async16(win[q] + r * S + 4 * k, img[q] + go);
+    }
+  } else {
+    constexpr int C = 4 * CHUNKS, LPC = 32 / C;  // columns, lanes per column
+    static_assert(LPC >= 1, "a warp covers a row");
+    if (lane < C * LPC) {
+      const int c = lane % C;
+      const int x = min(max(ax + c, 0), w - 1);
+#pragma unroll 4
+      for (int r = lane / C; r < ROWS; r += LPC) {
+        const size_t go = (size_t)min(max(by + r, 0), h - 1) * pitch + x;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) cp_async4(win[q] + r * S + c, img[q] + go);
+      }
+    }
+  }
+}
+
+template <int ROWS, int CHUNKS, int S>
+__device__ __forceinline__ void stage_aligned(float* win, const float* img, int pitch, int w, int h, int ax, int by,
+                                              int lane) {
+  float* const wv[1] = {win};
+  const float* const iv[1] = {img};
+  stage_planes<ROWS, CHUNKS, S, 1>(wv, iv, pitch, w, h, ax, by, lane);
+}
+
+// Windows of one warp: sized for both the adjoint's layout (kPS / kCS strides) and the tracker's
+// aligned one (kPAS / kCAS); 16-byte aligned for the chunked copies.
+struct alignas(16) WarpSmem {
+  float img[kPW * kPAS];
+  float gx[kPW * kPAS];
+  float gy[kPW * kPAS];
+  float cur[kCW * kCAS];
 };
+static_assert(kPW * kPAS >= kPW * kPS && kCW * kCAS >= kCW * kCS, "window arrays hold both layouts");
+static_assert(kPW * kPAS % 4 == 0 && kCW * kCAS % 4 == 0, "16-byte aligned window arrays");
+static_assert(4 * kPA >= kPW + 3 && 4 * kCA >= kCW + 3, "aligned windows cover the windows from any origin");
 
 // Value and spatial derivative of the bilinear interpolant at tap t (exact weights: t.w00 = fx,
 // t.w10 = fy).  The value is computed exactly as sample<FE_SAMPLE_EXACT>.

@@ -75,6 +75,14 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
       const cudaTextureObject_t t_gy = HORIZ ? 0 : (cudaTextureObject_t)T.prev_gy[level];
       const cudaTextureObject_t t_p1 = (cudaTextureObject_t)T.prev_img[level];
       const cudaTextureObject_t t_p2 = (cudaTextureObject_t)T.cur_img[level];
+      // the first Gauss-Newton step's patch (the loop's first iterate, same coordinates), fetched
+      // together with the template's so that both wait on one texture round trip
+      float p2[kTE];
+      {
+        const float xm = (cx + -4.f), ym = (cy + -4.f);
+#pragma unroll
+        for (int e = 0; e < kTE; ++e) p2[e] = valid[e] ? tex(t_p2, (xm + fx[e]), (ym + fy[e])) : 0.f;
+      }
       float gxp[kTE], gyp[kTE], p1[kTE];
       float sgx = 0.f, sgy = 0.f, sp = 0.f;
 #pragma unroll
@@ -129,9 +137,6 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
         det_rcp = __fdividef(1.0f, det);
       }
       const float savex = cx, savey = cy;
-      float p2[kTE];
-#pragma unroll
-      for (int e = 0; e < kTE; ++e) p2[e] = 0.f;
       for (int it = 0; it < 11; ++it) {
         xmin = (cx + -4.f);
         ymin = (cy + -4.f);
@@ -140,7 +145,7 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
 #pragma unroll
         for (int e = 0; e < kTE; ++e) {
           if (valid[e]) {
-            p2[e] = tex(t_p2, (xmin + fx[e]), (ymin + fy[e]));
+            if (it > 0) p2[e] = tex(t_p2, (xmin + fx[e]), (ymin + fy[e]));
             sc = (sc + p2[e]);
           }
         }

@@ -87,25 +87,44 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
     }
     if (good) {
       if (cnt && lane == 0) atomicAdd(cnt, 1ull);
-      // previous-frame patch: image and gradients
+      // previous-frame patch: image and gradients; the window [bx, bx + 12) is staged from the
+      // 16-byte aligned column ax = bx rounded down to a multiple of 4
       const int bx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, by = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
+      const int ax = bx & ~3;
       __syncwarp();
-      stage<kPW, kPS>(sm.img, PL.img, PL.pitch, PL.w, PL.h, bx, by, lane);
-      stage<kPW, kPS>(sm.gx, PL.gx, PL.pitch, PL.w, PL.h, bx, by, lane);
-      if (!HORIZ) stage<kPW, kPS>(sm.gy, PL.gy, PL.pitch, PL.w, PL.h, bx, by, lane);
+      if (HORIZ) {
+        float* const wv[2] = {sm.img, sm.gx};
+        const float* const iv[2] = {PL.img, PL.gx};
+        stage_planes<kPW, kPA, kPAS, 2>(wv, iv, PL.pitch, PL.w, PL.h, ax, by, lane);
+      } else {
+        float* const wv[3] = {sm.img, sm.gx, sm.gy};
+        const float* const iv[3] = {PL.img, PL.gx, PL.gy};
+        stage_planes<kPW, kPA, kPAS, 3>(wv, iv, PL.pitch, PL.w, PL.h, ax, by, lane);
+      }
+      // the current frame's window for the first Gauss-Newton step (the origin gn_step would choose),
+      // staged together with the previous frame's so that one wait covers both
+      int wbx = INT_MIN / 2, wby = INT_MIN / 2;  // current-frame window origin (none yet)
+      {
+        const float cxm = __fadd_rn(cx, -4.f), cym = __fadd_rn(cy, -4.f);
+        if (cxm >= 0.f && __fadd_rn(cx, 5.f) < (float)W && cym >= 0.f && __fadd_rn(cy, 5.f) < (float)H) {
+          wbx = ((int)floorf(__fsub_rn(cxm, 0.5f)) - 3) & ~3;
+          wby = (int)floorf(__fsub_rn(cym, 0.5f)) - 3;
+          stage_aligned<kCW, kCA, kCAS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+        }
+      }
       cp_async_wait_all();
       __syncwarp();
-      const TapSet ts = make_taps<SAMPLING>(xmin, ymin, bx, by, kPS, lane);
+      const TapSet ts = make_taps<SAMPLING>(xmin, ymin, ax, by, kPAS, lane);
       float gxp[kNE], gyp[kNE], p1[kNE];
       float sgx = 0.f, sgy = 0.f, sp = 0.f;
 #pragma unroll
       for (int e = 0; e < kNE; ++e) {
         gxp[e] = gyp[e] = p1[e] = 0.f;
-        const Tap t = tap_of<SAMPLING>(ts, ix[e], iy[e], bx, by, kPS);
+        const Tap t = tap_of<SAMPLING>(ts, ix[e], iy[e], ax, by, kPAS);
         if (valid[e]) {
-          gxp[e] = sample<SAMPLING>(sm.gx, kPS, t);
-          if (!HORIZ) gyp[e] = sample<SAMPLING>(sm.gy, kPS, t);
-          p1[e] = sample<SAMPLING>(sm.img, kPS, t);
+          gxp[e] = sample<SAMPLING>(sm.gx, kPAS, t);
+          if (!HORIZ) gyp[e] = sample<SAMPLING>(sm.gy, kPAS, t);
+          p1[e] = sample<SAMPLING>(sm.img, kPAS, t);
           sgx = __fadd_rn(sgx, gxp[e]);
           if (!HORIZ) sgy = __fadd_rn(sgy, gyp[e]);
           sp = __fadd_rn(sp, p1[e]);
@@ -154,7 +173,6 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
       float p2[kNE];
 #pragma unroll
       for (int e = 0; e < kNE; ++e) p2[e] = 0.f;
-      int wbx = INT_MIN / 2, wby = INT_MIN / 2;  // current-frame window origin (none yet)
       float last_delta = 0.f;
       // One Gauss-Newton step at (cx, cy): samples p2 and returns the update; false when the patch
       // leaves the level.
@@ -162,23 +180,24 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
         xmin = __fadd_rn(cx, -4.f);
         ymin = __fadd_rn(cy, -4.f);
         if (!(xmin >= 0.f && __fadd_rn(cx, 5.f) < (float)W && ymin >= 0.f && __fadd_rn(cy, 5.f) < (float)H)) return false;
-        // taps reach texels [base0 - 1, base0 + 10]; keep the 16x16 window while it covers them
+        // taps reach texels [base0 - 1, base0 + 10]; keep the window (20 columns from the aligned
+        // wbx, 16 rows from wby) while it covers them
         const int nbx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, nby = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
-        if (nbx < wbx || nbx + kPW > wbx + kCW || nby < wby || nby + kPW > wby + kCW) {
-          wbx = nbx - 2;
+        if (nbx < wbx || nbx + kPW > wbx + 4 * kCA || nby < wby || nby + kPW > wby + kCW) {
+          wbx = (nbx - 2) & ~3;
           wby = nby - 2;
           __syncwarp();
-          stage<kCW, kCS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+          stage_aligned<kCW, kCA, kCAS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
           cp_async_wait_all();
           __syncwarp();
         }
-        const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCS, lane);
+        const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCAS, lane);
         float sc = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
-          const Tap t = tap_of<SAMPLING>(tc, ix[e], iy[e], wbx, wby, kCS);
+          const Tap t = tap_of<SAMPLING>(tc, ix[e], iy[e], wbx, wby, kCAS);
           if (valid[e]) {
-            p2[e] = sample<SAMPLING>(sm.cur, kCS, t);
+            p2[e] = sample<SAMPLING>(sm.cur, kCAS, t);
             sc = __fadd_rn(sc, p2[e]);
           }
         }
@@ -278,23 +297,23 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           ymin = __fadd_rn(cy, -4.f);
           if (!(xmin >= 0.f && __fadd_rn(cx, 5.f) < (float)W && ymin >= 0.f && __fadd_rn(cy, 5.f) < (float)H)) break;
           const int nbx = (int)floorf(__fsub_rn(xmin, 0.5f)) - 1, nby = (int)floorf(__fsub_rn(ymin, 0.5f)) - 1;
-          if (nbx < wbx || nbx + kPW > wbx + kCW || nby < wby || nby + kPW > wby + kCW) {
-            wbx = nbx - 2;
+          if (nbx < wbx || nbx + kPW > wbx + 4 * kCA || nby < wby || nby + kPW > wby + kCW) {
+            wbx = (nbx - 2) & ~3;
             wby = nby - 2;
             __syncwarp();
-            stage<kCW, kCS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
+            stage_aligned<kCW, kCA, kCAS>(sm.cur, CL.img, CL.pitch, CL.w, CL.h, wbx, wby, lane);
             cp_async_wait_all();
             __syncwarp();
           }
-          const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCS, lane);
+          const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCAS, lane);
           float dxs[kNE], dys[kNE];
           float sc = 0.f, sdx = 0.f, sdy = 0.f;
 #pragma unroll
           for (int e = 0; e < kNE; ++e) {
             dxs[e] = dys[e] = 0.f;
-            const Tap t = tap_of<SAMPLING>(tc, ix[e], iy[e], wbx, wby, kCS);
+            const Tap t = tap_of<SAMPLING>(tc, ix[e], iy[e], wbx, wby, kCAS);
             if (valid[e]) {
-              sample_vg(sm.cur, kCS, t, p2[e], dxs[e], dys[e]);
+              sample_vg(sm.cur, kCAS, t, p2[e], dxs[e], dys[e]);
               sc = __fadd_rn(sc, p2[e]);
               sdx = __fadd_rn(sdx, dxs[e]);
               sdy = __fadd_rn(sdy, dys[e]);

@@ -669,63 +669,83 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
     }
   }
 
-  // 4. core outputs, four pixels per thread and store
+  // 4. core outputs
   // level 0: 128x128 from the uint8 tile.  Bytes become floats exactly as (2^23 + b) - 2^23 (a byte
   // permute into the mantissa, then one packed subtract per pair); the 7-tap derivatives of pixel
   // pairs run as packed FP32x2 FMAs, each lane rounding exactly as the scalar FMA chain.
+  // (a) image and grad_y: a thread takes a pixel pair's column over a strip of 16 rows and slides the
+  //     derivative's 7-row window down it in registers, so each byte is converted once per strip.
+  {
+    const int pc = tid & 63, strip = tid >> 6;  // 64 pairs x 8 strips of 16 rows
+    const int x = 4 * X2 + 2 * pc, y0 = 4 * Y2 + 16 * strip;
+    if (x < w0 && y0 < h0) {
+      const uint8_t* colp = B0 + (y0 - a0y - 3) * kS0W + (x - a0x);  // rows y0-3 .. y0+18
+      auto pair = [&](int k) {
+        return bytes_to_float2((uint32_t)*reinterpret_cast<const uint16_t*>(colp + k * kS0W), 0);
+      };
+      const bool two = x + 1 < w0;
+      float2 win[7];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) win[k] = pair(k);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        win[6] = pair(i + 6);
+        const int y = y0 + i;
+        if (y < h0) {
+          float2 gy = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int j = 0; j < 7; ++j) {
+            if (j == 3) continue;
+            gy = __ffma2_rn(make_float2(dsp_tap(j), dsp_tap(j)), win[j], gy);
+          }
+          if (!(y > 2 && y < h0 - 3)) gy = make_float2(0.f, 0.f);
+          const int64_t o = (int64_t)y * L0.pitch + x;
+          if (two) {
+            *reinterpret_cast<float2*>(L0.img + o) = win[3];
+            *reinterpret_cast<float2*>(L0.gy + o) = gy;
+          } else {
+            L0.img[o] = win[3].x;
+            L0.gy[o] = gy.x;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) win[k] = win[k + 1];
+      }
+    }
+  }
+  // (b) grad_x: a thread takes four pixels of a row and their horizontal neighbours x-4 .. x+7.
 #pragma unroll 1
   for (int q = tid; q < 128 * 32; q += kThreads) {
     const int y = 4 * Y2 + (q >> 5), x = 4 * X2 + (q & 31) * 4;
     if (y >= h0 || x >= w0) continue;
-    const int r = y - a0y, c = x - a0x;
-    float2 col[7][2];  // rows y-3 .. y+3, pixel pairs (x, x+1) and (x+2, x+3)
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const uint32_t wd = *reinterpret_cast<const uint32_t*>(B0 + (r - 3 + k) * kS0W + c);
-      col[k][0] = bytes_to_float2(wd, 0);
-      col[k][1] = bytes_to_float2(wd, 2);
-    }
-    // horizontal neighbours x-4 .. x+7 as pairs; the middle word is row y of the column window
-    const uint32_t wl = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c - 4);
-    const uint32_t wr = *reinterpret_cast<const uint32_t*>(B0 + r * kS0W + c + 4);
-    const float2 v[6] = {bytes_to_float2(wl, 0), bytes_to_float2(wl, 2), col[3][0],
-                         col[3][1],              bytes_to_float2(wr, 0), bytes_to_float2(wr, 2)};
+    const uint8_t* p = B0 + (y - a0y) * kS0W + (x - a0x);
+    const uint32_t wl = *reinterpret_cast<const uint32_t*>(p - 4);
+    const uint32_t wm = *reinterpret_cast<const uint32_t*>(p);
+    const uint32_t wr = *reinterpret_cast<const uint32_t*>(p + 4);
+    const float2 v[6] = {bytes_to_float2(wl, 0), bytes_to_float2(wl, 2), bytes_to_float2(wm, 0),
+                         bytes_to_float2(wm, 2), bytes_to_float2(wr, 0), bytes_to_float2(wr, 2)};
     // pixel x+i needs v at flat indices 1+i+j (j = 0..6); pairs (i, i+1) for i = 0, 2
     auto hv = [&](int f) { return (f & 1) ? make_float2(v[f >> 1].y, v[(f >> 1) + 1].x) : v[f >> 1]; };
-    float2 gx2[2], gy2[2];
+    float2 gx2[2];
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      float2 sx = make_float2(0.f, 0.f), sy = make_float2(0.f, 0.f);
+    for (int pp = 0; pp < 2; ++pp) {
+      float2 sx = make_float2(0.f, 0.f);
 #pragma unroll
       for (int j = 0; j < 7; ++j) {
         if (j == 3) continue;
-        const float2 d = make_float2(dsp_tap(j), dsp_tap(j));
-        sx = __ffma2_rn(d, hv(1 + 2 * p + j), sx);
-        sy = __ffma2_rn(d, col[j][p], sy);
+        sx = __ffma2_rn(make_float2(dsp_tap(j), dsp_tap(j)), hv(1 + 2 * pp + j), sx);
       }
-      gx2[p] = sx;
-      gy2[p] = sy;
+      gx2[pp] = sx;
     }
-    const bool vin = y > 2 && y < h0 - 3;
     float gx[4] = {gx2[0].x, gx2[0].y, gx2[1].x, gx2[1].y};
-    float gy[4] = {gy2[0].x, gy2[0].y, gy2[1].x, gy2[1].y};
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 4; ++i)
       if (!(x + i > 2 && x + i < w0 - 3)) gx[i] = 0.f;
-      if (!vin) gy[i] = 0.f;
-    }
-    const float img[4] = {v[2].x, v[2].y, v[3].x, v[3].y};
     const int64_t o = (int64_t)y * L0.pitch + x;
     if (x + 3 < w0) {
-      *reinterpret_cast<float4*>(L0.img + o) = make_float4(img[0], img[1], img[2], img[3]);
       *reinterpret_cast<float4*>(L0.gx + o) = make_float4(gx[0], gx[1], gx[2], gx[3]);
-      *reinterpret_cast<float4*>(L0.gy + o) = make_float4(gy[0], gy[1], gy[2], gy[3]);
     } else {
-      for (int i = 0; i < 4 && x + i < w0; ++i) {
-        L0.img[o + i] = img[i];
-        L0.gx[o + i] = gx[i];
-        L0.gy[o + i] = gy[i];
-      }
+      for (int i = 0; i < 4 && x + i < w0; ++i) L0.gx[o + i] = gx[i];
     }
   }
   // levels 1 and 2 from their shared-memory tiles

@@ -425,7 +425,7 @@ class Batch:
     OVERLAP = ["after LK", "beside LK", "beside deep pyramid stages and LK"]
 
     def set_tuning(self, lk_block="8x4", response_overlap="beside LK", stage_tile=8, l012_ctas_per_sm=2):
-        shape = ["8x4", "8x3", "4x8", "16x2"].index(lk_block)
+        shape = ["8x4", "8x3", "4x8", "12x2"].index(lk_block)
         tile = int(stage_tile) | (64 if int(l012_ctas_per_sm) == 3 else 0)
         _lib.check(self.ctx.lib.fe_batch_set_tuning(self.handle, shape, self.OVERLAP.index(response_overlap), tile),
                    "fe_batch_set_tuning")
@@ -433,7 +433,7 @@ class Batch:
     def tuning(self):
         v = [ctypes.c_int32() for _ in range(3)]
         _lib.check(self.ctx.lib.fe_batch_tuning(self.handle, *[ctypes.byref(x) for x in v]), "fe_batch_tuning")
-        shapes = ["8x4", "8x3", "4x8", "16x2"]
+        shapes = ["8x4", "8x3", "4x8", "12x2"]
         return {"lk_block": shapes[v[0].value], "response_overlap": self.OVERLAP[v[1].value],
                 "stage_tile": v[2].value & 31, "l012_ctas_per_sm": 3 if v[2].value & 64 else 2}
 

@@ -430,7 +430,7 @@ FE_API int fe_batch_kernel_count(fe_batch* batch);
  * (the drop-in launch pattern of MonoSOFGPU::track, sof_mono_gpu.cpp:106-137), for comparison. */
 FE_API int fe_batch_run_plain(fe_batch* batch, fe_stream stream);
 /* Autotuner: times the planned step (reps graph launches per candidate, after one warm-up) over
- *   the LK block shape (warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 16x2),
+ *   the LK block shape (warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 12x2),
  *   the response tiles after LK (0), on a second stream beside LK (1), or beside the deeper
  *   pyramid stages and LK (2),
  *   the generic pyramid stages' deepest-level tile (8 or 16) and the levels 0-2 kernel's register

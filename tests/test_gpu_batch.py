@@ -114,7 +114,7 @@ def test_autotuned_batch_gives_the_same_results(ctx):
             f.tracks.copy_(tracks_to_device(t))
     torch.cuda.synchronize()
     tuned = b.autotune(reps=2)
-    assert tuned["lk_block"] in ("8x4", "8x3", "4x8", "16x2") and tuned["stage_tile"] in (8, 16)
+    assert tuned["lk_block"] in ("8x4", "8x3", "4x8", "12x2") and tuned["stage_tile"] in (8, 16)
     assert tuned["response_overlap"] in Batch.OVERLAP and tuned["l012_ctas_per_sm"] in (2, 3)
     for f, t in zip(frames, host):  # restored by the tuner
         if f.tracks is not None:
@@ -128,7 +128,7 @@ def test_autotuned_batch_gives_the_same_results(ctx):
         for x, y in zip(pa, pb):
             np.testing.assert_array_equal(x, y)
     # every combination of shapes, set directly
-    for block in ("8x4", "8x3", "4x8", "16x2"):
+    for block in ("8x4", "8x3", "4x8", "12x2"):
         for overlap in Batch.OVERLAP:
             for tile, ctas in ((8, 2), (16, 3)):
                 b.set_tuning(block, overlap, tile, ctas)
