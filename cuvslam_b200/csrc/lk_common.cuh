@@ -50,7 +50,9 @@ struct TapSet {
 // Texture-unit weight rule (8-bit fractions) in both texture modes.
 constexpr bool quantised(int sampling) { return sampling != FE_SAMPLE_EXACT; }
 
-template <int SAMPLING>
+// PER_LANE = false: in the common case the per-lane column/row values (only the non-uniform taps
+// read them) are left at zero.
+template <int SAMPLING, bool PER_LANE = true>
 __device__ __forceinline__ TapSet make_taps(float xmin, float ymin, int bx, int by, int stride, int lane) {
   TapSet s;
   const bool is_col = lane < 9, is_row = lane >= 16 && lane < 25;
@@ -68,9 +70,14 @@ __device__ __forceinline__ TapSet make_taps(float xmin, float ymin, int bx, int 
     const int q0x = quantised(SAMPLING) ? (int)floorf(__fmaf_rn(frx, 256.f, 0.5f)) : 0;
     const int q0y = quantised(SAMPLING) ? (int)floorf(__fmaf_rn(fry, 256.f, 0.5f)) : 0;
     s.uniform = true;
-    s.base = is_col ? b0x + lane : (is_row ? b0y + (lane - 16) : b0y);
-    s.fr = is_col ? frx : fry;
-    s.q = is_col ? q0x : q0y;
+    if (PER_LANE) {
+      s.base = is_col ? b0x + lane : (is_row ? b0y + (lane - 16) : b0y);
+      s.fr = is_col ? frx : fry;
+      s.q = is_col ? q0x : q0y;
+    } else {
+      s.base = s.q = 0;
+      s.fr = 0.f;
+    }
     if (quantised(SAMPLING)) {
       tex_weights(q0x, q0y, s.u);
     } else {

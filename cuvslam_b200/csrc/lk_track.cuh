@@ -114,7 +114,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
       }
       cp_async_wait_all();
       __syncwarp();
-      const TapSet ts = make_taps<SAMPLING>(xmin, ymin, ax, by, kPAS, lane);
+      const TapSet ts = make_taps<SAMPLING, false>(xmin, ymin, ax, by, kPAS, lane);
       float gxp[kNE], gyp[kNE], p1[kNE];
       float sgx = 0.f, sgy = 0.f, sp = 0.f;
 #pragma unroll
@@ -191,7 +191,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           cp_async_wait_all();
           __syncwarp();
         }
-        const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCAS, lane);
+        const TapSet tc = make_taps<SAMPLING, false>(xmin, ymin, wbx, wby, kCAS, lane);
         float sc = 0.f;
 #pragma unroll
         for (int e = 0; e < kNE; ++e) {
@@ -305,7 +305,7 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
             cp_async_wait_all();
             __syncwarp();
           }
-          const TapSet tc = make_taps<SAMPLING>(xmin, ymin, wbx, wby, kCAS, lane);
+          const TapSet tc = make_taps<SAMPLING, false>(xmin, ymin, wbx, wby, kCAS, lane);
           float dxs[kNE], dys[kNE];
           float sc = 0.f, sdx = 0.f, sdy = 0.f;
 #pragma unroll

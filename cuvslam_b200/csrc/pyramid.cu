@@ -573,40 +573,71 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
     __syncthreads();
   }
 
-  // 2. level 1: column strips of 14 rows, sliding window of horizontal sums
-  if (tid < kS1 * 6) {
-    const int c = tid % kS1, band = tid / kS1;
+  // 2. level 1 (integer sums: exact in any order): a thread takes a pair of columns (c, c + 1) and a
+  //    band of 7 rows, sliding the 5-row window of horizontal sums down the band.  Away from the
+  //    image's edges the taps of both columns are bytes 4 pp + 14 .. 4 pp + 20 of a staged row: three
+  //    words, one byte permute and two dp4a with the weights (1, 4, 6, 4) plus the fifth tap; near an
+  //    edge each column takes its mirrored taps one by one.
+  if (tid < 40 * 12) {
+    const int pp = tid % 40, band = tid / 40;
+    const int c = 2 * pp;
+    const int ys = max(a1y + band * 7, 0), ye = min(a1y + min(band * 7 + 7, kS1), h1);
     const int x1 = a1x + c;
-    const int ys = max(a1y + band * 14, 0), ye = min(a1y + min(band * 14 + 14, kS1), h1);
-    if (x1 >= 0 && x1 < w1 && ys < ye) {
-      int col[5];
-#pragma unroll
-      for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * x1 - 2 + l, w0) - a0x;
-      // away from the left/right edges the five taps are contiguous bytes: two aligned words, a byte
-      // permute to taps 0-3 and one dp4a with the weights (1, 4, 6, 4), plus tap 4
-      const bool contiguous = 2 * x1 - 2 >= 0 && 2 * x1 + 2 < w0;
-      const int wofs = col[0] & ~3;
-      const uint32_t sel = (col[0] & 3) ? 0x5432u : 0x3210u;
-      const int sh4 = (col[0] & 3) ? 16 : 0;
-      auto H = [&](int r) {
-        const uint8_t* p = B0 + (mirror_index(r, h0) - a0y) * kS0W;
-        if (contiguous) {
-          const uint32_t w0_ = *reinterpret_cast<const uint32_t*>(p + wofs);
-          const uint32_t w1_ = *reinterpret_cast<const uint32_t*>(p + wofs + 4);
-          return (int)__dp4a(__byte_perm(w0_, w1_, sel), 0x04060401u, (w1_ >> sh4) & 0xffu);
+    if (ys < ye) {
+      if (2 * x1 - 2 >= 0 && 2 * x1 + 4 < w0 && c + 1 < kS1 && 2 * ys - 2 >= 0 && 2 * ye < h0) {
+        const uint8_t* p = B0 + (2 * ys - 2 - a0y) * kS0W + 4 * pp + 12;
+        auto H2 = [&](const uint8_t* q, int& ha, int& hb) {
+          const uint32_t wa = *reinterpret_cast<const uint32_t*>(q);
+          const uint32_t wb = *reinterpret_cast<const uint32_t*>(q + 4);
+          const uint32_t wc = *reinterpret_cast<const uint32_t*>(q + 8);
+          ha = (int)__dp4a(__byte_perm(wa, wb, 0x5432u), 0x04060401u, (wb >> 16) & 0xffu);
+          hb = (int)__dp4a(wb, 0x04060401u, wc & 0xffu);
+        };
+        int a0_, b0_, a1_, b1_, a2_, b2_, a3_, b3_, a4_, b4_;
+        H2(p, a0_, b0_);
+        H2(p + kS0W, a1_, b1_);
+        H2(p + 2 * kS0W, a2_, b2_);
+        p += 3 * kS0W;
+        for (int y = ys;;) {
+          H2(p, a3_, b3_);
+          H2(p + kS0W, a4_, b4_);
+          const int Sa = a0_ + a4_ + 4 * (a1_ + a3_) + 6 * a2_;
+          const int Sb = b0_ + b4_ + 4 * (b1_ + b3_) + 6 * b2_;
+          *reinterpret_cast<float2*>(B1 + (y - a1y) * kS1S + c) =
+              make_float2((float)Sa * (1.f / 256.f), (float)Sb * (1.f / 256.f));
+          if (++y >= ye) break;
+          a0_ = a2_;
+          b0_ = b2_;
+          a1_ = a3_;
+          b1_ = b3_;
+          a2_ = a4_;
+          b2_ = b4_;
+          p += 2 * kS0W;
         }
-        return (int)p[col[0]] + (int)p[col[4]] + 4 * ((int)p[col[1]] + (int)p[col[3]]) + 6 * (int)p[col[2]];
-      };
-      int h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
-      for (int y = ys;; ) {
-        const int S = h0_ + h4_ + 4 * (h1_ + h3_) + 6 * h2_;
-        B1[(y - a1y) * kS1S + c] = (float)S * (1.f / 256.f);
-        if (++y >= ye) break;
-        h0_ = h2_;
-        h1_ = h3_;
-        h2_ = h4_;
-        h3_ = H(2 * y + 1);
-        h4_ = H(2 * y + 2);
+      } else {
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+          const int cc = c + k, xx = x1 + k;
+          if (cc >= kS1 || xx < 0 || xx >= w1) continue;
+          int col[5];
+#pragma unroll
+          for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * xx - 2 + l, w0) - a0x;
+          auto H = [&](int r) {
+            const uint8_t* q = B0 + (mirror_index(r, h0) - a0y) * kS0W;
+            return (int)q[col[0]] + (int)q[col[4]] + 4 * ((int)q[col[1]] + (int)q[col[3]]) + 6 * (int)q[col[2]];
+          };
+          int h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
+          for (int y = ys;;) {
+            const int S = h0_ + h4_ + 4 * (h1_ + h3_) + 6 * h2_;
+            B1[(y - a1y) * kS1S + cc] = (float)S * (1.f / 256.f);
+            if (++y >= ye) break;
+            h0_ = h2_;
+            h1_ = h3_;
+            h2_ = h4_;
+            h3_ = H(2 * y + 1);
+            h4_ = H(2 * y + 2);
+          }
+        }
       }
     }
   }
@@ -618,29 +649,68 @@ __device__ __forceinline__ void l012_tile(const StageBatch& batch, const StageJo
   }
   __syncthreads();
 
-  // 3. level 2 from level 1, same scheme in FP32 (exact)
-  if (tid < kS2 * 13) {
-    const int c = tid % kS2, band = tid / kS2;
+  // 3. level 2 from level 1, same scheme in FP32 (exact: level 1 holds multiples of 1/256 below 256
+  //    and every partial sum fits FP32's 24 bits): a pair of columns and a band of 3 rows per thread;
+  //    away from the edges both columns' taps are the level-1 values 4 pp .. 4 pp + 6 of a row (two
+  //    16-byte loads)
+  if (tid < 19 * 13) {
+    const int pp = tid % 19, band = tid / 19;
+    const int c = 2 * pp;
     const int x2 = X2 - 3 + c;
     const int ys = max(a2y + band * 3, 0), ye = min(a2y + min(band * 3 + 3, kS2), h2);
-    if (x2 >= 0 && x2 < w2 && ys < ye) {
-      int col[5];
+    if (ys < ye) {
+      if (2 * x2 - 2 >= 0 && 2 * x2 + 4 < w1 && 2 * ys - 2 >= 0 && 2 * ye < h1) {
+        const float* p = B1 + (2 * ys - 2 - a1y) * kS1S + 4 * pp;
+        auto H2 = [&](const float* q, float& ha, float& hb) {
+          const float4 u = *reinterpret_cast<const float4*>(q);
+          const float4 v = *reinterpret_cast<const float4*>(q + 4);
+          ha = (u.x + v.x) + 4.f * (u.y + u.w) + 6.f * u.z;
+          hb = (u.z + v.z) + 4.f * (u.w + v.y) + 6.f * v.x;
+        };
+        float a0_, b0_, a1_, b1_, a2_, b2_, a3_, b3_, a4_, b4_;
+        H2(p, a0_, b0_);
+        H2(p + kS1S, a1_, b1_);
+        H2(p + 2 * kS1S, a2_, b2_);
+        p += 3 * kS1S;
+        for (int y = ys;;) {
+          H2(p, a3_, b3_);
+          H2(p + kS1S, a4_, b4_);
+          float* o = B2 + (y - a2y) * kS2S + (x2 - a2x);
+          o[0] = ((a0_ + a4_) + 4.f * (a1_ + a3_) + 6.f * a2_) * (1.f / 256.f);
+          o[1] = ((b0_ + b4_) + 4.f * (b1_ + b3_) + 6.f * b2_) * (1.f / 256.f);
+          if (++y >= ye) break;
+          a0_ = a2_;
+          b0_ = b2_;
+          a1_ = a3_;
+          b1_ = b3_;
+          a2_ = a4_;
+          b2_ = b4_;
+          p += 2 * kS1S;
+        }
+      } else {
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+          const int xx = x2 + k;
+          if (xx < 0 || xx >= w2) continue;
+          int col[5];
 #pragma unroll
-      for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * x2 - 2 + l, w1) - a1x;
-      auto H = [&](int r) {
-        const float* p = B1 + (mirror_index(r, h1) - a1y) * kS1S;
-        return (p[col[0]] + p[col[4]]) + 4.f * (p[col[1]] + p[col[3]]) + 6.f * p[col[2]];
-      };
-      float h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
-      for (int y = ys;; ) {
-        const float S = (h0_ + h4_) + 4.f * (h1_ + h3_) + 6.f * h2_;
-        B2[(y - a2y) * kS2S + (x2 - a2x)] = S * (1.f / 256.f);
-        if (++y >= ye) break;
-        h0_ = h2_;
-        h1_ = h3_;
-        h2_ = h4_;
-        h3_ = H(2 * y + 1);
-        h4_ = H(2 * y + 2);
+          for (int l = 0; l < 5; ++l) col[l] = mirror_index(2 * xx - 2 + l, w1) - a1x;
+          auto H = [&](int r) {
+            const float* q = B1 + (mirror_index(r, h1) - a1y) * kS1S;
+            return (q[col[0]] + q[col[4]]) + 4.f * (q[col[1]] + q[col[3]]) + 6.f * q[col[2]];
+          };
+          float h0_ = H(2 * ys - 2), h1_ = H(2 * ys - 1), h2_ = H(2 * ys), h3_ = H(2 * ys + 1), h4_ = H(2 * ys + 2);
+          for (int y = ys;;) {
+            const float S = (h0_ + h4_) + 4.f * (h1_ + h3_) + 6.f * h2_;
+            B2[(y - a2y) * kS2S + (xx - a2x)] = S * (1.f / 256.f);
+            if (++y >= ye) break;
+            h0_ = h2_;
+            h1_ = h3_;
+            h2_ = h4_;
+            h3_ = H(2 * y + 1);
+            h4_ = H(2 * y + 2);
+          }
+        }
       }
     }
   }

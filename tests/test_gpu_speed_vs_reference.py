@@ -2,7 +2,8 @@
 cuVSLAM sources for sm_100a into oracle/_ref by oracle/build_ref.sh) on the same inputs: one
 1920x1200 frame pair (seeded scene, similarity warp), 8192 Shi-Tomasi features with predicted
 offsets.  Stages: the current frame's pyramid + gradients (uint8 in device memory -> every level),
-pyramidal LK (texture-weight emulation), the affine tracker (0 shift + 20 full steps) and its cached
+pyramidal LK (texture-weight emulation, and the texture unit's own filtering; 8191 tracks and the same
+features seven times over, 57 337), the affine tracker (0 shift + 20 full steps) and its cached
 variant.  Both sides are timed with CUDA events around the stage alone (records reset before each
 run, outside the timed interval, and the host's enqueue time hidden behind a spin kernel), mean of 20 runs after 3 warm-up
 runs.  Prints one JSON line.
@@ -87,6 +88,17 @@ def test_stages_vs_reference_kernels(ctx):
     lk = LKFeatureTracker(ctx, False, _lib.FE_SAMPLE_TEXTURE)
     ours["lk"] = _ours(lambda: lk.track_points(pp, cp, d), lambda: d.copy_(src))
     ref["lk"] = _ref_stage(lib, prev, nxt, rec, 1)
+    lk_hw = LKFeatureTracker(ctx, False, _lib.FE_SAMPLE_HARDWARE)
+    ours["lk_hw"] = _ours(lambda: lk_hw.track_points(pp, cp, d), lambda: d.copy_(src))
+    ref["lk_hw"] = ref["lk"]
+    # the same features seven times over: 57 337 tracks, the 32-camera step's track count
+    rec7 = np.tile(rec, 7)
+    src7 = torch.from_numpy(rec7.view(np.uint8).reshape(len(rec7), 80).copy()).to(dev)
+    d7 = src7.clone()
+    ours["lk_57k"] = _ours(lambda: lk.track_points(pp, cp, d7), lambda: d7.copy_(src7))
+    ours["lk_hw_57k"] = _ours(lambda: lk_hw.track_points(pp, cp, d7), lambda: d7.copy_(src7))
+    ref["lk_57k"] = _ref_stage(lib, prev, nxt, rec7, 1)
+    ref["lk_hw_57k"] = ref["lk_57k"]
     st = STFeatureTracker(ctx, 0, 20)
     ours["affine"] = _ours(lambda: st.track_points(pp, cp, d), lambda: d.copy_(src))
     ref["affine"] = _ref_stage(lib, prev, nxt, rec, 2)
@@ -97,7 +109,7 @@ def test_stages_vs_reference_kernels(ctx):
     src_c = d.clone()
     ours["affine_cached"] = _ours(lambda: stc.track_points(cp, cache, d), lambda: d.copy_(src_c))
     ref["affine_cached"] = _ref_stage(lib, prev, nxt, rec, 3)
-    line = {"workload": f"{W}x{H} pair, {len(rec)} Shi-Tomasi features", "ours_ms": ours, "reference_ms": ref,
+    line = {"workload": f"{W}x{H} pair, {len(rec)} Shi-Tomasi features (lk_57k: {len(rec7)} tracks)", "ours_ms": ours, "reference_ms": ref,
             "speedup": {k: ref[k] / ours[k] for k in ours}}
     print(json.dumps(line))
     for k in ("pyramid", "affine", "affine_cached"):
