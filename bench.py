@@ -57,6 +57,9 @@ def parse():
                          "'part'), whole batched steps (ranges named 'step'), or the LK adjoint workload's "
                          "forward and backward in one mode (ranges 'fwd', 'bwd'), warmup + steps times, or "
                          "the affine tracker's workload alone")
+    ap.add_argument("--adj-cams", type=int, default=None,
+                    help="cameras of the LK adjoint workload under --profile implicit/unrolled (a smaller case "
+                         "for an ncu capture; default 8)")
     return ap.parse_args()
 
 
@@ -862,6 +865,10 @@ def profile_adjoint(args, local):
     import torch
 
     from cuvslam_b200.frontend import Context
+
+    global ADJ_CAMS
+    if args.adj_cams:
+        ADJ_CAMS = int(args.adj_cams)
 
     torch.cuda.set_device(local)
     ctx = Context(local)

@@ -743,6 +743,15 @@ __device__ __forceinline__ void warp_add_records(const AdjGather& G, int key, in
                                                  int lane) {
   const int4 mine = lane < m ? G.hdr[key] : make_int4(0, 0, 0, 0);
   const int X = X0 + lane;
+  if (lane < m) {
+    // every record of the group is requested into L2 up front (lane r: record r's rows inside the
+    // tile), so that the in-order adds below wait on L2 rather than on DRAM
+    int S;
+    const float* d = record_data(G, key, S) + max(0, X0 - mine.x);
+    const int r1 = min(mine.w, Y0 + kTile - mine.y);
+    for (int row = max(0, Y0 - mine.y); row < r1; ++row)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(d + (size_t)row * S));
+  }
   for (int r = 0; r < m; ++r) {
     const int k = __shfl_sync(kFull, key, r);
     const int hx = __shfl_sync(kFull, mine.x, r), hy = __shfl_sync(kFull, mine.y, r);
@@ -797,14 +806,18 @@ __global__ void __launch_bounds__(kGatherThreads) gather_warp_kernel(const __gri
   }
 }
 
-// Tiles with more than kWarpList records (coarse levels), from the scan's list: a CTA sorts the
-// tile's slots, warp k of 32 adds the k-th contiguous part of the sorted list (32 records at a time)
+// Tiles with more than kWarpList records (coarse levels), from the scan's list: a CTA orders the
+// tile's slots by track, warp k of 32 adds the k-th contiguous part of the sorted list (32 records at a time)
 // into its registers, and the 32 partial tiles are summed in warp order.  Each record costs its warp
 // one memory round trip, so the records of a tile are spread over as many warps as one CTA holds.
 __global__ void __launch_bounds__(kLongThreads, 1) gather_long_kernel(const __grid_constant__ AdjGather G) {
   extern __shared__ __align__(16) unsigned char gsm[];
   float* part = reinterpret_cast<float*>(gsm);                                // [kLongWarps][1024]
   int* keys = reinterpret_cast<int*>(gsm + kLongWarps * kTile * kTile * 4);  // [list_cap]
+  const int nwords = (G.list_cap + 31) >> 5;                                  // bitmap words (<= 1024)
+  uint32_t* bits = reinterpret_cast<uint32_t*>(keys + G.list_cap);            // [nwords]
+  int* prefix = reinterpret_cast<int*>(bits + nwords);                        // [nwords]
+  __shared__ int wsum[32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nlong = *G.long_count;
   for (int li = blockIdx.x; li < nlong; li += gridDim.x) {
@@ -813,26 +826,49 @@ __global__ void __launch_bounds__(kLongThreads, 1) gather_long_kernel(const __gr
     const int lt = t - P.tile_begin;
     const int X0 = (lt % P.tiles_x) * kTile, Y0 = (lt / P.tiles_x) * kTile;
     const int begin = G.off[t], n = min(G.off[t + 1] - begin, G.list_cap);
-    int np2 = 1;
-    while (np2 < n) np2 <<= 1;
-    __syncthreads();  // the previous tile's readers of keys and part are done
-    for (int k = tid; k < np2; k += kLongThreads) keys[k] = k < n ? G.list[begin + k] : INT_MAX;
+    // the tile's records in track order without a comparison sort: a tile belongs to one plane of
+    // one camera, so each record is a distinct track of that camera; mark the tracks in a bitmap,
+    // then a record's rank is the number of marked tracks before it
+    const int pi = (int)(&P - G.planes);
+    const int cbegin = G.cams[pi / (4 * G.L)].lk.begin;
+    __syncthreads();  // the previous tile's readers of keys, bitmap and part are done
+    for (int k = tid; k < nwords; k += kLongThreads) bits[k] = 0u;
     __syncthreads();
-    for (int size = 2; size <= np2; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int k = tid; k < np2; k += kLongThreads) {
-          const int o = k ^ stride;
-          if (o > k) {
-            const int a = keys[k], b = keys[o];
-            if ((a > b) == ((k & size) == 0)) {
-              keys[k] = b;
-              keys[o] = a;
-            }
-          }
-        }
-        __syncthreads();
-      }
+    for (int k = tid; k < n; k += kLongThreads) {
+      const int rel = G.list[begin + k] % G.total - cbegin;
+      atomicOr(&bits[rel >> 5], 1u << (rel & 31));
     }
+    __syncthreads();
+    // exclusive prefix of the words' population counts (nwords <= kLongThreads)
+    {
+      const int c = tid < nwords ? __popc(bits[tid]) : 0;
+      int x = c;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, d);
+        if (lane >= d) x += y;
+      }
+      if (lane == 31) wsum[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        int w = wsum[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_up_sync(kFull, w, d);
+          if (lane >= d) w += y;
+        }
+        wsum[lane] = w;
+      }
+      __syncthreads();
+      if (tid < nwords) prefix[tid] = (wid > 0 ? wsum[wid - 1] : 0) + x - c;
+    }
+    __syncthreads();
+    for (int k = tid; k < n; k += kLongThreads) {
+      const int key = G.list[begin + k];
+      const int rel = key % G.total - cbegin;
+      keys[prefix[rel >> 5] + __popc(bits[rel >> 5] & ((1u << (rel & 31)) - 1u))] = key;
+    }
+    __syncthreads();
     float acc[kTile];
 #pragma unroll
     for (int r = 0; r < kTile; ++r) acc[r] = 0.f;
@@ -1004,7 +1040,7 @@ size_t lk_record_bytes() { return sizeof(LkRecord); }
 
 cudaError_t adjoint_init() {
   cudaError_t e = cudaFuncSetAttribute(gather_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kLongWarps * kTile * kTile * 4 + kMaxSelectKeys * 4);
+                                       kLongWarps * kTile * kTile * 4 + kMaxSelectKeys * 4 + 8 * (kMaxSelectKeys / 32));
   return e;
 }
 
@@ -1029,7 +1065,7 @@ cudaError_t launch_adjoint_gather(const AdjGather& g, cudaStream_t s) {
   if (nb > 0) bin_kernel<false><<<nb, 256, 0, s>>>(g);
   scan_kernel<<<1, 1024, 0, s>>>(g);
   if (nb > 0) bin_kernel<true><<<nb, 256, 0, s>>>(g);
-  const size_t smem = kLongWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4;
+  const size_t smem = kLongWarps * kTile * kTile * 4 + (size_t)g.list_cap * 4 + 8 * (size_t)((g.list_cap + 31) / 32);
   gather_warp_kernel<<<(g.total_tiles + kGatherWarps - 1) / kGatherWarps, kGatherThreads, 0, s>>>(g);
   static const int sms = [] {
     int dev = 0, n = 0;
