@@ -949,10 +949,16 @@ def main():
         host_tracks.append(t)
         prev_pyr.append(pp)
         cur_pyr.append(ImagePyramid(w, h, device=dev))
+    # every camera's tracks in one device buffer (a view per camera), so that a step's inputs are
+    # restored with one copy
+    trk_offs = np.concatenate([[0], np.cumsum([len(t) for t in host_tracks])]).astype(np.int64)
+    trk_all = torch.empty((int(trk_offs[-1]), 80), dtype=torch.uint8, device=dev)
     for i in range(len(shapes)):
-        td = tracks_to_device(host_tracks[i], dev)
-        pristine.append(td.clone())
+        td = trk_all[trk_offs[i]:trk_offs[i + 1]]
+        td.copy_(tracks_to_device(host_tracks[i], dev))
         frames.append(CameraFrame(img_dev[i], cur_pyr[i], prev_pyr[i], td, counts[i], (0, 0, 0, 0)))
+    pristine_all = trk_all.clone()
+    pristine = [pristine_all[trk_offs[i]:trk_offs[i + 1]] for i in range(len(shapes))]
     batch = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)
     tuning = batch.autotune(reps=10, stream=stream)  # restores the tracks it moved
     attempted = sum(len(t) for t in host_tracks)
@@ -982,8 +988,7 @@ def main():
     kernels_per_step = batch.kernel_count()
 
     def restore():
-        for f, p in zip(frames, pristine):
-            f.tracks.copy_(p, non_blocking=True)
+        trk_all.copy_(pristine_all, non_blocking=True)
 
     def step_batched():
         restore()
@@ -1017,19 +1022,20 @@ def main():
     # ---- the whole MonoSOFGPU frame: the same step plus the retrack pass and the finish filters
     #      (collect, ages, border kill, collapse) between LK and selection
     from cuvslam_b200.frontend import TrackFinish
-    fin_frames, fin_ages = [], []
-    for f, p in zip(frames, pristine):
-        age = torch.ones(p.shape[0], dtype=torch.int32, device=dev)
-        fin_ages.append(age)
+    fin_frames = []
+    fin_trk = pristine_all.clone()
+    fin_age0 = torch.ones(int(trk_offs[-1]), dtype=torch.int32, device=dev)
+    fin_age = fin_age0.clone()
+    for i, f in enumerate(frames):
         fin_frames.append(CameraFrame(f.image, ImagePyramid(f.image.shape[1], f.image.shape[0], device=dev), f.prev,
-                                      p.clone(), f.num_desired, f.border, finish=TrackFinish(age.clone(), 0.85)))
+                                      fin_trk[trk_offs[i]:trk_offs[i + 1]], f.num_desired, f.border,
+                                      finish=TrackFinish(fin_age[trk_offs[i]:trk_offs[i + 1]], 0.85)))
     batch_f = Batch(ctx, fin_frames, _lib.FE_SAMPLE_TEXTURE)
     batch_f.set_tuning(**tuning)
 
     def step_finish():
-        for f, p, a in zip(fin_frames, pristine, fin_ages):
-            f.tracks.copy_(p, non_blocking=True)
-            f.finish.age.copy_(a, non_blocking=True)
+        fin_trk.copy_(pristine_all, non_blocking=True)
+        fin_age.copy_(fin_age0, non_blocking=True)
         batch_f.run(stream)
 
     ms_fin = timed(step_finish, max(3, args.steps // 2), 2)
@@ -1040,24 +1046,48 @@ def main():
     ms_plain = timed(step_plain, max(3, args.steps // 2), 2)
     plain_value = throughput(total_units, max(3, args.steps // 2), ms_plain)
 
-    # ---- end to end through the public API with host buffers
-    pin_imgs = [torch.from_numpy(n).pin_memory() for n in nexts]
-    pin_tracks = [torch.from_numpy(np.ascontiguousarray(t).view(np.uint8).reshape(len(t), 80).copy()).pin_memory()
-                  for t in host_tracks]
-    out_tracks = [torch.empty_like(t).pin_memory() for t in pin_tracks]
-    out_new = [torch.empty((f.new_xy.shape[0], 2), dtype=torch.float32).pin_memory() for f in frames]
-    out_cnt = [torch.empty(1, dtype=torch.int32).pin_memory() for _ in frames]
-    h2d = sum(i.numel() for i in pin_imgs) + sum(t.numel() for t in pin_tracks)
-    d2h = sum(t.numel() for t in out_tracks) + sum(o.numel() * 4 for o in out_new) + 4 * len(out_cnt)
+    # ---- end to end through the public API with host buffers: every camera's frame and tracks in
+    #      one pinned host buffer each (as a capture ring would hold them), so that a step's inputs go
+    #      up in two copies and its results come back in three
+    img_sizes = [n.size for n in nexts]
+    img_offs = np.concatenate([[0], np.cumsum(img_sizes)]).astype(np.int64)
+    trk_counts = [len(t) for t in host_tracks]
+    trk_offs = np.concatenate([[0], np.cumsum(trk_counts)]).astype(np.int64)
+    nd_counts = [max(f.num_desired, 1) for f in frames]
+    nd_offs = np.concatenate([[0], np.cumsum(nd_counts)]).astype(np.int64)
+    pin_img = torch.empty(int(img_offs[-1]), dtype=torch.uint8).pin_memory()
+    pin_trk = torch.empty((int(trk_offs[-1]), 80), dtype=torch.uint8).pin_memory()
+    for i, n in enumerate(nexts):
+        pin_img[img_offs[i]:img_offs[i + 1]].copy_(torch.from_numpy(n.reshape(-1)))
+        pin_trk[trk_offs[i]:trk_offs[i + 1]].copy_(
+            torch.from_numpy(np.ascontiguousarray(host_tracks[i]).view(np.uint8).reshape(-1, 80)))
+    out_trk = torch.empty_like(pin_trk).pin_memory()
+    out_new = torch.empty((int(nd_offs[-1]), 2), dtype=torch.float32).pin_memory()
+    out_cnt = torch.empty(len(frames), dtype=torch.int32).pin_memory()
+    h2d = pin_img.numel() + pin_trk.numel()
+    d2h = out_trk.numel() + out_new.numel() * 4 + out_cnt.numel() * 4
 
-    # Two batches over the same cameras (own frame buffers, current pyramids, tracks and outputs; the
-    # previous pyramids shared read-only) in ping-pong: while one computes its step, the other's
-    # frames and tracks come in on an upload stream and its results go out on a download stream.
-    frames_b = [CameraFrame(torch.empty_like(f.image), ImagePyramid(f.image.shape[1], f.image.shape[0], device=dev),
-                            f.prev, f.tracks.clone(), f.num_desired, f.border) for f in frames]
-    batch_b = Batch(ctx, frames_b, _lib.FE_SAMPLE_TEXTURE)
-    batch_b.set_tuning(**tuning)
-    sets = [(batch, frames), (batch_b, frames_b)]
+    # Two batches over the same cameras (own packed frame, track and output buffers and current
+    # pyramids; the previous pyramids shared read-only) in ping-pong: while one computes its step, the
+    # other's frames and tracks come in on an upload stream and its results go out on a download stream.
+    def packed_set():
+        d_img = torch.empty_like(pin_img, device=dev)
+        d_trk = torch.empty_like(pin_trk, device=dev)
+        d_new = torch.zeros((int(nd_offs[-1]), 2), dtype=torch.float32, device=dev)
+        d_cnt = torch.zeros(len(frames), dtype=torch.int32, device=dev)
+        fr = []
+        for i, f in enumerate(frames):
+            h, w = f.image.shape
+            cf = CameraFrame(d_img[img_offs[i]:img_offs[i + 1]].view(h, w), ImagePyramid(w, h, device=dev), f.prev,
+                             d_trk[trk_offs[i]:trk_offs[i + 1]], f.num_desired, f.border)
+            cf.new_xy = d_new[nd_offs[i]:nd_offs[i + 1]]
+            cf.new_count = d_cnt[i:i + 1]
+            fr.append(cf)
+        bt = Batch(ctx, fr, _lib.FE_SAMPLE_TEXTURE)
+        bt.set_tuning(**tuning)
+        return bt, (d_img, d_trk, d_new, d_cnt)
+
+    sets = [packed_set(), packed_set()]
     up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     ev_in = [torch.cuda.Event() for _ in range(2)]
     ev_done = [torch.cuda.Event() for _ in range(2)]
@@ -1066,22 +1096,20 @@ def main():
         e.record(stream)
 
     def step_e2e(k):
-        b, fr = sets[k % 2]
+        b, (d_img, d_trk, d_new, d_cnt) = sets[k % 2]
         with torch.cuda.stream(up):
             up.wait_event(ev_free[k % 2])  # this set's previous results are out
-            for f, pi, pt in zip(fr, pin_imgs, pin_tracks):
-                f.image.copy_(pi, non_blocking=True)
-                f.tracks.copy_(pt, non_blocking=True)
+            d_img.copy_(pin_img, non_blocking=True)
+            d_trk.copy_(pin_trk, non_blocking=True)
             ev_in[k % 2].record(up)
         stream.wait_event(ev_in[k % 2])
         b.run(stream)
         ev_done[k % 2].record(stream)
         with torch.cuda.stream(down):
             down.wait_event(ev_done[k % 2])
-            for f, ot, on, oc in zip(fr, out_tracks, out_new, out_cnt):
-                ot.copy_(f.tracks, non_blocking=True)
-                on.copy_(f.new_xy, non_blocking=True)
-                oc.copy_(f.new_count, non_blocking=True)
+            out_trk.copy_(d_trk, non_blocking=True)
+            out_new.copy_(d_new, non_blocking=True)
+            out_cnt.copy_(d_cnt, non_blocking=True)
             ev_free[k % 2].record(down)
 
     for k in range(max(args.warmup, 3)):
@@ -1208,7 +1236,8 @@ def main():
                                   "what": "the step plus the retrack pass (NCC 0.85) and the finish filters"},
             "parts_ms": part_ms,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "pipeline": "two batches in ping-pong, uploads and downloads on their own streams"},
+                    "pipeline": "two batches in ping-pong, uploads and downloads on their own streams; each step's "
+                                "inputs and results in packed pinned buffers (2 copies up, 3 down)"},
             "roofline": {"bound": "hbm", "kernel": "pyramid stages (all cameras)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": traffic_src, "algorithmic_bytes": alg_bytes, "peak_source": peak_src},
@@ -1229,7 +1258,8 @@ def main():
         }
         print(json.dumps(line), flush=True)
     batch.close()
-    batch_b.close()
+    for bt, _ in sets:
+        bt.close()
     batch_f.close()
     ctx.close()
     if dist:
