@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
 // Redoes the cells that an alive feature's 9x9 window reaches: NMS again from the response map,
 // burned pixels zeroed (filter_maximums_kernel, selection_v2.cu:251-277), the cell's max/argmax
 // again with the reference's lane order, then the refinement.  One warp per 32 cells of the
-// touched-cell bit mask.
+// touched-cell bit mask, four touched cells at a time.
 __global__ void __launch_bounds__(256) cells_kernel(const __grid_constant__ SelectBatch b, int words_total) {
   const int lane = threadIdx.x & 31;
   const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -440,48 +440,57 @@ __global__ void __launch_bounds__(256) cells_kernel(const __grid_constant__ Sele
   const int word = gw - c.touched_begin;
   const int vcw = (c.w + 7) / 8, vch = (c.h + 7) / 8;  // cell grid incl. partial border cells
   if (word * 32 >= vcw * vch) return;
-  uint32_t bits = c.touched[word];
+  const uint32_t bits = c.touched[word];
   const int w = c.w, h = c.h, cw = w / 8, ch = h / 8;
   const int bwords = (w + 31) / 32;
-  while (bits) {
-    const int k = __ffs(bits) - 1;
-    bits &= bits - 1;
-    const int vcell = word * 32 + k;
-    if (vcell >= vcw * vch) break;
+  // the word's touched cells, four at a time: eight lanes per cell, lane g of a cell scanning the
+  // reference's lanes 4g .. 4g+3 (pixels l and l + 32 of lane l, the second taken only when strictly
+  // greater) and a 3-level merge that keeps the lower lane on ties: the first maximum in the
+  // reference's (lane, element) order, as downsample_gftt_x8_kernel's warp finds it
+  const uint32_t valid = (word * 32 + 32 <= vcw * vch) ? 0xffffffffu : ((1u << (vcw * vch - word * 32)) - 1u);
+  const uint32_t cells = bits & valid;
+  const int ncells = __popc(cells);
+  const int j = lane >> 3, g = lane & 7;
+  for (int base = 0; base < ncells; base += 4) {
+    const int ci = base + j;
+    const int k = ci < ncells ? (int)__fns(cells, 0, ci + 1) : -1;
+    const int vcell = word * 32 + (k >= 0 ? k : 0);
     const int cellx = vcell % vcw, celly = vcell / vcw;
     float m = 0.f;
     unsigned idx = 0;
+    if (k >= 0) {
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int f = lane + 32 * e, dy = f >> 3, dx = f & 7;
-      const int x = cellx * 8 + dx, y = celly * 8 + dy;
-      if (x < w && y < h && !((c.burn[(size_t)y * bwords + (x >> 5)] >> (x & 31)) & 1u)) {
-        const float v = c.resp[(size_t)y * w + x];
-        bool is_max = true;
+      for (int kk = 0; kk < 8; ++kk) {
+        const int f = 4 * g + (kk >> 1) + 32 * (kk & 1), dy = f >> 3, dx = f & 7;
+        const int x = cellx * 8 + dx, y = celly * 8 + dy;
+        if (x < w && y < h && !((c.burn[(size_t)y * bwords + (x >> 5)] >> (x & 31)) & 1u)) {
+          const float v = c.resp[(size_t)y * w + x];
+          bool is_max = true;
 #pragma unroll
-        for (int ny = -1; ny <= 1; ++ny)
+          for (int ny = -1; ny <= 1; ++ny)
 #pragma unroll
-          for (int nx = -1; nx <= 1; ++nx) {
-            if (!nx && !ny) continue;
-            const int yy = min(max(y + ny, 0), h - 1), xx = min(max(x + nx, 0), w - 1);
-            is_max &= c.resp[(size_t)yy * w + xx] <= v;
+            for (int nx = -1; nx <= 1; ++nx) {
+              if (!nx && !ny) continue;
+              const int yy = min(max(y + ny, 0), h - 1), xx = min(max(x + nx, 0), w - 1);
+              is_max &= c.resp[(size_t)yy * w + xx] <= v;
+            }
+          if (is_max && v > m) {
+            m = v;
+            idx = (unsigned)dx | ((unsigned)dy << 16);
           }
-        if (is_max && v > m) {
-          m = v;
-          idx = (unsigned)dx | ((unsigned)dy << 16);
         }
       }
     }
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const float m2 = __shfl_down_sync(0xffffffffu, m, d);
-      const unsigned i2 = __shfl_down_sync(0xffffffffu, idx, d);
+    for (int d = 1; d < 8; d <<= 1) {
+      const float m2 = __shfl_down_sync(0xffffffffu, m, d, 8);
+      const unsigned i2 = __shfl_down_sync(0xffffffffu, idx, d, 8);
       if (m2 > m) {
         m = m2;
         idx = i2;
       }
     }
-    if (lane == 0 && cellx < cw && celly < ch) {
+    if (g == 0 && k >= 0 && cellx < cw && celly < ch) {
       const int cell = celly * cw + cellx;
       const int px = cellx * 8 + (int)(idx & 0xffffu), py = celly * 8 + (int)(idx >> 16);
       float out_m = 0.f;
@@ -691,7 +700,7 @@ cudaError_t launch_quota_bins_final(const SelectBatch& b, int bin_key_cap, int f
 cudaError_t launch_select_rest(const SelectBatch& b, int touched_words, int bin_key_cap, int final_key_cap,
                                cudaStream_t s) {
   if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
-  alive_kernel<<<b.ncams, 256, 0, s>>>(b);
+  alive_kernel<<<b.ncams, 1024, 0, s>>>(b);
   cells_kernel<<<(touched_words + 7) / 8, 256, 0, s>>>(b, touched_words);
   return launch_quota_bins_final(b, bin_key_cap, final_key_cap, s);
 }
@@ -699,7 +708,7 @@ cudaError_t launch_select_rest(const SelectBatch& b, int touched_words, int bin_
 cudaError_t launch_select(const SelectBatch& b, int total_tiles, int bin_key_cap, int final_key_cap,
                           cudaStream_t s) {
   if (bin_key_cap > kMaxSelectKeys || final_key_cap > kMaxSelectKeys) return cudaErrorInvalidValue;
-  alive_kernel<<<b.ncams, 256, 0, s>>>(b);
+  alive_kernel<<<b.ncams, 1024, 0, s>>>(b);
   tile_kernel<false><<<total_tiles, tile::kThreads, tile::kSmem, s>>>(b);
   return launch_quota_bins_final(b, bin_key_cap, final_key_cap, s);
 }
