@@ -47,26 +47,34 @@ def check_tile(sizes, X2, Y2):
         assert 0 <= row < S0H and 0 <= col < S0W, (row, col)
         assert 0 <= a0y + row < h0 and 0 <= a0x + col < w0, "read outside the frame"
 
-    # level 1: column strips of 14 rows, six bands
+    # level 1: column pairs (c, c + 1) over bands of 7 rows, 40 pairs x 12 bands; away from the edges
+    # both columns' taps are bytes 4 pp + 14 .. 4 pp + 20 of the three words at 4 pp + 12
     done1 = np.zeros((S1, S1S), bool)
-    for tid in range(S1 * 6):
-        c, band = tid % S1, tid // S1
+    for tid in range(40 * 12):
+        pp, band = tid % 40, tid // 40
+        c = 2 * pp
         x1 = a1x + c
-        ys, ye = max(a1y + band * 14, 0), min(a1y + min(band * 14 + 14, S1), h1)
-        if not (0 <= x1 < w1 and ys < ye):
+        ys, ye = max(a1y + band * 7, 0), min(a1y + min(band * 7 + 7, S1), h1)
+        if ys >= ye:
             continue
-        cols = [mirror(2 * x1 - 2 + l, w0) - a0x for l in range(5)]
-        contiguous = 2 * x1 - 2 >= 0 and 2 * x1 + 2 < w0
-        rows = [mirror(r, h0) - a0y for r in range(2 * ys - 2, 2 * (ye - 1) + 3)]
-        for r in rows:
-            if contiguous:
-                wofs = cols[0] & ~3
-                assert wofs >= 0 and wofs + 8 <= S0W  # the two aligned words
-                assert cols == list(range(cols[0], cols[0] + 5))
-            for cc in cols:
-                b0(r, cc)
-        for y in range(ys, ye):
-            done1[y - a1y, c] = True
+        if 2 * x1 - 2 >= 0 and 2 * x1 + 4 < w0 and c + 1 < S1 and 2 * ys - 2 >= 0 and 2 * ye < h0:
+            assert 4 * pp + 12 + 12 <= S0W  # the three words of a row
+            for r in range(2 * ys - 2, 2 * ye + 1):
+                for col in range(4 * pp + 14, 4 * pp + 21):
+                    b0(r - a0y, col)
+            for y in range(ys, ye):
+                done1[y - a1y, c] = done1[y - a1y, c + 1] = True
+            continue
+        for k in range(2):
+            cc, xx = c + k, x1 + k
+            if cc >= S1 or not (0 <= xx < w1):
+                continue
+            cols = [mirror(2 * xx - 2 + l, w0) - a0x for l in range(5)]
+            for r in range(2 * ys - 2, 2 * (ye - 1) + 3):
+                for col in cols:
+                    b0(mirror(r, h0) - a0y, col)
+            for y in range(ys, ye):
+                done1[y - a1y, cc] = True
     for tid in range(4):  # corners redone with the 25-tap rule
         x1, y1 = (w1 - 1 if tid & 1 else 0), (h1 - 1 if tid & 2 else 0)
         if a1x <= x1 < a1x + S1 and a1y <= y1 < a1y + S1:
@@ -78,22 +86,38 @@ def check_tile(sizes, X2, Y2):
                     b0(mirror(yc, h0) - a0y, mirror(xc, w0) - a0x)
             done1[y1 - a1y, x1 - a1x] = True
 
-    # level 2: column strips of 3 rows, 13 bands
+    # level 2: column pairs over bands of 3 rows, 19 pairs x 13 bands; away from the edges both
+    # columns' taps are the level-1 values 4 pp .. 4 pp + 6 of a row (two 16-byte loads)
     done2 = np.zeros((S2, S2S), bool)
-    for tid in range(S2 * 13):
-        c, band = tid % S2, tid // S2
+    for tid in range(19 * 13):
+        pp, band = tid % 19, tid // 19
+        c = 2 * pp
         x2 = X2 - 3 + c
         ys, ye = max(a2y + band * 3, 0), min(a2y + min(band * 3 + 3, S2), h2)
-        if not (0 <= x2 < w2 and ys < ye):
+        if ys >= ye:
             continue
-        cols = [mirror(2 * x2 - 2 + l, w1) - a1x for l in range(5)]
-        for r in range(2 * ys - 2, 2 * (ye - 1) + 3):
-            rr = mirror(r, h1) - a1y
-            for cc in cols:
-                assert 0 <= rr < S1 and 0 <= cc < S1S and done1[rr, cc], (rr, cc)
-        for y in range(ys, ye):
-            assert 0 <= x2 - a2x < S2S
-            done2[y - a2y, x2 - a2x] = True
+        if 2 * x2 - 2 >= 0 and 2 * x2 + 4 < w1 and 2 * ys - 2 >= 0 and 2 * ye < h1:
+            assert 4 * pp + 8 <= S1S  # the two 16-byte loads of a row
+            for r in range(2 * ys - 2, 2 * ye + 1):
+                rr = r - a1y
+                for cc in range(4 * pp, 4 * pp + 7):
+                    assert 0 <= rr < S1 and done1[rr, cc], (rr, cc)
+            for y in range(ys, ye):
+                assert x2 + 1 - a2x < S2S
+                done2[y - a2y, x2 - a2x] = done2[y - a2y, x2 + 1 - a2x] = True
+            continue
+        for k in range(2):
+            xx = x2 + k
+            if not (0 <= xx < w2):
+                continue
+            cols = [mirror(2 * xx - 2 + l, w1) - a1x for l in range(5)]
+            for r in range(2 * ys - 2, 2 * (ye - 1) + 3):
+                rr = mirror(r, h1) - a1y
+                for cc in cols:
+                    assert 0 <= rr < S1 and 0 <= cc < S1S and done1[rr, cc], (rr, cc)
+            for y in range(ys, ye):
+                assert 0 <= xx - a2x < S2S
+                done2[y - a2y, xx - a2x] = True
 
     def l2_taps(x, y, sw, sh, ax, ay, done, rows, stride):  # downscale_px on a region
         x0, y0 = 2 * x - 2, 2 * y - 2
@@ -119,23 +143,38 @@ def check_tile(sizes, X2, Y2):
             if x3 < w3 and y3 < h3:
                 l2_taps(x3, y3, w2, h2, a2x, a2y, done2, S2, S2S)
 
-    # level-0 outputs: four pixels per item
+    # level-0 outputs.  (a) image and grad_y: a pixel pair's column over a strip of 16 rows, 64
+    # pairs x 8 strips, its 7-row window sliding down (rows y0 - 3 .. y0 + 18 loaded)
+    for tid in range(512):
+        pc, strip = tid & 63, tid >> 6
+        x, y0 = 4 * X2 + 2 * pc, 4 * Y2 + 16 * strip
+        if x >= w0 or y0 >= h0:
+            continue
+        c = x - a0x
+        assert 0 <= c and c + 1 < S0W
+        for k in range(22):
+            assert 0 <= y0 - a0y - 3 + k < S0H  # every 2-byte load
+        two = x + 1 < w0
+        for i in range(16):
+            y = y0 + i
+            if y >= h0:
+                continue
+            for px in ((0, 1) if two else (0,)):
+                b0(y - a0y, c + px)  # the image value
+                if 2 < y < h0 - 3:
+                    for j in range(-3, 4):
+                        b0(y - a0y + j, c + px)
+    # (b) grad_x: four pixels of a row per item from the words at x - 4, x, x + 4
     for q in range(128 * 32):
         y, x = 4 * Y2 + (q >> 5), 4 * X2 + (q & 31) * 4
         if y >= h0 or x >= w0:
             continue
         r, c = y - a0y, x - a0x
-        assert 3 <= r and r + 3 < S0H and c >= 4 and c + 8 <= S0W  # every word read
+        assert 0 <= r < S0H and c >= 4 and c + 8 <= S0W  # every word read
         for i in range(4):
-            if x + i >= w0:
-                continue
-            b0(r, c + i)  # the image value
-            if 2 < x + i < w0 - 3:
+            if x + i < w0 and 2 < x + i < w0 - 3:
                 for j in range(-3, 4):
                     b0(r, c + i + j)
-            if 2 < y < h0 - 3:
-                for j in range(-3, 4):
-                    b0(r + j, c + i)
 
     # level-1 and level-2 outputs: four pixels per item
     for q in range(64 * 16 + 32 * 8):
