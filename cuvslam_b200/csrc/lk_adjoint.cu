@@ -140,7 +140,7 @@ struct Templ {
   float sp, gxx, gxy, gyy, det_rcp;
   int bx, by;  // the patch's 12x12 texel window
   int ax;      // its staged window's first column (bx rounded down to a multiple of 4)
-  TapSet ts;
+  float sx, sy;  // the template position (its tap set is recomputed where needed, not kept live)
 };
 
 // The current-image window for a patch at c, staged from the 16-byte aligned column at or below
@@ -179,13 +179,15 @@ __device__ void make_template(const Level& PL, float sx, float sy, const bool (&
   if (CL) stage_cur(*CL, c.x, c.y, *wbx, *wby, sm, lane);
   cp_async_wait_all();
   __syncwarp();
-  T.ts = make_taps<FE_SAMPLE_EXACT>(xmin, ymin, T.ax, T.by, kPAS, lane);
+  T.sx = sx;
+  T.sy = sy;
+  const TapSet ts = make_taps<FE_SAMPLE_EXACT>(xmin, ymin, T.ax, T.by, kPAS, lane);
   float gxp[kNE], gyp[kNE];
   float sgx = 0.f, sgy = 0.f, sp = 0.f;
 #pragma unroll
   for (int e = 0; e < kNE; ++e) {
     gxp[e] = gyp[e] = T.p1[e] = 0.f;
-    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.ax, T.by, kPAS);
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(ts, ix[e], iy[e], T.ax, T.by, kPAS);
     if (valid[e]) {
       gxp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gx, kPAS, t);
       gyp[e] = sample<FE_SAMPLE_EXACT>(sm.win.gy, kPAS, t);
@@ -223,10 +225,11 @@ __device__ void finish_template(const AdjLaunch& p, int g, int level, int W, int
                                 const bool (&valid)[kNE], const int (&ix)[kNE], const int (&iy)[kNE], AdjSmem& sm,
                                 int lane, float& dsx, float& dsy) {
   // dL/ds from the staged windows
+  const TapSet ts = make_taps<FE_SAMPLE_EXACT>(__fadd_rn(T.sx, -4.f), __fadd_rn(T.sy, -4.f), T.ax, T.by, kPAS, lane);
   float sx = 0.f, sy = 0.f;
 #pragma unroll
   for (int e = 0; e < kNE; ++e) {
-    const Tap t = tap_of<FE_SAMPLE_EXACT>(T.ts, ix[e], iy[e], T.ax, T.by, kPAS);
+    const Tap t = tap_of<FE_SAMPLE_EXACT>(ts, ix[e], iy[e], T.ax, T.by, kPAS);
     if (valid[e]) {
       float v, dx, dy;
       sample_vg(sm.win.img, kPAS, t, v, dx, dy);
@@ -247,7 +250,7 @@ __device__ void finish_template(const AdjLaunch& p, int g, int level, int W, int
   zero_smem(&sm.prec[0][0], 3 * kRP * kRP, lane);
   float* const dst[3] = {sm.prec[0], sm.prec[1], sm.prec[2]};
   const float c[3][kNE] = {{p1b[0], p1b[1], p1b[2]}, {gxb[0], gxb[1], gxb[2]}, {gyb[0], gyb[1], gyb[2]}};
-  scatter_taps<3>(dst, kRP, rx0, ry0, T.ts, c, valid, ix, iy, W, H, sm, lane);
+  scatter_taps<3>(dst, kRP, rx0, ry0, ts, c, valid, ix, iy, W, H, sm, lane);
   const int rw = min(kRP, W - rx0), rh = min(kRP, H - ry0);
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
@@ -600,7 +603,7 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kAdjWarps * 32, 4) adjoint_kernel(const __grid_constant__ AdjLaunch p) {
+__global__ void __launch_bounds__(kAdjWarps * 32, MODE == kLkImplicit ? 5 : 4) adjoint_kernel(const __grid_constant__ AdjLaunch p) {
   __shared__ AdjSmem smem[kAdjWarps];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (;;) {
