@@ -159,14 +159,14 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           if (lane == 0) td.track_status = 0;
           return;
         }
-        det_rcp = __fdiv_rn(1.f, gxx);
+        det_rcp = __frcp_rn(gxx);  // correctly rounded: equals __fdiv_rn(1.f, gxx)
       } else {
         const float det = __fmaf_rn(gxx, gyy, -__fmul_rn(gxy, gxy));
         if (det < 1.1920928955078125e-07f) {
           if (lane == 0) td.track_status = 0;
           return;
         }
-        det_rcp = __fdiv_rn(1.f, det);
+        det_rcp = __frcp_rn(det);  // correctly rounded: equals __fdiv_rn(1.f, det)
       }
       if (MODE == kModeUnrolled && rec && lane == 0) rec->flags[level] = 1;
       const float savex = cx, savey = cy;
@@ -251,7 +251,8 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
         rec->K[level] = steps;
       }
       if (conv) {
-        const float r = __fdiv_rn(radius, (float)(1 << level));
+        // radius / 2^level, exact as a product with 2^-level (no subnormal for a pixel radius)
+        const float r = __fmul_rn(radius, __int_as_float((127 - level) << 23));
         const float dx = __fsub_rn(cx, savex), dy = __fsub_rn(cy, savey);
         if (__fmaf_rn(dx, dx, __fmul_rn(dy, dy)) > __fmul_rn(r, r)) conv = false;
       }
