@@ -73,6 +73,37 @@ __device__ __forceinline__ float warp_sum(float x) {
   return x;
 }
 
+// Two warp sums at once, each bit-identical to warp_sum of its argument (the same pairs added at
+// every stage): after the first stage a lane keeps one of the two partial sums (lanes with bit 0
+// clear keep a's), so the later stages move one value instead of two; the totals are read from
+// lanes 0 and 1.
+__device__ __forceinline__ void warp_sum2(float& a, float& b, int lane) {
+  const bool odd = (lane & 1) != 0;
+  float keep = odd ? b : a;
+  keep += __shfl_xor_sync(0xffffffffu, odd ? a : b, 1);
+#pragma unroll
+  for (int m = 2; m < 32; m <<= 1) keep += __shfl_xor_sync(0xffffffffu, keep, m);
+  a = __shfl_sync(0xffffffffu, keep, 0);
+  b = __shfl_sync(0xffffffffu, keep, 1);
+}
+
+// Three warp sums at once, each bit-identical to warp_sum of its argument: after stage 1 even lanes
+// keep a's and b's partial sums and odd lanes c's, after stage 2 each lane keeps one (a on lanes with
+// bits 0 and 1 clear, b with bit 1 set, c on odd lanes); the totals are read from lanes 0, 2 and 1.
+__device__ __forceinline__ void warp_sum3(float& a, float& b, float& c, int lane) {
+  const bool odd = (lane & 1) != 0, hi = (lane & 2) != 0;
+  const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a : c, 1);  // even lanes: a; odd lanes: c
+  const float r2 = __shfl_xor_sync(0xffffffffu, b, 1);            // even lanes: b
+  const float ka = a + r1, kb = b + r2, kc = c + r1;
+  float keep = odd ? kc : (hi ? kb : ka);
+  keep += __shfl_xor_sync(0xffffffffu, odd ? kc : (hi ? ka : kb), 2);
+#pragma unroll
+  for (int m = 4; m < 32; m <<= 1) keep += __shfl_xor_sync(0xffffffffu, keep, m);
+  a = __shfl_sync(0xffffffffu, keep, 0);
+  b = __shfl_sync(0xffffffffu, keep, 2);
+  c = __shfl_sync(0xffffffffu, keep, 1);
+}
+
 // Asynchronous global->shared copies (cp.async, sm_80+); both addresses aligned to the copy size.
 // A thread sees its own copies after cp_async_wait_all(); other threads after a barrier
 // (__syncwarp / __syncthreads) that follows the wait.

@@ -197,9 +197,8 @@ __device__ void make_template(const Level& PL, float sx, float sy, const bool (&
       sp = __fadd_rn(sp, T.p1[e]);
     }
   }
-  sgx = warp_sum(sgx);
-  sgy = warp_sum(sgy);
-  T.sp = warp_sum(sp);
+  warp_sum3(sgx, sgy, sp, lane);
+  T.sp = sp;
   float lxx = 1.f / 32.f, lxy = 0.f, lyy = 1.f / 32.f;
 #pragma unroll
   for (int e = 0; e < kNE; ++e) {
@@ -212,9 +211,10 @@ __device__ void make_template(const Level& PL, float sx, float sy, const bool (&
       lyy = __fmaf_rn(__fmul_rn(T.b[e], T.b[e]), wt[e], lyy);
     }
   }
-  T.gxx = warp_sum(lxx);
-  T.gxy = warp_sum(lxy);
-  T.gyy = warp_sum(lyy);
+  warp_sum3(lxx, lxy, lyy, lane);
+  T.gxx = lxx;
+  T.gxy = lxy;
+  T.gyy = lyy;
   T.det_rcp = __fdiv_rn(1.f, __fmaf_rn(T.gxx, T.gyy, -__fmul_rn(T.gxy, T.gxy)));
 }
 
@@ -243,8 +243,9 @@ __device__ void finish_template(const AdjLaunch& p, int g, int level, int W, int
       sy = __fmaf_rn(gyb[e], dy, sy);
     }
   }
-  dsx = warp_sum(sx);
-  dsy = warp_sum(sy);
+  warp_sum2(sx, sy, lane);
+  dsx = sx;
+  dsy = sy;
   // records
   const int rx0 = max(T.bx, 0), ry0 = max(T.by, 0);
   zero_smem(&sm.prec[0][0], 3 * kRP * kRP, lane);
@@ -345,8 +346,8 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
         sdy = __fadd_rn(sdy, dy[e]);
       }
     }
-    sc = warp_sum(sc);
-    const float mdx = __fmul_rn(warp_sum(sdx), rcp81), mdy = __fmul_rn(warp_sum(sdy), rcp81);
+    warp_sum3(sc, sdx, sdy, lane);
+    const float mdx = __fmul_rn(sdx, rcp81), mdy = __fmul_rn(sdy, rcp81);
     const float delta = __fmul_rn(__fsub_rn(sc, T.sp), rcp81);
     float r[kNE], j00 = 0.f, j01 = 0.f, j10 = 0.f, j11 = 0.f;
 #pragma unroll
@@ -362,10 +363,8 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
         j11 = __fmaf_rn(wb, ddy, j11);
       }
     }
-    j00 = warp_sum(j00);
-    j01 = warp_sum(j01);
-    j10 = warp_sum(j10);
-    j11 = warp_sum(j11);
+    warp_sum2(j00, j01, lane);
+    warp_sum2(j10, j11, lane);
     const float detj = __fmaf_rn(j00, j11, -__fmul_rn(j01, j10));
     if (!(fabsf(detj) > 0.f) || !isfinite(detj)) return drop(0.f);
     // J^T lambda = dL/dc*
@@ -386,8 +385,9 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
         sb = __fadd_rn(sb, bb[e]);
       }
     }
-    const float mu = __fmul_rn(warp_sum(su), rcp81);
-    const float ma = __fmul_rn(warp_sum(sa), rcp81), mb = __fmul_rn(warp_sum(sb), rcp81);
+    warp_sum3(su, sa, sb, lane);
+    const float mu = __fmul_rn(su, rcp81);
+    const float ma = __fmul_rn(sa, rcp81), mb = __fmul_rn(sb, rcp81);
     float p2b[kNE], p1b[kNE], gxb[kNE], gyb[kNE];
 #pragma unroll
     for (int e = 0; e < kNE; ++e) {
@@ -555,8 +555,9 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
           const float c1[1][kNE] = {{p2b[0], p2b[1], p2b[2]}};
           scatter_taps<1>(dst, rs, rx0, ry0, tc, c1, valid, ix, iy, W, H, sm, lane);
         }
-        cbx = __fadd_rn(cbx, warp_sum(gx));
-        cby = __fadd_rn(cby, warp_sum(gy));
+        warp_sum2(gx, gy, lane);
+        cbx = __fadd_rn(cbx, gx);
+        cby = __fadd_rn(cby, gy);
       }
       if (pending) flush();
       const float hs = __fadd_rn(hxy, hyx);
@@ -570,7 +571,8 @@ __device__ void adjoint_one(const AdjLaunch& p, const AdjCam& cam, int g, AdjSme
           sb = __fadd_rn(sb, bb[e]);
         }
       }
-      const float ma = __fmul_rn(warp_sum(sa), rcp81), mb = __fmul_rn(warp_sum(sb), rcp81);
+      warp_sum2(sa, sb, lane);
+      const float ma = __fmul_rn(sa, rcp81), mb = __fmul_rn(sb, rcp81);
       float gxb[kNE], gyb[kNE];
 #pragma unroll
       for (int e = 0; e < kNE; ++e) {

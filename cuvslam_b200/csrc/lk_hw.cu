@@ -98,9 +98,8 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
           sp = (sp + p1[e]);
         }
       }
-      sgx = warp_sum(sgx);
-      if (!HORIZ) sgy = warp_sum(sgy);
-      sp = warp_sum(sp);
+      if (HORIZ) warp_sum2(sgx, sp, lane);
+      else warp_sum3(sgx, sgy, sp, lane);
       float lxx = 1.f / 32.f, lxy = 0.f, lyy = 1.f / 32.f;
 #pragma unroll
       for (int e = 0; e < kTE; ++e) {
@@ -118,9 +117,11 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
           }
         }
       }
-      const float gxx = warp_sum(lxx);
-      const float gxy = HORIZ ? 0.f : warp_sum(lxy);
-      const float gyy = HORIZ ? 0.f : warp_sum(lyy);
+      if (HORIZ) lxx = warp_sum(lxx);
+      else warp_sum3(lxx, lxy, lyy, lane);
+      const float gxx = lxx;
+      const float gxy = HORIZ ? 0.f : lxy;
+      const float gyy = HORIZ ? 0.f : lyy;
       float det_rcp;
       if (HORIZ) {
         if (gxx < 1.1920928955078125e-07f) {
@@ -160,13 +161,13 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
             if (!HORIZ) ey = (wd * gyp[e] + ey);
           }
         }
-        ex = warp_sum(ex);
         float vx, vy;
         if (HORIZ) {
+          ex = warp_sum(ex);
           vx = (ex * det_rcp);
           vy = 0.f;
         } else {
-          ey = warp_sum(ey);
+          warp_sum2(ex, ey, lane);
           vx = (gyy * ex - gxy * ey) * det_rcp;
           vy = (gxx * ey - gxy * ex) * det_rcp;
         }
@@ -192,11 +193,8 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
             s12 = (p2[e] * p1[e] + s12);
           }
         }
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        s11 = warp_sum(s11);
-        s22 = warp_sum(s22);
-        s12 = warp_sum(s12);
+        warp_sum3(s1, s2, s11, lane);
+        warp_sum2(s22, s12, lane);
         const float a1 = (s1 * rcp25), a2 = (s2 * rcp25);
         const float d1 = s11 * rcp25 - a1 * a1;
         const float d2 = s22 * rcp25 - a2 * a2;

@@ -130,9 +130,8 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           sp = __fadd_rn(sp, p1[e]);
         }
       }
-      sgx = warp_sum(sgx);
-      if (!HORIZ) sgy = warp_sum(sgy);
-      sp = warp_sum(sp);
+      if (HORIZ) warp_sum2(sgx, sp, lane);
+      else warp_sum3(sgx, sgy, sp, lane);
       float lxx = 1.f / 32.f, lxy = 0.f, lyy = 1.f / 32.f;
 #pragma unroll
       for (int e = 0; e < kNE; ++e) {
@@ -150,9 +149,11 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
           }
         }
       }
-      const float gxx = warp_sum(lxx);
-      const float gxy = HORIZ ? 0.f : warp_sum(lxy);
-      const float gyy = HORIZ ? 0.f : warp_sum(lyy);
+      if (HORIZ) lxx = warp_sum(lxx);
+      else warp_sum3(lxx, lxy, lyy, lane);
+      const float gxx = lxx;
+      const float gxy = HORIZ ? 0.f : lxy;
+      const float gyy = HORIZ ? 0.f : lyy;
       float det_rcp;
       if (HORIZ) {
         if (gxx < 1.1920928955078125e-07f) {
@@ -214,12 +215,12 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
             if (!HORIZ) ey = __fmaf_rn(wd, gyp[e], ey);
           }
         }
-        ex = warp_sum(ex);
         if (HORIZ) {
+          ex = warp_sum(ex);
           vx = __fmul_rn(ex, det_rcp);
           vy = 0.f;
         } else {
-          ey = warp_sum(ey);
+          warp_sum2(ex, ey, lane);
           vx = __fmul_rn(__fmaf_rn(gyy, ex, -__fmul_rn(gxy, ey)), det_rcp);
           vy = __fmul_rn(__fmaf_rn(gxx, ey, -__fmul_rn(gxy, ex)), det_rcp);
         }
@@ -269,11 +270,8 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
             s12 = __fmaf_rn(p2[e], p1[e], s12);
           }
         }
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        s11 = warp_sum(s11);
-        s22 = warp_sum(s22);
-        s12 = warp_sum(s12);
+        warp_sum3(s1, s2, s11, lane);
+        warp_sum2(s22, s12, lane);
         const float a1 = __fmul_rn(s1, rcp25), a2 = __fmul_rn(s2, rcp25);
         const float d1 = __fmaf_rn(s11, rcp25, -__fmul_rn(a1, a1));
         const float d2 = __fmaf_rn(s22, rcp25, -__fmul_rn(a2, a2));
@@ -320,8 +318,8 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
               sdy = __fadd_rn(sdy, dys[e]);
             }
           }
-          sc = warp_sum(sc);
-          const float mdx = __fmul_rn(warp_sum(sdx), rcp81), mdy = __fmul_rn(warp_sum(sdy), rcp81);
+          warp_sum3(sc, sdx, sdy, lane);
+          const float mdx = __fmul_rn(sdx, rcp81), mdy = __fmul_rn(sdy, rcp81);
           const float delta = __fmul_rn(__fsub_rn(sc, sp), rcp81);
           float ex = 0.f, ey = 0.f, j00 = 0.f, j01 = 0.f, j10 = 0.f, j11 = 0.f;
 #pragma unroll
@@ -338,12 +336,8 @@ __device__ void track_one(const LkCam& cam, fe_track_data& td, WarpSmem& sm, int
               j11 = __fmaf_rn(wb, ddy, j11);
             }
           }
-          ex = warp_sum(ex);
-          ey = warp_sum(ey);
-          j00 = warp_sum(j00);
-          j01 = warp_sum(j01);
-          j10 = warp_sum(j10);
-          j11 = warp_sum(j11);
+          warp_sum3(ex, ey, j00, lane);
+          warp_sum3(j01, j10, j11, lane);
           const float detj = __fmaf_rn(j00, j11, -__fmul_rn(j01, j10));
           if (!(fabsf(detj) > 0.f)) break;
           // c -= J^-1 e
