@@ -1460,7 +1460,7 @@ int fe_batch_run_part(fe_batch* b, int part, fe_stream stream) {
 }
 
 int fe_batch_lk_work(fe_batch* b, uint64_t* device_counts, fe_stream stream) {
-  if (!b || !device_counts || b->sampling == FE_SAMPLE_HARDWARE) return FE_ERR_INVALID_ARGUMENT;
+  if (!b || !device_counts) return FE_ERR_INVALID_ARGUMENT;
   if (b->lk.total <= 0) return FE_OK;
   fe::LkLaunch counted = b->lk;
   counted.counts = reinterpret_cast<unsigned long long*>(device_counts);

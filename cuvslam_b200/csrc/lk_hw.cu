@@ -23,8 +23,11 @@ constexpr int kTE = 3;  // taps per lane: ceil(81 / 32)
 
 __device__ __forceinline__ float tex(cudaTextureObject_t t, float x, float y) { return tex2D<float>(t, x, y); }
 
-template <bool HORIZ>
-__device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, float ncc_thr, int lane) {
+// COUNT: `cnt` counts the work done, as lk_track.cuh's: [0] levels set up, [1] Gauss-Newton steps,
+// [2] NCC evaluations (a separate instantiation, so that the timed kernel carries no counting code).
+template <bool HORIZ, bool COUNT>
+__device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, float ncc_thr, int lane,
+                         unsigned long long* cnt) {
   const float radius = td.search_radius_px;
   if (radius < 0.f) {
     __syncwarp();
@@ -71,6 +74,7 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
     float xmin = (sx + -4.f), ymin = (sy + -4.f);
     bool good = xmin >= 0.f && (sx + 5.f) < (float)W && ymin >= 0.f && (sy + 5.f) < (float)H;
     if (good) {
+      if (COUNT && lane == 0) atomicAdd(cnt, 1ull);
       const cudaTextureObject_t t_gx = (cudaTextureObject_t)T.prev_gx[level];
       const cudaTextureObject_t t_gy = HORIZ ? 0 : (cudaTextureObject_t)T.prev_gy[level];
       const cudaTextureObject_t t_p1 = (cudaTextureObject_t)T.prev_img[level];
@@ -142,6 +146,7 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
         xmin = (cx + -4.f);
         ymin = (cy + -4.f);
         if (!(xmin >= 0.f && (cx + 5.f) < (float)W && ymin >= 0.f && (cy + 5.f) < (float)H)) break;
+        if (COUNT && lane == 0) atomicAdd(cnt + 1, 1ull);
         float sc = 0.f;
 #pragma unroll
         for (int e = 0; e < kTE; ++e) {
@@ -182,6 +187,7 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
         if ((dx * dx +  (dy * dy)) > (r * r)) conv = false;
       }
       if (conv) {
+        if (COUNT && lane == 0) atomicAdd(cnt + 2, 1ull);
         float s1 = 0.f, s2 = 0.f, s11 = 0.f, s22 = 0.f, s12 = 0.f;
 #pragma unroll
         for (int e = 0; e < kTE; ++e) {
@@ -226,7 +232,7 @@ __device__ void track_hw(const LkCam& cam, const LkTex& T, fe_track_data& td, fl
   }
 }
 
-template <bool HORIZ>
+template <bool HORIZ, bool COUNT>
 __global__ void __launch_bounds__(32) lk_hw_kernel(const __grid_constant__ LkLaunch p) {
   const int lane = threadIdx.x;
   const int g = blockIdx.x;
@@ -246,12 +252,13 @@ __global__ void __launch_bounds__(32) lk_hw_kernel(const __grid_constant__ LkLau
       reinterpret_cast<uint32_t*>(&td)[lane] = reinterpret_cast<const uint32_t*>(&cam.tracks_in[g - cam.begin])[lane];
     __syncwarp();
   }
-  track_hw<HORIZ>(cam, T, td, td.ncc_threshold, lane);
+  track_hw<HORIZ, COUNT>(cam, T, td, td.ncc_threshold, lane, p.counts);
   if (cam.retrack_ncc > 0.f) {
     // MonoSOFGPU's retrack pass (as lk.cu): a track the first pass lost runs again from the same
     // inputs with the retrack NCC threshold
     __syncwarp();
-    if (td.track_status == 0 && td.search_radius_px >= 0.f) track_hw<HORIZ>(cam, T, td, cam.retrack_ncc, lane);
+    if (td.track_status == 0 && td.search_radius_px >= 0.f)
+      track_hw<HORIZ, COUNT>(cam, T, td, cam.retrack_ncc, lane, p.counts);
   }
 }
 
@@ -260,10 +267,16 @@ __global__ void __launch_bounds__(32) lk_hw_kernel(const __grid_constant__ LkLau
 cudaError_t launch_lk_hw(const LkLaunch& p, cudaStream_t s) {
   if (p.total <= 0) return cudaSuccess;
   if (!p.texs && p.cams) return cudaErrorInvalidValue;
-  if (p.horizontal)
-    lk_hw_kernel<true><<<p.total, 32, 0, s>>>(p);
-  else
-    lk_hw_kernel<false><<<p.total, 32, 0, s>>>(p);
+  if (p.counts) {
+    if (p.horizontal)
+      lk_hw_kernel<true, true><<<p.total, 32, 0, s>>>(p);
+    else
+      lk_hw_kernel<false, true><<<p.total, 32, 0, s>>>(p);
+  } else if (p.horizontal) {
+    lk_hw_kernel<true, false><<<p.total, 32, 0, s>>>(p);
+  } else {
+    lk_hw_kernel<false, false><<<p.total, 32, 0, s>>>(p);
+  }
   return cudaGetLastError();
 }
 

@@ -420,8 +420,7 @@ FE_API int fe_batch_run_part(fe_batch* batch, int part, fe_stream stream);
  * per-track counting on, and adds to device_counts[0..2] (device memory, zeroed by the caller) the
  * number of pyramid levels at which a track was set up (previous patch and gradients sampled,
  * Hessian formed), of Gauss-Newton steps (current patch sampled, update solved) and of NCC
- * evaluations, over all tracks and both passes.  Timed steps never count.  Not for
- * FE_SAMPLE_HARDWARE batches (FE_ERR_INVALID_ARGUMENT). */
+ * evaluations, over all tracks and both passes.  Timed steps never count.  Every sampling mode. */
 FE_API int fe_batch_lk_work(fe_batch* batch, uint64_t* device_counts, fe_stream stream);
 /* Number of kernel launches in one fe_batch_run (kernel nodes of the captured graph); -1 for a
  * NULL batch. */

@@ -144,12 +144,14 @@ def test_autotuned_batch_gives_the_same_results(ctx):
                         np.testing.assert_array_equal(x, y)
 
 
-def test_lk_work_counters(ctx):
+@pytest.mark.parametrize("sampling", ["texture", "hardware"])
+def test_lk_work_counters(ctx, sampling):
     """The kernel's work counters (fe_batch_lk_work) change no result, repeat exactly from the same
     inputs, and bound the work: every kept track was set up, stepped and NCC-checked at least at level
-    0, and no level takes more than the 11 steps of the reference rule."""
+    0, and no level takes more than the 11 steps of the reference rule.  Both LK kernels (the
+    texture-weight emulation and the texture unit) count."""
     frames, prevs, host = _setup(ctx, SHAPES[:3], seed=3)
-    b = Batch(ctx, frames)
+    b = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE if sampling == "texture" else _lib.FE_SAMPLE_HARDWARE)
 
     def restore():
         for f, t in zip(frames, host):
