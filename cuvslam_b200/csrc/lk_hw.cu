@@ -4,12 +4,13 @@
 // the coordinates xmin + i, ymin + j).
 //
 // One warp per track (a one-warp block per track, so that a long track holds no other warp), tap
-// f = lane + 32 e (e < 3) as in lk.cu, window sums as lane partial sums then the xor butterfly: the
-// same order as the emulated modes.  The arithmetic is written plainly, as the reference writes it,
-// and left to the compiler to contract into fused multiply-adds as the reference's build does, with
-// the reference's fast reciprocal of the determinant (this mode is compared with tolerances, not bit
-// for bit).  A level's texture handles are read once into
-// registers before its samples.
+// f = lane + 32 e (e < 3) as in lk.cu, window sums as lane partial sums then the xor butterfly over
+// masks 1, 2, 4, 8, 16, which pairs lanes as the reference's warp reduction does.  The arithmetic is
+// written plainly, as the reference writes it, and left to the compiler to contract into fused
+// multiply-adds as the reference's build does, with the reference's fast reciprocal of the
+// determinant: the records equal lk_track_kernel's bit for bit (the emulated modes cannot, their
+// samples differ from the texture unit's in the last bits).  A level's texture handles are read once
+// into registers before its samples.
 #include <cuda_runtime.h>
 
 #include "fe_common.cuh"

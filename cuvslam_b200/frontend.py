@@ -19,6 +19,12 @@ from . import _lib
 from .types import TRACK_DTYPE
 
 
+# LK's default sampling: the texture unit's own linear filtering, as the reference samples its
+# pyramid planes (lk_tracker.cu's tex2D reads).  FE_SAMPLE_TEXTURE restates that filtering in FP32
+# and equals the oracle bit for bit; FE_SAMPLE_HARDWARE is the faster kernel.
+DEFAULT_LK_SAMPLING = _lib.FE_SAMPLE_HARDWARE
+
+
 def _stream_handle(stream=None):
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
@@ -145,7 +151,7 @@ class ImagePyramid:
                 for l in range(self.levels)]
 
 
-def track_mono(ctx, prev, cur, tracks, retrack_ncc=0.85, sampling=_lib.FE_SAMPLE_TEXTURE, stream=None):
+def track_mono(ctx, prev, cur, tracks, retrack_ncc=0.85, sampling=DEFAULT_LK_SAMPLING, stream=None):
     """MonoSOFGPU::launch's track + retrack passes as collect merges them (fe_track_mono;
     sof_mono_gpu.cpp:34-104)."""
     _lib.check(ctx.lib.fe_track_mono(ctx.handle, ctypes.byref(prev.desc), ctypes.byref(cur.desc), _ptr(tracks),
@@ -168,7 +174,7 @@ class LKFeatureTracker:
     """GPULKFeatureTracker (horizontal=False) / GPULKTrackerHorizontal (horizontal=True):
     track_points of cuda_modules/lk_tracker.cpp:24-73 (kernels lk_tracker.cu:69-379, 381-665)."""
 
-    def __init__(self, ctx, horizontal=False, sampling=_lib.FE_SAMPLE_TEXTURE):
+    def __init__(self, ctx, horizontal=False, sampling=DEFAULT_LK_SAMPLING):
         self.ctx = ctx
         self.horizontal = bool(horizontal)
         self.sampling = sampling
@@ -370,7 +376,7 @@ class Batch:
     """Batched multi-camera frame step captured in a CUDA graph (fe_batch_*); no counterpart in the
     reference (sof_multicamera_base.cpp:62-116 loops over the cameras)."""
 
-    def __init__(self, ctx, frames, sampling=_lib.FE_SAMPLE_TEXTURE):
+    def __init__(self, ctx, frames, sampling=DEFAULT_LK_SAMPLING):
         self.ctx = ctx
         self.frames = list(frames)
         arr = (_lib.FeCameraFrame * len(self.frames))()

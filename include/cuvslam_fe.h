@@ -95,9 +95,10 @@ typedef enum {
                                  pitch alignment (32 bytes), as fe_pyramid_init lays them out in
                                  512-byte aligned memory.  The context keeps a texture object per
                                  plane it tracked on until fe_destroy, at most 4096 (then
-                                 FE_ERR_CAPACITY): reuse pyramids.  Not bit-identical to an
-                                 emulation: within 0.01 px of the wide mode's results on the test
-                                 frames */
+                                 FE_ERR_CAPACITY): reuse pyramids.  Equals the reference's
+                                 lk_track_kernel bit for bit on the test frames (the same samples,
+                                 arithmetic and summation order); not bit-identical to the
+                                 emulations above.  The host wrappers' default */
 } fe_sampling;
 
 /* ---------------------------------------------------------------------------------------- */

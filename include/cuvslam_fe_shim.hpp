@@ -409,9 +409,10 @@ class GPUSelection {
 /* GPULKFeatureTracker (lk_tracker.h:27-37): pyramidal LK of TrackData records in device memory. */
 class GPULKFeatureTracker {
  public:
-  /* sampling: FE_SAMPLE_TEXTURE (the texture unit's filtering restated exactly, the default) or
-   * another fe_sampling mode. */
-  explicit GPULKFeatureTracker(int sampling = FE_SAMPLE_TEXTURE) : sampling_(sampling) {}
+  /* sampling: FE_SAMPLE_HARDWARE (the default: the texture unit's own filtering on texture objects
+   * of the pyramid planes, as the reference's kernels sample) or another fe_sampling mode
+   * (FE_SAMPLE_TEXTURE restates that filtering in FP32, bit for bit with the CPU restatement). */
+  explicit GPULKFeatureTracker(int sampling = FE_SAMPLE_HARDWARE) : sampling_(sampling) {}
   virtual ~GPULKFeatureTracker() = default;
 
   /* GPULKFeatureTracker::track_points (cuda_modules/lk_tracker.cpp:24-73): tracks the first

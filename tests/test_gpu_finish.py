@@ -7,7 +7,7 @@ import pytest
 import torch
 
 from conftest import assert_tracks_equal, gpu_pyramid
-from cuvslam_b200 import synthetic
+from cuvslam_b200 import _lib, synthetic
 from cuvslam_b200.frontend import (Batch, CameraFrame, ImagePyramid, Selection, TrackFinish, finish_tracks,
                                    track_mono, tracks_from_device, tracks_to_device)
 from cuvslam_b200.types import make_tracks
@@ -21,7 +21,7 @@ def test_retrack_matches_oracle(ctx, oracle, golden, name):
     tin = ref[f"{name}/lk_pred/in"]
     pp, cp = gpu_pyramid(ctx, inp[f"{name}/prev"]), gpu_pyramid(ctx, inp[f"{name}/next"])
     d = tracks_to_device(tin)
-    track_mono(ctx, pp, cp, d, 0.85)
+    track_mono(ctx, pp, cp, d, 0.85, sampling=_lib.FE_SAMPLE_TEXTURE)
     got = tracks_from_device(d)
     want = oracle.lk_retrack(oracle.pyramid(inp[f"{name}/prev"]), oracle.pyramid(inp[f"{name}/next"]), tin, 0.85)
     assert_tracks_equal(got, want)
@@ -89,7 +89,7 @@ def test_batched_step_with_finish_equals_plain_and_oracle(ctx, oracle):
         fin = TrackFinish(torch.from_numpy(age.astype(np.int32)).cuda(), 0.85)
         frames.append(CameraFrame(torch.from_numpy(nx).cuda(), ImagePyramid(w, h), pp, tracks_to_device(t), 450,
                                   (2, 2, 2, 2), finish=fin))
-    b = Batch(ctx, frames)
+    b = Batch(ctx, frames, _lib.FE_SAMPLE_TEXTURE)  # compared with the oracle bit for bit
     b.run()
     torch.cuda.synchronize()
     batched = [(tracks_from_device(f.tracks), f.finish.age.cpu().numpy().copy(),

@@ -1,13 +1,13 @@
-"""LK with the texture unit's own filtering (FE_SAMPLE_HARDWARE, lk_hw.cu).
+"""LK with the texture unit's own filtering (FE_SAMPLE_HARDWARE, lk_hw.cu), the default sampling of
+the LK wrappers.
 
-Its samples are the reference's (the same hardware filtering at the same coordinates) and its
-arithmetic is written as the reference writes it, but its window sums run in this library's order
-(lane partial sums, then the xor butterfly), so it is compared with tolerances:
-  - against the reference kernels' outputs (tests/golden/reference.npz): statuses identical except
-    at most one marginal track per run, positions of tracks both keep within 0.01 px (max) and
-    1e-4 px (median);
-  - against the oracle's wide texture mode: statuses agree on >= 99% of tracks, positions within
-    0.01 px (max);
+Its samples are the reference's (the same hardware filtering at the same coordinates), its
+arithmetic is written as the reference writes it and its window sums pair lanes as the reference's
+warp reduction does, so it equals the reference kernels' outputs bit for bit:
+  - against the reference kernels' outputs (tests/golden/reference.npz): every record field
+    identical, for the 2-D, predicted, NCC-0.85, horizontal and 4-level runs;
+  - against the oracle's wide texture mode (an FP64 restatement of the texture unit's filtering):
+    statuses agree on >= 99% of tracks, positions within 0.01 px (max);
   - the batched step in this mode equals its per-camera calls bit for bit (same kernel).
 """
 
@@ -52,8 +52,7 @@ def test_matches_reference(ctx, golden, name, run):
     tin, tout = ref[f"{name}/{src}/in"], ref[f"{name}/{run}/out"]
     ml = 4 if run == "lk_pred4" else 10
     pp, cp = gpu_pyramid(ctx, inp[f"{name}/prev"], ml), gpu_pyramid(ctx, inp[f"{name}/next"])
-    got = _run(ctx, pp, cp, tin, run == "lk_horiz")
-    _agree(got, tout, 1, 0.01, 1e-4)
+    assert_tracks_equal(_run(ctx, pp, cp, tin, run == "lk_horiz"), tout)
 
 
 @pytest.mark.parametrize("name", ["c1", "half"])
