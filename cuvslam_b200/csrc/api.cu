@@ -996,6 +996,7 @@ struct fe_batch {
   StagePlan plan;
   fe::LkCam* d_lk = nullptr;
   fe::LkTex* d_tex = nullptr;  // FE_SAMPLE_HARDWARE: texture objects per LK camera
+  CUtensorMap* d_grad_tmaps = nullptr;  // selection cameras' [gx, gy] level-0 tensor maps
   int* lk_counter = nullptr;
   fe::LkLaunch lk;
   fe::SelectBatch* sel = nullptr;  // heap: large
@@ -1019,31 +1020,34 @@ struct fe_batch {
 
 namespace {
 
-// One frame step.  After the pyramids the step forks: LK on `st` and the selection's response tiles
-// (which do not depend on tracking) on `side` run concurrently; the rest of the selection (burn of
-// the LK survivors, burned cells, quotas, order) joins after both.
-// overlap 1: the fork follows the whole pyramid (response tiles beside LK); overlap 2: it follows the
-// levels 0-2 stage (response tiles beside the deeper pyramid stages and LK).
-int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap = 1) {
-  const size_t split = overlap == 2 ? 1 : b->plan.size();
+// One frame step: the pyramids, LK (and the finish filters), the selection's response tiles (which
+// do not depend on tracking), then the rest of the selection (burn of the LK survivors, burned
+// cells, quotas, order).  Where the response tiles run (`overlap`):
+//   0: after LK on `st` (LK reads the pyramids the pyramid launch has just left in L2);
+//   1: on `side`, forked after the whole pyramid, beside LK; joined before the rest;
+//   2: on `side`, forked after the levels 0-2 stage, beside the deeper pyramid stages and LK;
+//   3: before LK on `st`.
+int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap) {
+  const bool fork = b->any_select && side && (overlap == 1 || overlap == 2);
+  const size_t split = (fork && overlap == 2) ? 1 : b->plan.size();
   int rc = run_stages(b->plan, 0, split, st);
   if (rc) return rc;
   if (b->any_select) FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
-  const bool fork = b->any_select && side;
   if (fork) {
     FE_CUDA(cudaEventRecord(b->fork_ev, st));
     FE_CUDA(cudaStreamWaitEvent(side, b->fork_ev, 0));
     FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, side));
-  } else if (b->any_select) {
-    FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   }
   rc = run_stages(b->plan, split, b->plan.size(), st);
   if (rc) return rc;
+  if (b->any_select && !fork && overlap == 3) FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   if (b->lk.total > 0) FE_CUDA(fe::launch_lk(b->lk, st));
   if (b->finish) FE_CUDA(fe::launch_finish(*b->finish, st));
   if (fork) {
     FE_CUDA(cudaEventRecord(b->join_ev, side));
     FE_CUDA(cudaStreamWaitEvent(st, b->join_ev, 0));
+  } else if (b->any_select && overlap != 3) {
+    FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   }
   if (b->any_select)
     FE_CUDA(fe::launch_select_rest(*b->sel, b->touched_words, b->bin_cap, b->final_cap, st));
@@ -1059,7 +1063,7 @@ int capture_batch(fe_batch* b) {
   b->lk.shape = b->lk_shape;
   cudaError_t e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(e);
-  int rc = enqueue_batch(b, b->cap_stream, b->overlap ? b->side_stream : nullptr, b->overlap);
+  int rc = enqueue_batch(b, b->cap_stream, b->side_stream, b->overlap);
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(b->cap_stream, &g);
   if (rc) {
@@ -1150,7 +1154,7 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
     if (!rc && t < best) best = t;
     else b->lk_shape = keep;
   }
-  for (int ov = 0; !rc && b->any_select && ov < 3; ++ov) {
+  for (int ov = 0; !rc && b->any_select && ov < 4; ++ov) {
     if (ov == b->overlap) continue;
     const int keep = b->overlap;
     b->overlap = ov;
@@ -1183,7 +1187,7 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
 
 int fe_batch_set_tuning(fe_batch* b, int lk_shape, int overlap, int stage_tile) {
   const int tile = stage_tile & ~fe::kL012Three;
-  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (tile != 8 && tile != 16) || overlap < 0 || overlap > 2)
+  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (tile != 8 && tile != 16) || overlap < 0 || overlap > 3)
     return FE_ERR_INVALID_ARGUMENT;
   b->lk_shape = lk_shape;
   b->overlap = overlap;
@@ -1414,6 +1418,28 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
       sc.tile_begin = b->sel_tiles;
       b->sel_tiles += sc.tiles_x * sc.tiles_y;
     }
+    // the response tiles of cameras whose level-0 gradient planes meet TMA alignment stage their
+    // interior windows by TMA (the others with asynchronous 16-byte copies)
+    sb.status = ctx->dev_status;
+    sb.wait_limit = ctx->wait_limit;
+    if (sb.ncams > 0) {
+      std::vector<CUtensorMap> maps((size_t)2 * sb.ncams);
+      std::vector<char> ok(sb.ncams, 0);
+      bool any = false;
+      for (int k = 0; k < sb.ncams; ++k) {
+        const fe::SelectCam& sc = sb.cam[k];
+        ok[k] = fe::encode_select_grad_tmaps(&maps[2 * k], sc.gx, sc.gy, sc.w, sc.h, sc.pitch) ? 1 : 0;
+        any = any || ok[k];
+      }
+      if (any) {
+        cudaError_t e = dev_alloc((void**)&b->d_grad_tmaps, sizeof(CUtensorMap) * maps.size());
+        if (e == cudaSuccess)
+          e = cudaMemcpy(b->d_grad_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fail(cuda_fail(e));
+        for (int k = 0; k < sb.ncams; ++k)
+          if (ok[k]) sb.cam[k].grad_tmap = b->d_grad_tmaps + 2 * k;
+      }
+    }
   }
   // capture the step into a graph
   cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
@@ -1543,6 +1569,7 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   if (b->side_stream) cudaStreamDestroy(b->side_stream);
+  if (b->d_grad_tmaps) cudaFree(b->d_grad_tmaps);
   if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->join_ev) cudaEventDestroy(b->join_ev);
   if (b->d_lk) cudaFree(b->d_lk);

@@ -60,6 +60,10 @@ int l012_deep_floats();  // shared-memory floats a deeper-level item of the leve
 // Encodes the uint8 frame's tensor map into job.tmap; returns false when the frame does not meet
 // TMA alignment (the stage then stages its tile with ordinary loads).
 bool encode_frame_tmap(StageJob& job);
+// Encodes a 2-D FP32 plane's tensor map (w x h floats, rows pitch_floats apart) with a box of
+// box_w x box_h floats; false when the driver entry point is missing or the plane does not meet TMA
+// alignment (16-byte base and pitch).
+bool encode_plane_tmap_f32(CUtensorMap* map, const float* base, int w, int h, int pitch_floats, int box_w, int box_h);
 cudaError_t pyramid_init();  // kernel attributes; call once per device before capture
 cudaError_t launch_pyramid_stage(const StageBatch& b, int tiles, bool u8, int nl, int kt, bool tail, cudaStream_t s);
 // Level 0 of a pyramid from a uint8 mono (channels 1) or RGB8 (channels 3) frame: the reference's cast
@@ -100,15 +104,24 @@ struct SelectCam {
   float2* q_xy;
   int q_cap;
   int tiles_x, tiles_y, tile_begin;  // 32x32 response tiles
+  const CUtensorMap* grad_tmap;  // optional: [gx, gy] tensor maps (device memory, 64-byte aligned)
+                                 // whose box is a response tile's gradient window: interior tiles
+                                 // are then staged by TMA
 };
 
 struct SelectBatch {
   int ncams;
   int debug;
+  int* status;     // device flags (bit 2: a response tile's TMA staging did not arrive; the tile
+                   // is skipped), or null
+  int wait_limit;  // iterations of that bounded wait
   SelectCam cam[kMaxCams];
 };
 
 constexpr int kMaxSelectKeys = 16384;  // shared-memory sort capacity of the selection kernels
+// The [gx, gy] tensor maps of a camera's level-0 gradient planes with the response tile's gradient
+// window as their box (SelectCam::grad_tmap); false when the planes do not meet TMA alignment.
+bool encode_select_grad_tmaps(CUtensorMap* maps, const float* gx, const float* gy, int w, int h, int pitch_floats);
 int select_tile_w();  // response tile (level-0 pixels)
 int select_tile_h();
 cudaError_t select_init();

@@ -1001,19 +1001,45 @@ int l012_deep_floats() { return l012::kDeepFloats; }
 
 int stage_tile(bool u8, int nl, int kt) { return (u8 && nl == 2) ? l012::kT2 : ((kt & 31) == 16 ? 16 : 8); }
 
-bool encode_frame_tmap(StageJob& job) {
-  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  // looked up once per process; the initialisation of a function-local static is thread-safe
-  static const Encode encode = []() -> Encode {
+namespace {
+
+using TmapEncode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point, looked up once per process (the
+// initialisation of a function-local static is thread-safe); null when unavailable.
+TmapEncode tmap_encoder() {
+  static const TmapEncode encode = []() -> TmapEncode {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      return reinterpret_cast<Encode>(fn);
+      return reinterpret_cast<TmapEncode>(fn);
     return nullptr;
   }();
+  return encode;
+}
+
+}  // namespace
+
+bool encode_plane_tmap_f32(CUtensorMap* map, const float* base, int w, int h, int pitch_floats, int box_w, int box_h) {
+  const TmapEncode encode = tmap_encoder();
+  if (!encode || !map || !base || w <= 0 || h <= 0 || box_w <= 0 || box_h <= 0 || box_w > 256 || box_h > 256)
+    return false;
+  const int64_t pitch_bytes = (int64_t)pitch_floats * 4;
+  if (((uintptr_t)base % 16) != 0 || (pitch_bytes % 16) != 0 || ((int64_t)box_w * 4) % 16 != 0) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
+  const cuuint64_t strides[1] = {(cuuint64_t)pitch_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool encode_frame_tmap(StageJob& job) {
+  const TmapEncode encode = tmap_encoder();
   job.use_tma = 0;
   if (!encode) return false;
   // TMA needs a 16-byte aligned base and pitch; frames smaller than the box use plain loads

@@ -158,11 +158,26 @@ constexpr int kSmem = kOffG + 2 * GH * GS * 4;
 
 __device__ __forceinline__ float2 dup(float c) { return make_float2(c, c); }
 
+// Bounded wait on phase `phase` of the mbarrier at shared address `bar`: false when `limit` polls
+// all found it incomplete.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase, int limit) {
+  for (int i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 
 template <bool kSplit>
 __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_constant__ SelectBatch b) {
   using namespace tile;
-  extern __shared__ __align__(16) unsigned char tsm[];
+  extern __shared__ __align__(128) unsigned char tsm[];
   float* hxx = reinterpret_cast<float*>(tsm + kOffH);
   float* hxy = hxx + GH * HS;
   float* hyy = hxy + GH * HS;
@@ -171,6 +186,7 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
   float* resp = reinterpret_cast<float*>(tsm + kOffG);  // after the horizontal pass
   float* nms = hxx;                                      // after the vertical pass
   __shared__ float part[8][8];
+  __shared__ __align__(8) uint64_t tbar;  // the TMA staging's mbarrier
 
   int lo = 0, hi = b.ncams - 1;
   while (lo < hi) {
@@ -187,7 +203,37 @@ __global__ void __launch_bounds__(tile::kThreads) tile_kernel(const __grid_const
   //    clamped, as its texture does, for images smaller than the mirror span).  Every copy is an
   //    asynchronous global->shared copy issued before the one wait, so a thread has all of its
   //    loads in flight at once.
-  if (X >= 4 && Y >= 4 && X - 4 + GW <= w && Y - 4 + GH <= h) {
+  const bool interior = X >= 4 && Y >= 4 && X - 4 + GW <= w && Y - 4 + GH <= h;
+  if (interior && c.grad_tmap) {
+    // interior tile, batched path: one TMA copy per plane of the GS x GH box at (X - 4, Y - 4)
+    // (X - 4 is a multiple of 4: its byte offset a multiple of 16; the box's two spare columns are
+    // not read), completing on an mbarrier.  The wait is bounded: a copy that does not arrive skips
+    // the tile and raises the batch's status flag.
+    const uint32_t bar = smem_addr(&tbar);
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(2 * GH * GS * 4)
+                   : "memory");
+#pragma unroll
+      for (int plane = 0; plane < 2; ++plane)
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_addr(plane ? gys : gxs)),
+            "l"(reinterpret_cast<uint64_t>(c.grad_tmap + plane)), "r"(X - 4), "r"(Y - 4), "r"(bar)
+            : "memory");
+    }
+    if (__syncthreads_or(!mbar_wait_bounded(bar, 0, b.wait_limit))) {
+      if (tid == 0 && b.status) atomicOr(b.status, 4);
+      // the copies may still land: wait once more with the full bound, so that no write targets a
+      // retired CTA's shared memory
+      mbar_wait_bounded(bar, 0, kDefaultWaitLimit);
+      return;
+    }
+  } else if (interior) {
     // interior tile: 16-byte copies (X - 4 is a multiple of 4 and rows are 16-byte aligned)
     for (int i = tid; i < GH * 19 * 2; i += kThreads) {
       const int plane = i / (GH * 19), k = i - plane * (GH * 19);
@@ -667,6 +713,11 @@ __global__ void final_kernel(const __grid_constant__ SelectBatch b, int key_cap)
 }
 
 }  // namespace
+
+bool encode_select_grad_tmaps(CUtensorMap* maps, const float* gx, const float* gy, int w, int h, int pitch_floats) {
+  return encode_plane_tmap_f32(maps, gx, w, h, pitch_floats, tile::GS, tile::GH) &&
+         encode_plane_tmap_f32(maps + 1, gy, w, h, pitch_floats, tile::GS, tile::GH);
+}
 
 int select_tile_w() { return tile::TW; }
 int select_tile_h() { return tile::TH; }

@@ -124,8 +124,10 @@ FE_API int fe_destroy(fe_context* ctx);
  * pyramid does wait (a tile for its TMA copy, a deeper level for the tiles it reads), each wait
  * bounded.  A wait that runs out skips its work and sets a flag in the context's device status word
  * instead of hanging: bit 0 = a tile's staging copy did not arrive (the tile is not written), bit 1 =
- * a deeper-level item gave up waiting for its inputs (its levels are not written).  Every pyramid
- * launched through this context (fe_build_pyramid*, batches, adjoint plans) reports there.
+ * a deeper-level item gave up waiting for its inputs (its levels are not written), bit 2 = a
+ * batch's response tile gave up waiting for its gradient window's TMA copy (its cells and sums are
+ * not written).  Every pyramid launched through this context (fe_build_pyramid*, batches, adjoint
+ * plans) and every batch's selection reports there.
  * fe_device_status synchronises `stream`, copies the word to *flags (may be NULL), clears it and
  * returns FE_ERR_DEVICE_FAULT when any flag was set, FE_OK otherwise. */
 FE_API int fe_device_status(fe_context* ctx, fe_stream stream, int32_t* flags);
@@ -431,15 +433,15 @@ FE_API int fe_batch_kernel_count(fe_batch* batch);
 FE_API int fe_batch_run_plain(fe_batch* batch, fe_stream stream);
 /* Autotuner: times the planned step (reps graph launches per candidate, after one warm-up) over
  *   the LK block shape (warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 12x2),
- *   the response tiles after LK (0), on a second stream beside LK (1), or beside the deeper
- *   pyramid stages and LK (2),
+ *   the response tiles after LK (0), on a second stream beside LK (1), beside the deeper
+ *   pyramid stages and LK (2), or before LK (3),
  *   the generic pyramid stages' deepest-level tile (8 or 16) and the levels 0-2 kernel's register
  *   budget (2 or 3 CTAs per SM; stage_tile | 64 for 3),
  * one after the other (coordinate descent), keeps the fastest and re-captures the graph.  The
  * tracks are restored to their values before the call; the selection outputs hold the last run's.
  * Synchronises `stream`; allocates (call it before any capture of your own). */
 FE_API int fe_batch_autotune(fe_batch* batch, int reps, fe_stream stream);
-/* Sets the shapes directly (lk_shape 0..3 in the order above, overlap 0..2, stage_tile 8 or 16,
+/* Sets the shapes directly (lk_shape 0..3 in the order above, overlap 0..3, stage_tile 8 or 16,
  * plus 64 for the three-CTA levels 0-2 kernel) and re-captures the graph. */
 FE_API int fe_batch_set_tuning(fe_batch* batch, int lk_shape, int overlap, int stage_tile);
 /* The shapes in use (defaults 0, 1, 8 until fe_batch_autotune runs). */

@@ -46,9 +46,9 @@ def test_bench_uses_the_oracle_only_in_cpu_legs():
         if isinstance(node, ast.FunctionDef) and any(m.split(".")[0] == "oracle" for m in _imports(node)):
             users.add(node.name)
     # the reference arm / CPU baseline of the headline, the CPU legs of the other workloads, and the
-    # parity checker against the reference's own kernels
+    # checkers against the reference's own kernels (the headline's parity, the stream's deviation)
     assert users <= {"cpu_reference_step_fn", "config_sequence", "config_stereo_plain", "config_l2r",
-                     "config_affine", "reference_parity"}, users
+                     "config_affine", "reference_parity", "stream_reference_deviation"}, users
     assert "main" not in users
 
 

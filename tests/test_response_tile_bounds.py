@@ -29,6 +29,22 @@ def test_regions_fit_and_alias_as_stated():
     assert TH * TW <= GH * HS  # the NMS map fits in the first sums plane
 
 
+def test_tma_staging_box():
+    """Interior tiles of batches stage each gradient plane with one TMA copy of a GS x GH box at
+    (X - 4, Y - 4): the box fills its plane exactly, the planes start 128-byte aligned in the
+    dynamic shared memory, and the copy's x coordinate and row bytes meet TMA's 16-byte rule for
+    every tile origin X (a multiple of TW); the box's last GS - GW columns are never read (phase
+    B reads columns below GW)."""
+    box_w, box_h = GS, GH
+    assert box_w <= 256 and box_h <= 256 and (box_w * 4) % 16 == 0
+    for plane in range(2):
+        start = (OFF_G + plane * GH * GS) * 4
+        assert start % 128 == 0 and start + box_w * box_h * 4 <= SMEM_FLOATS * 4
+    for X in range(TW, 4096, TW):
+        assert ((X - 4) * 4) % 16 == 0
+    assert max(q0 + 9 for q0 in range(0, HS, 4)) < GW
+
+
 def test_phases_read_written_cells():
     grads = np.zeros((GH, GS), bool)  # either plane
     # A (interior tiles): per row 18 copies of 16 bytes and one of 8 -> columns 0..73
