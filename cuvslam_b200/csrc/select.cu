@@ -620,10 +620,16 @@ __global__ void __launch_bounds__(512) quota_kernel(const __grid_constant__ Sele
 }
 
 // ---------------------------------------------------------------- per-bin selection
+// Ascending bitonic sort of n_pow2 (a power of two) keys in shared memory by the whole block
+// (blockDim.x a multiple of 32).  Compare-exchange steps whose partner index i ^ j lies in the same
+// run of 32 keys (j <= 16) run in registers, lane i of a warp holding key i of its run and swapping
+// through shuffles, so the block meets at a barrier once per merge width k for them instead of once
+// per step; wider steps exchange through shared memory.  The network is the same, so is the result.
 template <typename K>
 __device__ void block_bitonic_sort(K* keys, int n_pow2) {
+  const int lane = threadIdx.x & 31;
   for (int k = 2; k <= n_pow2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
+    for (int j = k >> 1; j >= 32; j >>= 1) {
       for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
         const int ixj = i ^ j;
         if (ixj > i) {
@@ -637,6 +643,20 @@ __device__ void block_bitonic_sort(K* keys, int n_pow2) {
       }
       __syncthreads();
     }
+    // steps j = min(k/2, 16) .. 1: the lower index of a pair keeps the smaller key when the run of
+    // width k ascends ((i & k) == 0) and the larger one when it descends
+    for (int base = (int)(threadIdx.x & ~31u); base < n_pow2; base += blockDim.x) {
+      const int i = base + lane;
+      K v = i < n_pow2 ? keys[i] : K(0);
+      const bool up = (i & k) == 0;
+      for (int j = min(k >> 1, 16); j > 0; j >>= 1) {
+        const K o = __shfl_xor_sync(0xffffffffu, v, j);
+        const bool lower = (lane & j) == 0;
+        v = (lower == up) ? (o < v ? o : v) : (o > v ? o : v);
+      }
+      if (i < n_pow2) keys[i] = v;
+    }
+    __syncthreads();
   }
 }
 
