@@ -11,8 +11,8 @@
 //                    does not depend on tracking and runs concurrently with LK; cells_kernel then
 //                    redoes the cells that alive features burned into.
 //   quota_kernel   : per camera: 64 bin sums in a fixed order, the strength total, per-bin quotas.
-//   bin_kernel     : per (bin, camera): filter the bin's candidates (borders, mask), sort by key
-//                    and keep the best `quota` of them.
+//   bin_kernel     : per (bin, camera): filter the bin's candidates (borders, mask) and keep the
+//                    best `quota` of them (a radix select of the quota-th key; final_kernel orders).
 //   final_kernel   : per camera: sort the kept candidates and emit the first num_desired.
 //
 // Parity with GPUSelection::computeGFTTAndSelectFeatures (selection_v2.cpp:27-184):
@@ -660,6 +660,60 @@ __device__ void block_bitonic_sort(K* keys, int n_pow2) {
   }
 }
 
+// The k-th smallest (1 <= k < n) of n distinct keys in shared memory, by the whole block: a radix
+// select from the top byte down.  Each pass histograms the byte of the keys that share the bytes
+// fixed so far, and warp 0 finds the bucket that holds the k-th key (each lane scanning eight
+// buckets after a prefix sum over the lanes).  Returned to every thread.
+__device__ uint64_t block_select_kth(const uint64_t* keys, int n, int k) {
+  __shared__ int hist[256];
+  __shared__ uint64_t s_prefix;
+  __shared__ int s_k;
+  if (threadIdx.x == 0) {
+    s_prefix = 0ull;
+    s_k = k;
+  }
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint64_t prefix = s_prefix;
+    const uint64_t hi = shift == 56 ? 0ull : (~0ull << (shift + 8));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint64_t key = keys[i];
+      if ((key & hi) == prefix) atomicAdd(&hist[(int)(key >> shift) & 255], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      int h[8], sum = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        h[q] = hist[8 * lane + q];
+        sum += h[q];
+      }
+      int incl = sum;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+      }
+      const int kk = s_k;
+      int cum = incl - sum;
+      if (cum < kk && kk <= incl) {
+        int sel = 7;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (sel == 7 && q < 7 && cum + h[q] >= kk) sel = q;
+          else if (sel == 7 && q < 7) cum += h[q];
+        }
+        s_prefix = prefix | ((uint64_t)(8 * lane + sel) << shift);
+        s_k = kk - cum;
+      }
+    }
+    __syncthreads();
+  }
+  return s_prefix;
+}
+
 __global__ void bin_kernel(const __grid_constant__ SelectBatch b, int key_cap) {
   extern __shared__ uint64_t keys[];
   __shared__ int count;
@@ -693,18 +747,21 @@ __global__ void bin_kernel(const __grid_constant__ SelectBatch b, int key_cap) {
   __syncthreads();
   const int n = min(count, key_cap);
   if (count > key_cap && threadIdx.x == 0) atomicOr(&c.stats[3], 1);  // capacity flag
-  int np = 1;
-  while (np < n) np <<= 1;
-  for (int i = n + threadIdx.x; i < np; i += blockDim.x) keys[i] = ~0ull;
-  __syncthreads();
-  block_bitonic_sort(keys, np);
+  // the bin keeps its `keep` smallest keys (strongest first); final_kernel orders all kept keys, so
+  // only the set matters here: every key up to the keep-th smallest (keys are distinct, a cell each)
   const int keep = min(want, n);
-  __shared__ int base;
-  if (threadIdx.x == 0) base = atomicAdd(&c.stats[2], keep);
+  const uint64_t last = keep < n ? block_select_kth(keys, n, keep) : ~0ull;
+  __shared__ int base, written;
+  if (threadIdx.x == 0) {
+    base = atomicAdd(&c.stats[2], keep);
+    written = 0;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < keep; i += blockDim.x) {
-    const int slot = base + i;
-    if (slot < c.q_cap) c.q_keys[slot] = keys[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint64_t key = keys[i];
+    if (key > last) continue;
+    const int slot = base + atomicAdd(&written, 1);
+    if (slot < c.q_cap) c.q_keys[slot] = key;
     else atomicOr(&c.stats[3], 2);
   }
 }
