@@ -1000,6 +1000,7 @@ struct fe_batch {
   int* lk_counter = nullptr;
   fe::LkLaunch lk;
   fe::SelectBatch* sel = nullptr;  // heap: large
+  fe::SelectBatch* sel_burned = nullptr;  // the same cameras without touched-cell marks (placement 4)
   int sel_tiles = 0, bin_cap = 1, final_cap = 1, touched_words = 0;
   void* sel_mem = nullptr;
   size_t zero_bytes = 0;
@@ -1026,7 +1027,9 @@ namespace {
 //   0: after LK on `st` (LK reads the pyramids the pyramid launch has just left in L2);
 //   1: on `side`, forked after the whole pyramid, beside LK; joined before the rest;
 //   2: on `side`, forked after the levels 0-2 stage, beside the deeper pyramid stages and LK;
-//   3: before LK on `st`.
+//   3: before LK on `st`;
+//   4: after LK on `st`, after the burn of the LK survivors (alive_kernel), which the tiles then
+//      apply themselves, as the single-camera selection does: no burned-cell pass, no response map.
 int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap) {
   const bool fork = b->any_select && side && (overlap == 1 || overlap == 2);
   const size_t split = (fork && overlap == 2) ? 1 : b->plan.size();
@@ -1046,6 +1049,9 @@ int enqueue_batch(fe_batch* b, cudaStream_t st, cudaStream_t side, int overlap) 
   if (fork) {
     FE_CUDA(cudaEventRecord(b->join_ev, side));
     FE_CUDA(cudaStreamWaitEvent(st, b->join_ev, 0));
+  } else if (b->any_select && overlap == 4) {
+    FE_CUDA(fe::launch_select(*b->sel_burned, b->sel_tiles, b->bin_cap, b->final_cap, st));
+    return FE_OK;
   } else if (b->any_select && overlap != 3) {
     FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
   }
@@ -1154,7 +1160,7 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
     if (!rc && t < best) best = t;
     else b->lk_shape = keep;
   }
-  for (int ov = 0; !rc && b->any_select && ov < 4; ++ov) {
+  for (int ov = 0; !rc && b->any_select && ov < 5; ++ov) {
     if (ov == b->overlap) continue;
     const int keep = b->overlap;
     b->overlap = ov;
@@ -1187,7 +1193,7 @@ int fe_batch_autotune(fe_batch* b, int reps, fe_stream stream) {
 
 int fe_batch_set_tuning(fe_batch* b, int lk_shape, int overlap, int stage_tile) {
   const int tile = stage_tile & ~fe::kL012Three;
-  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (tile != 8 && tile != 16) || overlap < 0 || overlap > 3)
+  if (!b || lk_shape < 0 || lk_shape >= fe::kLkShapes || (tile != 8 && tile != 16) || overlap < 0 || overlap > 4)
     return FE_ERR_INVALID_ARGUMENT;
   b->lk_shape = lk_shape;
   b->overlap = overlap;
@@ -1440,6 +1446,10 @@ int fe_batch_create(fe_context* ctx, const fe_camera_frame* cams, int ncams, int
           if (ok[k]) sb.cam[k].grad_tmap = b->d_grad_tmaps + 2 * k;
       }
     }
+    b->sel_burned = new (std::nothrow) fe::SelectBatch;
+    if (!b->sel_burned) return fail(FE_ERR_OUT_OF_MEMORY);
+    *b->sel_burned = sb;
+    for (int k = 0; k < sb.ncams; ++k) b->sel_burned->cam[k].touched = nullptr;
   }
   // capture the step into a graph
   cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
@@ -1580,6 +1590,7 @@ int fe_batch_destroy(fe_batch* b) {
   if (b->finish_cells) cudaFree(b->finish_cells);
   delete b->finish;
   delete b->sel;
+  delete b->sel_burned;
   delete b;
   return FE_OK;
 }

@@ -428,7 +428,7 @@ class Batch:
         _lib.check(self.ctx.lib.fe_batch_autotune(self.handle, int(reps), _stream_handle(stream)), "fe_batch_autotune")
         return self.tuning()
 
-    OVERLAP = ["after LK", "beside LK", "beside deep pyramid stages and LK", "before LK"]
+    OVERLAP = ["after LK", "beside LK", "beside deep pyramid stages and LK", "before LK", "after LK and the burn"]
 
     def set_tuning(self, lk_block="8x4", response_overlap="beside LK", stage_tile=8, l012_ctas_per_sm=2):
         shape = ["8x4", "8x3", "4x8", "12x2"].index(lk_block)

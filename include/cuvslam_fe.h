@@ -434,14 +434,15 @@ FE_API int fe_batch_run_plain(fe_batch* batch, fe_stream stream);
 /* Autotuner: times the planned step (reps graph launches per candidate, after one warm-up) over
  *   the LK block shape (warps per block x minimum resident blocks: 8x4, 8x3, 4x8, 12x2),
  *   the response tiles after LK (0), on a second stream beside LK (1), beside the deeper
- *   pyramid stages and LK (2), or before LK (3),
+ *   pyramid stages and LK (2), before LK (3), or after LK with the LK survivors' burn applied in
+ *   the tiles, which then need no pass over the burned cells (4),
  *   the generic pyramid stages' deepest-level tile (8 or 16) and the levels 0-2 kernel's register
  *   budget (2 or 3 CTAs per SM; stage_tile | 64 for 3),
  * one after the other (coordinate descent), keeps the fastest and re-captures the graph.  The
  * tracks are restored to their values before the call; the selection outputs hold the last run's.
  * Synchronises `stream`; allocates (call it before any capture of your own). */
 FE_API int fe_batch_autotune(fe_batch* batch, int reps, fe_stream stream);
-/* Sets the shapes directly (lk_shape 0..3 in the order above, overlap 0..3, stage_tile 8 or 16,
+/* Sets the shapes directly (lk_shape 0..3 in the order above, overlap 0..4, stage_tile 8 or 16,
  * plus 64 for the three-CTA levels 0-2 kernel) and re-captures the graph. */
 FE_API int fe_batch_set_tuning(fe_batch* batch, int lk_shape, int overlap, int stage_tile);
 /* The shapes in use (defaults 0, 1, 8 until fe_batch_autotune runs). */
