@@ -1486,8 +1486,12 @@ int fe_batch_run_part(fe_batch* b, int part, fe_stream stream) {
     case FE_PART_SELECT:
       if (b->any_select) {
         FE_CUDA(cudaMemsetAsync(b->sel_mem, 0, b->zero_bytes, st));
-        FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
-        FE_CUDA(fe::launch_select_rest(*b->sel, b->touched_words, b->bin_cap, b->final_cap, st));
+        if (b->overlap == 4) {  // as the step runs it: burn, then tiles that apply it
+          FE_CUDA(fe::launch_select(*b->sel_burned, b->sel_tiles, b->bin_cap, b->final_cap, st));
+        } else {
+          FE_CUDA(fe::launch_select_response(*b->sel, b->sel_tiles, st));
+          FE_CUDA(fe::launch_select_rest(*b->sel, b->touched_words, b->bin_cap, b->final_cap, st));
+        }
       }
       return FE_OK;
     default:
