@@ -13,8 +13,7 @@
 //   quota_kernel   : per camera: 64 bin sums in a fixed order, the strength total, per-bin quotas.
 //   bin_kernel     : per (bin, camera): filter the bin's candidates (borders, mask) and keep the
 //                    best `quota` of them (a radix select of the quota-th key; final_kernel orders).
-//   final_kernel   : per camera: sort the kept candidates and emit the first num_desired (a radix
-//                    sort when they fit 4096 slots, final_radix_kernel; else a bitonic sort).
+//   final_kernel   : per camera: sort the kept candidates and emit the first num_desired.
 //
 // Parity with GPUSelection::computeGFTTAndSelectFeatures (selection_v2.cpp:27-184):
 //   response      gftt_values_kernel (gftt.cu:80-162), same FMA order, __logf as the reference;
@@ -799,104 +798,6 @@ __global__ void final_kernel(const __grid_constant__ SelectBatch b, int key_cap)
   if (threadIdx.x == 0) *c.out_count = out;
 }
 
-// The same order by a stable least-significant-digit radix sort, for cameras whose kept keys fit
-// S x 1024 slots (the padding keys, all ones, sort last: a real key's high word is ~bits of a
-// positive strength, below 0xffffffff).  Keys i = s * 1024 + threadIdx.x; 4-bit digits over the
-// cell bits of the low word (the bits above the camera's largest cell index are zero) and the 32
-// bits of the high word.  Per pass: each warp ranks its keys of a digit with __match_any_sync, the
-// per-(digit, slot, warp) counts are scanned in (digit, slot, warp) order, the keys scatter to the
-// other buffer; the order of equal digits is kept, so after the last pass the keys are sorted.
-template <int S>
-__global__ void __launch_bounds__(1024) final_radix_kernel(const __grid_constant__ SelectBatch b, int key_cap) {
-  extern __shared__ __align__(16) unsigned char fsm[];
-  uint64_t* src = reinterpret_cast<uint64_t*>(fsm);
-  uint64_t* dst = src + S * 1024;
-  int* table = reinterpret_cast<int*>(dst + S * 1024);  // [16][S][32]
-  __shared__ int wtot[32];
-  const SelectCam& c = b.cam[blockIdx.x];
-  const int n = min(min(c.stats[2], c.q_cap), key_cap);
-  if (c.stats[2] > key_cap && threadIdx.x == 0) atomicOr(&c.stats[3], 4);
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const unsigned lower_lanes = (1u << lane) - 1u;
-#pragma unroll
-  for (int s = 0; s < S; ++s) {
-    const int i = s * 1024 + t;
-    src[i] = i < n ? c.q_keys[i] : ~0ull;
-  }
-  const int cells = (c.w / 8) * (c.h / 8);
-  int cb = 0;
-  while ((1 << cb) < cells) cb += 4;
-  constexpr int T = 16 * S * 32;
-  constexpr int E = (T + 1023) / 1024;
-  for (int pass = 0, np = cb / 4 + 8; pass < np; ++pass) {
-    const int shift = pass < cb / 4 ? 4 * pass : 32 + 4 * (pass - cb / 4);
-    for (int k = t; k < T; k += 1024) table[k] = 0;
-    __syncthreads();
-    uint64_t key[S];
-    int dig[S], rank[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-      key[s] = src[s * 1024 + t];
-      dig[s] = (int)(key[s] >> shift) & 15;
-      const unsigned peers = __match_any_sync(0xffffffffu, dig[s]);
-      rank[s] = __popc(peers & lower_lanes);
-      if ((peers & lower_lanes) == 0u) table[(dig[s] * S + s) * 32 + wid] = __popc(peers);
-    }
-    __syncthreads();
-    // exclusive scan of the table in index order
-    int v[E], sum = 0;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int k = t * E + e;
-      v[e] = k < T ? table[k] : 0;
-      sum += v[e];
-    }
-    int incl = sum;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= d) incl += y;
-    }
-    if (lane == 31) wtot[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      int x = wtot[lane];
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= d) x += y;
-      }
-      wtot[lane] = x;
-    }
-    __syncthreads();
-    int base = (wid > 0 ? wtot[wid - 1] : 0) + incl - sum;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int k = t * E + e;
-      if (k < T) table[k] = base;
-      base += v[e];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < S; ++s) dst[table[(dig[s] * S + s) * 32 + wid] + rank[s]] = key[s];
-    __syncthreads();
-    uint64_t* tmp = src;
-    src = dst;
-    dst = tmp;
-  }
-  const int out = min(n, c.stats[4]);
-  for (int i = t; i < out; i += 1024) {
-    const int cell = (int)(src[i] & 0xffffffffu);
-    const float2 p = c.cell_xy[cell];
-    c.out_xy[2 * i] = p.x;
-    c.out_xy[2 * i + 1] = p.y;
-  }
-  if (t == 0) *c.out_count = out;
-}
-
-constexpr int kRadixSlots = 4;  // final_radix_kernel's largest S: kept keys <= 4096 per camera
-size_t radix_smem(int slots) { return (size_t)slots * (2 * 1024 * sizeof(uint64_t) + 16 * 32 * sizeof(int)); }
-
 }  // namespace
 
 bool encode_select_grad_tmaps(CUtensorMap* maps, const float* gx, const float* gy, int w, int h, int pitch_floats) {
@@ -915,10 +816,6 @@ cudaError_t select_init() {
   e = cudaFuncSetAttribute(bin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(uint64_t) * kMaxSelectKeys));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(final_radix_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_smem(3));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(final_radix_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_smem(4));
-  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(sizeof(uint64_t) * kMaxSelectKeys));
 }
@@ -932,15 +829,7 @@ namespace {
 cudaError_t launch_quota_bins_final(const SelectBatch& b, int bin_key_cap, int final_key_cap, cudaStream_t s) {
   quota_kernel<<<b.ncams, 512, 0, s>>>(b);
   bin_kernel<<<dim3(64, b.ncams), 256, sizeof(uint64_t) * bin_key_cap, s>>>(b, bin_key_cap);
-  // the kept keys of a camera fit final_key_cap: the radix sort up to 4096 of them, else the bitonic
-  switch ((final_key_cap + 1023) / 1024) {
-    case 0:
-    case 1: final_radix_kernel<1><<<b.ncams, 1024, radix_smem(1), s>>>(b, final_key_cap); break;
-    case 2: final_radix_kernel<2><<<b.ncams, 1024, radix_smem(2), s>>>(b, final_key_cap); break;
-    case 3: final_radix_kernel<3><<<b.ncams, 1024, radix_smem(3), s>>>(b, final_key_cap); break;
-    case kRadixSlots: final_radix_kernel<4><<<b.ncams, 1024, radix_smem(4), s>>>(b, final_key_cap); break;
-    default: final_kernel<<<b.ncams, 1024, sizeof(uint64_t) * final_key_cap, s>>>(b, final_key_cap);
-  }
+  final_kernel<<<b.ncams, 1024, sizeof(uint64_t) * final_key_cap, s>>>(b, final_key_cap);
   return cudaGetLastError();
 }
 }  // namespace

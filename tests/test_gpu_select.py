@@ -73,10 +73,10 @@ def test_random_configurations(dctx, oracle, seed):
     alive = np.stack([rng.uniform(0, w - 1, 300), rng.uniform(0, h - 1, 300)], 1).astype(np.float32)
     mask = np.zeros((h, w), np.uint8)
     mask[: h // 5, : w // 3] = 1
-    # 6000 wanted: more kept candidates than the final radix sort takes (4096), so the bitonic one
+    # 10000 wanted: more kept candidates than the headline's, up to the whole 1280x720 frame's cells
     for nd, a, m, borders in ((1000, None, None, (0, 0, 0, 0)), (600, alive, mask, (10, 20, 30, 40)),
                               (0, alive, None, (0, 0, 0, 0)), (5, None, None, (0, 0, 0, 0)),
-                              (6000, None, None, (0, 0, 0, 0))):
+                              (10000, None, None, (0, 0, 0, 0))):
         sel, resp, _ = _select(dctx, pyr, a, nd, borders, m)
         s = oracle.select(resp, a, nd, borders, m)
         _same_selection(sel, s["sel"], 2e-4)
